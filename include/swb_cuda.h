@@ -1,0 +1,228 @@
+/*
+ * swb_cuda.h -- C ABI of the B200 (sm_100a) Smith-Waterman hot path of swiftbwa.
+ *
+ * This header is the drop-in boundary.  The Swift Alignment module keeps its
+ * signatures; a maintainer adds this header next to
+ * Sources/CHelpers/include/CHelpers.h (that target is already a C module
+ * imported by Swift, Package.swift:55-58) and links libswb_cuda.so.  Every
+ * entry point below names the reference interface it replaces.
+ *
+ * Conventions
+ *   - Plain C: fixed-width integers, plain pointers and sizes.  No C++ or
+ *     CUDA types cross the boundary.
+ *   - The caller owns host buffers; the library owns device memory.
+ *   - Every call returns an int status: SWB_OK (0) or a negative SWB_ERR_*
+ *     code.  Nothing aborts or traps; swb_strerror() names the code and
+ *     swb_last_error_message() carries detail for the calling thread.
+ *   - A context is internally locked: concurrent calls from several host
+ *     threads (Swift TaskGroup children) on one context are serialised.
+ *   - Bases are 2-bit codes A=0 C=1 G=2 T=3, N=4, one byte per base
+ *     (Sources/BWACore/Base.swift:2-44).  The resident reference is the
+ *     bwa .pac layout: 4 bases per byte, first base in bits 7-6
+ *     (Sources/FMIndex/PackedReference.swift:4-5,34-38).
+ *   - Results are bit-exact with the reference's Swift CPU functions on the
+ *     same inputs (scores, end coordinates, tie-breaks and CIGARs).
+ */
+#ifndef SWB_CUDA_H
+#define SWB_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define SWB_OK                 0
+#define SWB_ERR_INVALID_ARG   -1  /* null pointer, negative length, bad flag   */
+#define SWB_ERR_NO_DEVICE     -2  /* no CUDA device / wrong architecture       */
+#define SWB_ERR_CUDA          -3  /* a CUDA runtime call failed                 */
+#define SWB_ERR_OOM           -4  /* allocation failed or over the memory budget */
+#define SWB_ERR_TOO_LARGE     -5  /* a task exceeds the supported maximum size  */
+#define SWB_ERR_NO_REFERENCE  -6  /* task reads the resident reference; none uploaded */
+#define SWB_ERR_TIMEOUT       -7  /* a bounded device wait ran out              */
+#define SWB_ERR_NOT_FOUND     -8  /* unknown ticket                             */
+#define SWB_ERR_KERNEL        -9  /* a kernel reported an internal check failure */
+
+/* --------------------------------------------------------------- scoring */
+/* Mirrors the SW-relevant fields of ScoringParameters
+ * (Sources/BWACore/ScoringParameters.swift:2-28).  The 5x5 matrix is
+ * derived exactly as scoringMatrix() does (:65-73): a on the diagonal,
+ * -b off it, -1 in any row or column of N. */
+typedef struct swb_scoring {
+    int32_t a;            /* matchScore                  (default 1)   */
+    int32_t b;            /* mismatchPenalty             (default 4)   */
+    int32_t o_ins;        /* gapOpenPenalty              (default 6)   */
+    int32_t e_ins;        /* gapExtendPenalty            (default 1)   */
+    int32_t o_del;        /* gapOpenPenaltyDeletion      (default 6)   */
+    int32_t e_del;        /* gapExtendPenaltyDeletion    (default 1)   */
+    int32_t zdrop;        /* zDrop                       (default 100) */
+    int32_t pen_clip5;    /* penClip5                    (default 5)   */
+    int32_t pen_clip3;    /* penClip3                    (default 5)   */
+    int32_t band_width;   /* bandWidth                   (default 100) */
+    int32_t min_seed_len; /* minSeedLength               (default 19)  */
+} swb_scoring;
+
+/* Fills *s with the defaults of ScoringParameters.init(). */
+void swb_scoring_default(swb_scoring *s);
+
+/* ------------------------------------------------------- task addressing */
+/* A task names its query and target as spans of the caller's `bases`
+ * buffer, or (target only) of the resident 2-bit reference.  Flags let
+ * the kernel read a span reversed and/or complemented, so the left
+ * extension's reversed prefix (ExtensionAligner.swift:209-224) and the
+ * reverse-strand fetch (FMIndex.swift:147-163) need no host copies. */
+#define SWB_Q_REVERSE   0x1u  /* query[j]  = bases[q_off + qlen-1-j]                 */
+#define SWB_T_REVERSE   0x2u  /* target[i] = src[t_off + tlen-1-i]                   */
+#define SWB_T_COMPLEMENT 0x4u /* target[i] = 3 - base (reference codes are 0-3)      */
+#define SWB_T_FROM_REF  0x8u  /* target span is forward reference [t_off, t_off+tlen) */
+
+/* ------------------------------------------------ kernel 1: banded extension */
+/* Field order is SWResult's (Sources/BWACore/SWResult.swift:2-24). */
+typedef struct swb_ext_result {
+    int32_t score;    /* score            */
+    int32_t qle;      /* queryEnd         */
+    int32_t tle;      /* targetEnd        */
+    int32_t gtle;     /* globalTargetEnd  */
+    int32_t gscore;   /* globalScore      */
+    int32_t max_off;  /* maxOff           */
+} swb_ext_result;
+
+/* One call of BandedSWScalar.align(query:target:scoring:w:h0:endBonus:)
+ * (Sources/Alignment/BandedSWScalar.swift:21-28). */
+typedef struct swb_ext_task {
+    uint64_t q_off;      /* query span start in `bases`                      */
+    uint64_t t_off;      /* target span start in `bases` or the reference    */
+    int32_t  qlen;       /* query length  (0 -> all-zero result, :33-35)      */
+    int32_t  tlen;       /* target length (0 -> all-zero result)              */
+    int32_t  w;          /* band width                                        */
+    int32_t  h0;         /* initial score                                     */
+    int32_t  end_bonus;  /* endBonus                                          */
+    uint32_t flags;      /* SWB_Q_REVERSE | SWB_T_*                           */
+} swb_ext_task;          /* 40 bytes */
+
+/* ---------------------------------------- kernel 2: banded global + CIGAR */
+/* One call of GlobalAligner.align(query:target:scoring:w:scoringMatrix:)
+ * (Sources/Alignment/GlobalAligner.swift:19-25); with true_score set and
+ * SWB_GLB_RETRY it also runs CIGARGenerator.generate's band-doubling retry
+ * (CIGARGenerator.swift:88-96) on the device. */
+#define SWB_GLB_RETRY 0x100u
+typedef struct swb_global_task {
+    uint64_t q_off, t_off;
+    int32_t  qlen, tlen;
+    int32_t  w;           /* band width (GlobalAligner's `w`)                 */
+    int32_t  true_score;  /* retry while score < true_score (SWB_GLB_RETRY)   */
+    uint32_t flags;       /* SWB_Q_REVERSE | SWB_T_* | SWB_GLB_RETRY          */
+    int32_t  reserved;
+} swb_global_task;        /* 40 bytes */
+
+/* CIGAR ops are packed (len << 4) | op, op M=0 I=1 D=2 S=4 H=5
+ * (Sources/Alignment/CIGARBuilder.swift:4-37). */
+typedef struct swb_global_result {
+    int32_t  score;       /* h[qlen] of the last attempt (GlobalAligner.swift:144) */
+    int32_t  n_cigar;     /* ops written at cigar + cigar_off                       */
+    int32_t  w_used;      /* band width of the last attempt                         */
+    int32_t  attempts;    /* 1 + retries                                             */
+    uint64_t cigar_off;   /* offset (in ops) of this task's CIGAR in the output      */
+} swb_global_result;
+
+/* ------------------------------------------------ kernel 3: local SW (rescue) */
+/* One call of LocalSWAligner.align(query:target:scoring:scoringMatrix:minSubScore:)
+ * (Sources/Alignment/LocalSWAligner.swift:42-45). */
+typedef struct swb_local_task {
+    uint64_t q_off, t_off;
+    int32_t  qlen, tlen;
+    int32_t  min_sub_score; /* clamped to 0..255 like UInt8(clamping:) (MateRescue.swift:125) */
+    uint32_t flags;
+} swb_local_task;           /* 32 bytes */
+
+/* LocalSWResult (LocalSWAligner.swift:4-23).  The Swift function returns
+ * nil exactly when score == 0 here. */
+typedef struct swb_local_result {
+    int32_t score;
+    int32_t qb, qe;   /* queryBegin, queryEnd (inclusive)   */
+    int32_t tb, te;   /* targetBegin, targetEnd (inclusive) */
+    int32_t score2;
+} swb_local_result;
+
+/* ------------------------------------------------------------------ context */
+typedef struct swb_ctx swb_ctx;
+
+/* Replaces MetalSWEngine.shared (Sources/MetalSW/MetalSWEngine.swift:8-17):
+ * binds `device`, creates the context's stream, and caps the library's
+ * device allocations at mem_budget_bytes (0 = 3/4 of free memory). */
+int  swb_init(int device, size_t mem_budget_bytes, swb_ctx **out);
+void swb_destroy(swb_ctx *ctx);
+const char *swb_strerror(int status);
+/* Detail of the last failing call on this host thread ("" if none). */
+const char *swb_last_error_message(void);
+
+/* Keeps the forward strand resident in HBM in .pac layout
+ * (PackedReference.swift:4-55).  n_bases bases, (n_bases+3)/4 bytes. */
+int swb_upload_reference(swb_ctx *ctx, const uint8_t *pac, uint64_t n_bases);
+
+/* ------------------------------------------------ synchronous batch entry points */
+/* Host buffers in, host results out.  Replaces
+ * BandedSWDispatcher.dispatchBatch8/dispatchBatch16
+ * (Sources/MetalSW/BandedSWDispatcher.swift:48,107); unlike those, one call
+ * returns exact results for every task (no nil, no caller-side rerun). */
+int swb_ext_batch(swb_ctx *ctx, const swb_scoring *sc,
+                  const uint8_t *bases, size_t n_bases,
+                  const swb_ext_task *tasks, size_t n_tasks,
+                  swb_ext_result *out);
+
+/* Replaces GlobalSWDispatcher.dispatchBatch (GlobalSWDispatcher.swift:40).
+ * cigar_out receives every task's ops; results[i].cigar_off indexes it.
+ * cigar_cap must be >= sum over tasks of (qlen + tlen). */
+int swb_global_batch(swb_ctx *ctx, const swb_scoring *sc,
+                     const uint8_t *bases, size_t n_bases,
+                     const swb_global_task *tasks, size_t n_tasks,
+                     swb_global_result *results,
+                     uint32_t *cigar_out, size_t cigar_cap);
+
+/* Replaces LocalSWDispatcher.dispatchBatch (LocalSWDispatcher.swift:31),
+ * with score2 computed on the device (the Metal path hard-codes it to 0,
+ * BWAMemAligner.swift:1942). */
+int swb_local_batch(swb_ctx *ctx, const swb_scoring *sc,
+                    const uint8_t *bases, size_t n_bases,
+                    const swb_local_task *tasks, size_t n_tasks,
+                    swb_local_result *out);
+
+/* ------------------------------------- device-resident entry point (HBM in/out) */
+/* Same as swb_ext_batch with every pointer a device pointer on the
+ * context's device, enqueued on `stream` (a cudaStream_t, NULL = the
+ * context's stream); returns without synchronising. */
+int swb_ext_batch_device(swb_ctx *ctx, const swb_scoring *sc,
+                         const uint8_t *d_bases, const swb_ext_task *d_tasks,
+                         size_t n_tasks, swb_ext_result *d_out, void *stream);
+
+/* --------------------------------------------- single-call Swift signatures */
+/* BandedSWScalar.align (BandedSWScalar.swift:21-28). */
+int swb_banded_sw_align(swb_ctx *ctx, const uint8_t *query, int32_t qlen,
+                        const uint8_t *target, int32_t tlen,
+                        const swb_scoring *sc, int32_t w, int32_t h0,
+                        int32_t end_bonus, swb_ext_result *out);
+/* GlobalAligner.align (GlobalAligner.swift:19-25).  *n_cigar in: capacity
+ * of cigar (>= qlen + tlen), out: ops written. */
+int swb_global_align(swb_ctx *ctx, const uint8_t *query, int32_t qlen,
+                     const uint8_t *target, int32_t tlen,
+                     const swb_scoring *sc, int32_t w,
+                     int32_t *score, uint32_t *cigar, int32_t *n_cigar);
+/* LocalSWAligner.align (LocalSWAligner.swift:42-45); out->score == 0 <=> nil. */
+int swb_local_align(swb_ctx *ctx, const uint8_t *query, int32_t qlen,
+                    const uint8_t *target, int32_t tlen,
+                    const swb_scoring *sc, int32_t min_sub_score,
+                    swb_local_result *out);
+
+/* ------------------------------------------------------- library introspection */
+/* Kernel launches issued by this context so far (for launch accounting). */
+uint64_t swb_kernel_launches(const swb_ctx *ctx);
+/* Device time (ms, CUDA events on the context's stream) of the last
+ * synchronous batch call's kernels, and DP cells it updated. */
+int swb_last_batch_stats(const swb_ctx *ctx, double *kernel_ms, uint64_t *cells);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SWB_CUDA_H */
