@@ -75,7 +75,7 @@ void swb_scoring_default(swb_scoring *s);
  * reverse-strand fetch (FMIndex.swift:147-163) need no host copies. */
 #define SWB_Q_REVERSE   0x1u  /* query[j]  = bases[q_off + qlen-1-j]                 */
 #define SWB_T_REVERSE   0x2u  /* target[i] = src[t_off + tlen-1-i]                   */
-#define SWB_T_COMPLEMENT 0x4u /* target[i] = 3 - base (reference codes are 0-3)      */
+#define SWB_T_COMPLEMENT 0x4u /* target[i] = 3 - base for codes 0-3; N (4) stays N    */
 #define SWB_T_FROM_REF  0x8u  /* target span is forward reference [t_off, t_off+tlen) */
 
 /* ------------------------------------------------ kernel 1: banded extension */

@@ -926,7 +926,7 @@ void load_span(const uint8_t *bases, const uint8_t *pac, uint64_t off, int len, 
     for (int k = 0; k < len; ++k) {
         const uint64_t idx = off + (uint64_t)(rev ? (len - 1 - k) : k);
         uint8_t b = from_ref ? pac_base(pac, (int64_t)idx) : bases[idx];
-        if (comp) b = (uint8_t)(3 - b);
+        if (comp && b < 4) b = (uint8_t)(3 - b);   // N stays N
         dst[k] = b;
     }
 }

@@ -1,0 +1,212 @@
+"""Host-side mirror of swiftbwa's Alignment API over libswb_cuda.so.
+
+Same names, argument meaning and nil behaviour as the reference's Swift
+functions, so a caller (or a parity test) reads like the reference's own
+code; every call goes through the C ABI (include/swb_cuda.h) to the sm_100a
+kernels.  There is no CPU fallback: if the library or a GPU is missing the
+calls raise.
+
+    BandedSWScalar.align(query, target, scoring, w, h0, end_bonus) -> SWResult
+        Sources/Alignment/BandedSWScalar.swift:21-28
+    GlobalAligner.align(query, target, scoring, w) -> GlobalAlignResult
+        Sources/Alignment/GlobalAligner.swift:19-25
+    LocalSWAligner.align(query, target, scoring, min_sub_score) -> LocalSWResult | None
+        Sources/Alignment/LocalSWAligner.swift:42-45
+and the batch dispatchers that replace the Metal ones
+(Sources/MetalSW/BandedSWDispatcher.swift:48,107, GlobalSWDispatcher.swift:40,
+LocalSWDispatcher.swift:31).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import abi
+from .abi import (EXT_RESULT_DTYPE, EXT_TASK_DTYPE, GLOBAL_RESULT_DTYPE, GLOBAL_TASK_DTYPE,
+                  LOCAL_RESULT_DTYPE, LOCAL_TASK_DTYPE, ExtResult, LocalResult, Scoring, ptr)
+
+
+class SWBError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        lib = abi.load_library()
+        msg = lib.swb_strerror(status).decode()
+        detail = lib.swb_last_error_message().decode()
+        super().__init__(f"{where}: {msg} ({status}){': ' + detail if detail else ''}")
+        self.status = status
+
+
+def _check(rc: int, where: str):
+    if rc != abi.SWB_OK:
+        raise SWBError(rc, where)
+
+
+@dataclass(frozen=True)
+class SWResult:
+    """Sources/BWACore/SWResult.swift:2-24."""
+    score: int = 0
+    queryEnd: int = 0
+    targetEnd: int = 0
+    globalTargetEnd: int = 0
+    globalScore: int = 0
+    maxOff: int = 0
+
+    def as_tuple(self):
+        return (self.score, self.queryEnd, self.targetEnd, self.globalTargetEnd,
+                self.globalScore, self.maxOff)
+
+
+@dataclass(frozen=True)
+class GlobalAlignResult:
+    """Sources/Alignment/GlobalAlignResult.swift:2-14."""
+    score: int = 0
+    cigar: tuple = ()
+    nm: int = 0
+
+
+@dataclass(frozen=True)
+class LocalSWResult:
+    """Sources/Alignment/LocalSWAligner.swift:4-23."""
+    score: int
+    queryBegin: int
+    queryEnd: int
+    targetBegin: int
+    targetEnd: int
+    score2: int = 0
+
+    def as_tuple(self):
+        return (self.score, self.queryBegin, self.queryEnd, self.targetBegin, self.targetEnd,
+                self.score2)
+
+
+def _u8(seq) -> np.ndarray:
+    a = np.ascontiguousarray(np.asarray(seq, dtype=np.uint8))
+    return a
+
+
+class Engine:
+    """One library context on one GPU (replaces MetalSWEngine.shared,
+    Sources/MetalSW/MetalSWEngine.swift:8-17)."""
+
+    def __init__(self, device: int = 0, mem_budget_bytes: int = 0):
+        self.lib = abi.load_library()
+        h = C.c_void_p()
+        _check(self.lib.swb_init(device, mem_budget_bytes, C.byref(h)), "swb_init")
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if self.h:
+            self.lib.swb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---------------------------------------------------------------- setup
+    def upload_reference(self, pac: np.ndarray, n_bases: int):
+        pac = np.ascontiguousarray(pac, dtype=np.uint8)
+        _check(self.lib.swb_upload_reference(self.h, ptr(pac), n_bases), "swb_upload_reference")
+
+    # ------------------------------------------------------------- batches
+    def ext_batch(self, sc: Scoring, bases: np.ndarray, tasks: np.ndarray) -> np.ndarray:
+        assert tasks.dtype == EXT_TASK_DTYPE
+        out = np.zeros(len(tasks), EXT_RESULT_DTYPE)
+        bases = np.ascontiguousarray(bases, dtype=np.uint8)
+        _check(self.lib.swb_ext_batch(self.h, C.byref(sc), ptr(bases), bases.size,
+                                      tasks.ctypes.data, len(tasks), out.ctypes.data),
+               "swb_ext_batch")
+        return out
+
+    def global_batch(self, sc: Scoring, bases: np.ndarray, tasks: np.ndarray):
+        assert tasks.dtype == GLOBAL_TASK_DTYPE
+        cap = int((tasks["qlen"].astype(np.int64) + tasks["tlen"]).sum()) + 1
+        res = np.zeros(len(tasks), GLOBAL_RESULT_DTYPE)
+        cig = np.zeros(cap, np.uint32)
+        bases = np.ascontiguousarray(bases, dtype=np.uint8)
+        _check(self.lib.swb_global_batch(self.h, C.byref(sc), ptr(bases), bases.size,
+                                         tasks.ctypes.data, len(tasks), res.ctypes.data,
+                                         ptr(cig, C.c_uint32), cap), "swb_global_batch")
+        return res, cig
+
+    def local_batch(self, sc: Scoring, bases: np.ndarray, tasks: np.ndarray) -> np.ndarray:
+        assert tasks.dtype == LOCAL_TASK_DTYPE
+        out = np.zeros(len(tasks), LOCAL_RESULT_DTYPE)
+        bases = np.ascontiguousarray(bases, dtype=np.uint8)
+        _check(self.lib.swb_local_batch(self.h, C.byref(sc), ptr(bases), bases.size,
+                                        tasks.ctypes.data, len(tasks), out.ctypes.data),
+               "swb_local_batch")
+        return out
+
+    def last_batch_stats(self):
+        ms, cells = C.c_double(), C.c_uint64()
+        _check(self.lib.swb_last_batch_stats(self.h, C.byref(ms), C.byref(cells)), "stats")
+        return ms.value, cells.value
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.swb_kernel_launches(self.h))
+
+    # --------------------------------------------------- single-call forms
+    def banded_sw_align(self, query, target, scoring: Scoring, w: int, h0: int,
+                        end_bonus: int = 0) -> SWResult:
+        q, t = _u8(query), _u8(target)
+        out = ExtResult()
+        _check(self.lib.swb_banded_sw_align(self.h, ptr(q), q.size, ptr(t), t.size, C.byref(scoring),
+                                            w, h0, end_bonus, C.byref(out)), "swb_banded_sw_align")
+        return SWResult(*out.as_tuple())
+
+    def global_align(self, query, target, scoring: Scoring, w: int) -> GlobalAlignResult:
+        q, t = _u8(query), _u8(target)
+        cap = q.size + t.size + 1
+        cig = np.zeros(cap, np.uint32)
+        n = C.c_int32(cap)
+        score = C.c_int32()
+        _check(self.lib.swb_global_align(self.h, ptr(q), q.size, ptr(t), t.size, C.byref(scoring), w,
+                                         C.byref(score), ptr(cig, C.c_uint32), C.byref(n)),
+               "swb_global_align")
+        return GlobalAlignResult(score.value, tuple(int(x) for x in cig[: n.value]))
+
+    def local_align(self, query, target, scoring: Scoring,
+                    min_sub_score: int = 0) -> Optional[LocalSWResult]:
+        q, t = _u8(query), _u8(target)
+        out = LocalResult()
+        _check(self.lib.swb_local_align(self.h, ptr(q), q.size, ptr(t), t.size, C.byref(scoring),
+                                        min_sub_score, C.byref(out)), "swb_local_align")
+        return LocalSWResult(*out.as_tuple()) if out.score != 0 else None
+
+
+_default_lock = threading.Lock()
+_default: Optional[Engine] = None
+
+
+def default_engine() -> Engine:
+    """Process-wide engine on device 0 (the MetalSWEngine.shared analogue)."""
+    global _default
+    with _default_lock:
+        if _default is None:
+            _default = Engine(0)
+        return _default
+
+
+class BandedSWScalar:
+    @staticmethod
+    def align(query, target, scoring: Scoring, w: int, h0: int, endBonus: int = 0) -> SWResult:
+        return default_engine().banded_sw_align(query, target, scoring, w, h0, endBonus)
+
+
+class GlobalAligner:
+    @staticmethod
+    def align(query, target, scoring: Scoring, w: int) -> GlobalAlignResult:
+        return default_engine().global_align(query, target, scoring, w)
+
+
+class LocalSWAligner:
+    @staticmethod
+    def align(query, target, scoring: Scoring, minSubScore: int = 0) -> Optional[LocalSWResult]:
+        return default_engine().local_align(query, target, scoring, minSubScore)

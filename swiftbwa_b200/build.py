@@ -1,0 +1,56 @@
+"""Builds libswb_cuda.so in-tree with nvcc for sm_100a.
+
+    python -m swiftbwa_b200.build [--debug]
+
+The library is a plain C-ABI shared object (include/swb_cuda.h): no torch,
+no Python.  cudart is linked statically so the .so only needs the driver.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "libswb_cuda.so")
+SOURCES = ["swb_runtime.cu", "swb_ext.cu", "swb_global.cu", "swb_local.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def build(debug: bool = False, verbose: bool = False, ptxas_v: bool = False) -> str:
+    srcs = [os.path.join(CSRC, s) for s in SOURCES]
+    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    deps.append(os.path.join(HERE, "..", "include", "swb_cuda.h"))
+    if os.path.exists(OUT) and not debug and not ptxas_v:
+        t = os.path.getmtime(OUT)
+        if all(os.path.getmtime(d) <= t for d in deps):
+            return OUT
+    cmd = [nvcc(), *ARCH, "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3",
+           "-shared", "-o", OUT + ".tmp", *srcs]
+    if debug:
+        cmd += ["-DSWB_DEBUG=1"]
+    if ptxas_v:
+        cmd += ["-Xptxas", "-v"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(OUT + ".tmp", OUT)
+    return OUT
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--debug", action="store_true")
+    ap.add_argument("--ptxas-v", action="store_true")
+    args = ap.parse_args()
+    print(build(debug=args.debug, verbose=True, ptxas_v=args.ptxas_v))

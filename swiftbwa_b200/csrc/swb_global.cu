@@ -1,0 +1,266 @@
+// swb_global.cu -- kernel 2: banded global alignment with CIGAR traceback,
+// bit-exact with GlobalAligner.align (Sources/Alignment/GlobalAligner.swift:19-232)
+// and, per task flag, CIGARGenerator.generate's band-doubling retry
+// (Sources/Alignment/CIGARGenerator.swift:88-96).
+//
+// One thread owns one alignment.  Its H/E rows (int32), staged query and
+// target, and the 4-bit backpointer matrix live in global scratch laid out
+// [index][slot] so the threads of a warp touch adjacent words/bytes.  The
+// backpointer matrix of the last attempt is walked by the same thread; ops
+// are written in traceback order into the task's CIGAR window, merged into
+// runs on the fly, and reversed in place at the end (CIGARBuilder.swift).
+#include "swb_device.cuh"
+#include "swb_internal.h"
+
+namespace swb {
+namespace {
+
+constexpr int kGT = 64;   // threads per block
+constexpr int kNegInf = INT32_MIN / 2;   // GlobalAligner.swift:52
+
+struct GlobalArgs {
+    DevScoring sc;
+    const uint8_t *bases;
+    const uint8_t *pac;
+    const swb_global_task *tasks;
+    swb_global_result *res;
+    uint32_t *cigar;
+    const unsigned long long *cigar_off;   // per task
+    unsigned long long *cells;
+    size_t n;
+};
+
+struct Scratch {
+    int *h, *e;
+    uint8_t *q, *t, *z;
+    size_t nslots, slot;
+    int qmax, tmax;
+    __device__ __forceinline__ int &H(int j) const { return h[(size_t)j * nslots + slot]; }
+    __device__ __forceinline__ int &E(int j) const { return e[(size_t)j * nslots + slot]; }
+    __device__ __forceinline__ uint8_t Q(int j) const { return q[(size_t)j * nslots + slot]; }
+    __device__ __forceinline__ uint8_t T(int i) const { return t[(size_t)i * nslots + slot]; }
+    __device__ __forceinline__ uint8_t &Z(int i, int col) const {
+        return z[((size_t)i * qmax + col) * nslots + slot];
+    }
+};
+
+// One DP attempt (GlobalAligner.swift:26-144); returns h[qlen].
+__device__ int global_dp(const DevScoring &sc, const Scratch &s, int qlen, int tlen, int w,
+                         int nCol, unsigned long long &cells) {
+    const int oDel = sc.o_del, eDel = sc.e_del, oIns = sc.o_ins, eIns = sc.e_ins;
+    const int oeDel = oDel + eDel, oeIns = oIns + eIns;
+    for (int j = 0; j <= qlen; ++j) {                                       // :75-76
+        s.H(j) = kNegInf;
+        s.E(j) = kNegInf;
+    }
+    s.H(0) = 0;                                                             // :80-84
+    const int initEnd = imin(w, qlen);
+    for (int j = 1; j <= initEnd; ++j) s.H(j) = 0 - (oIns + eIns * j);
+    for (int i = 0; i < tlen; ++i) {                                        // :89-142
+        const int beg = imax(0, i - w);
+        const int end = (int)min((long long)qlen, (long long)i + w + 1);
+        const RowTable rt = row_table(sc, s.T(i));
+        int f = kNegInf;
+        int hDiag = s.H(beg);
+        s.H(beg) = beg == 0 ? 0 - (oeDel + eDel * i) : kNegInf;
+        if (end > beg) cells += (unsigned long long)(end - beg);
+        int hLeft = s.H(beg);   // h[j] for the first column of the row
+        for (int j = beg; j < end; ++j) {
+            const int j1 = j + 1;
+            int hCur = hDiag + row_score(rt, s.Q(j));
+            hDiag = s.H(j1);
+            const int eOpen = hDiag - oeDel;
+            const int eExtend = s.E(j1) - eDel;
+            const uint32_t eFlag = eOpen > eExtend ? 0u : 1u;
+            const int eVal = eOpen > eExtend ? eOpen : eExtend;
+            s.E(j1) = eVal;
+            const int fOpen = hLeft - oeIns;
+            const int fExtend = f - eIns;
+            const uint32_t fFlag = fOpen > fExtend ? 0u : 2u;
+            const int fVal = fOpen > fExtend ? fOpen : fExtend;
+            f = fVal;
+            const uint32_t fromE = eVal > hCur ? 4u : 0u;
+            hCur = eVal > hCur ? eVal : hCur;
+            const uint32_t fromF = fVal > hCur ? 8u : 0u;
+            hCur = fVal > hCur ? fVal : hCur;
+            s.H(j1) = hCur;
+            hLeft = hCur;
+            s.Z(i, j - beg) = (uint8_t)(eFlag | fFlag | fromE | fromF);
+        }
+    }
+    (void)nCol;
+    return s.H(qlen);                                                       // :144
+}
+
+// Run-length CIGAR writer in traceback (reverse) order.
+struct CigarOut {
+    uint32_t *p;
+    int n = 0;
+    uint32_t op = 0xFFFFFFFFu, len = 0;
+    __device__ __forceinline__ void append(uint32_t o) {
+        if (o == op) {
+            ++len;
+        } else {
+            if (len) p[n++] = (len << 4) | op;
+            op = o;
+            len = 1;
+        }
+    }
+    __device__ __forceinline__ void finish() {
+        if (len) p[n++] = (len << 4) | op;
+        for (int a = 0, b = n - 1; a < b; ++a, --b) {                       // builder.reverse()
+            const uint32_t x = p[a];
+            p[a] = p[b];
+            p[b] = x;
+        }
+    }
+};
+
+// Traceback (GlobalAligner.swift:160-232).
+__device__ int global_traceback(const Scratch &s, int qlen, int tlen, int w, int nCol, uint32_t *out) {
+    CigarOut c{out};
+    int i = tlen - 1, j = qlen - 1, state = 0;
+    while (i >= 0 || j >= 0) {
+        if (i < 0) { c.append(1u); --j; continue; }
+        if (j < 0) { c.append(2u); --i; continue; }
+        const int beg = imax(0, i - w);
+        const int col = j - beg;
+        if (!(col >= 0 && col < nCol)) break;
+        const uint32_t d = s.Z(i, col);
+        if (state == 0) {
+            const uint32_t hDir = (d >> 2) & 3u;
+            if (hDir == 0) { c.append(0u); --i; --j; }
+            else if (hDir == 1) state = 1;
+            else state = 2;
+        } else if (state == 1) {
+            c.append(2u);
+            if ((d & 1u) == 0) state = 0;
+            --i;
+        } else {
+            c.append(1u);
+            if ((d & 2u) == 0) state = 0;
+            --j;
+        }
+    }
+    c.finish();
+    return c.n;
+}
+
+__global__ void __launch_bounds__(kGT) global_kernel(GlobalArgs a, Scratch base) {
+    Scratch s = base;
+    s.slot = blockIdx.x * (size_t)kGT + threadIdx.x;
+    unsigned long long cells = 0;
+    const size_t iters = (a.n + s.nslots - 1) / s.nslots;
+    for (size_t it = 0; it < iters; ++it) {
+        const size_t k = it * s.nslots + s.slot;
+        if (k >= a.n) continue;
+        const swb_global_task tk = a.tasks[k];
+        swb_global_result r{0, 0, tk.w, 1, a.cigar_off[k]};
+        const int qlen = tk.qlen, tlen = tk.tlen;
+        if (qlen > 0 && tlen > 0) {                                          // :29-31
+            for (int j = 0; j < qlen; ++j) s.q[(size_t)j * s.nslots + s.slot] =
+                (uint8_t)span_base(a.bases, a.pac, tk.q_off, j, qlen, tk.flags, false);
+            for (int i = 0; i < tlen; ++i) s.t[(size_t)i * s.nslots + s.slot] =
+                (uint8_t)span_base(a.bases, a.pac, tk.t_off, i, tlen, tk.flags, true);
+            int w0 = tk.w;
+            int w = imax(w0, abs(qlen - tlen));                               // :47
+            int nCol = (int)min((long long)qlen, 2ll * w + 1);               // :48
+            int score = global_dp(a.sc, s, qlen, tlen, w, nCol, cells);
+            if (tk.flags & SWB_GLB_RETRY) {                                  // CIGARGenerator.swift:88-96
+                int retries = 0;
+                while (score < tk.true_score && retries < 3) {
+                    w0 *= 2;
+                    ++retries;
+                    r.attempts++;
+                    w = imax(w0, abs(qlen - tlen));
+                    nCol = (int)min((long long)qlen, 2ll * w + 1);
+                    score = global_dp(a.sc, s, qlen, tlen, w, nCol, cells);
+                }
+            }
+            r.score = score;
+            r.w_used = w0;
+            r.n_cigar = global_traceback(s, qlen, tlen, w, nCol, a.cigar + r.cigar_off);
+        }
+        a.res[k] = r;
+    }
+    for (int o = 16; o > 0; o >>= 1) cells += __shfl_down_sync(0xFFFFFFFFu, cells, o);
+    if ((threadIdx.x & 31) == 0 && cells) atomicAdd(a.cells, cells);
+}
+
+__global__ void cigar_offsets_kernel(const swb_global_task *__restrict__ tasks, size_t n,
+                                     unsigned long long *__restrict__ lens) {
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i < n) lens[i] = (unsigned long long)max(tasks[i].qlen, 0) + (unsigned long long)max(tasks[i].tlen, 0);
+}
+
+}  // namespace
+}  // namespace swb
+
+#include <cub/device/device_scan.cuh>
+
+namespace swb {
+
+int launch_global(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
+                  const swb_global_task *d_tasks, size_t n, swb_global_result *d_res,
+                  uint32_t *d_cigar, unsigned long long *d_cells, cudaStream_t st, int max_q, int max_t) {
+    if (n == 0) return SWB_OK;
+    int rc;
+    // Per-task CIGAR windows: exclusive prefix sum of (qlen + tlen).
+    if ((rc = ensure_dev(ctx, ctx->d_keys, n * 8)) || (rc = ensure_dev(ctx, ctx->d_keys2, n * 8))) return rc;
+    unsigned long long *lens = (unsigned long long *)ctx->d_keys.p, *offs = (unsigned long long *)ctx->d_keys2.p;
+    cigar_offsets_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_tasks, n, lens);
+    ctx->launches++;
+    SWB_CUDA(cudaGetLastError());
+    size_t tmp = 0;
+    SWB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, lens, offs, (int)n, st));
+    if ((rc = ensure_dev(ctx, ctx->d_sort_tmp, tmp))) return rc;
+    SWB_CUDA(cub::DeviceScan::ExclusiveSum(ctx->d_sort_tmp.p, tmp, lens, offs, (int)n, st));
+
+    const int qmax = imax(max_q, 1), tmax = imax(max_t, 1);
+    // Slots: as many as fit a quarter of the remaining budget, capped at
+    // 8 resident blocks per SM.
+    const size_t per_slot = (size_t)(qmax + 1) * 8 + (size_t)qmax + (size_t)tmax + (size_t)tmax * qmax;
+    size_t nslots = (size_t)ctx->sm_count * 8 * kGT;
+    const size_t avail = ctx->budget > ctx->allocated ? (ctx->budget - ctx->allocated) / 2 : 0;
+    while (nslots > kGT && nslots * per_slot > avail) nslots /= 2;
+    nslots = (nslots / kGT) * kGT;
+    if (nslots == 0 || nslots * per_slot > avail)
+        return set_error(SWB_ERR_OOM, "global alignment scratch does not fit the memory budget");
+    const size_t bytes = nslots * per_slot + 1024;
+    if ((rc = ensure_dev(ctx, ctx->d_scratch, bytes))) return rc;
+    char *p = (char *)ctx->d_scratch.p;
+    Scratch s;
+    s.nslots = nslots;
+    s.slot = 0;
+    s.qmax = qmax;
+    s.tmax = tmax;
+    s.h = (int *)p;
+    p += (size_t)(qmax + 1) * nslots * 4;
+    s.e = (int *)p;
+    p += (size_t)(qmax + 1) * nslots * 4;
+    s.q = (uint8_t *)p;
+    p += (size_t)qmax * nslots;
+    s.t = (uint8_t *)p;
+    p += (size_t)tmax * nslots;
+    s.z = (uint8_t *)p;
+    GlobalArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_res, d_cigar, offs, d_cells, n};
+    const size_t grid = std::min(nslots / kGT, (n + kGT - 1) / kGT);
+    s.nslots = grid * kGT;   // fewer tasks than slots: pack the layout tighter
+    // Re-derive pointers for the tighter layout so strides match nslots.
+    p = (char *)ctx->d_scratch.p;
+    s.h = (int *)p;
+    p += (size_t)(qmax + 1) * s.nslots * 4;
+    s.e = (int *)p;
+    p += (size_t)(qmax + 1) * s.nslots * 4;
+    s.q = (uint8_t *)p;
+    p += (size_t)qmax * s.nslots;
+    s.t = (uint8_t *)p;
+    p += (size_t)tmax * s.nslots;
+    s.z = (uint8_t *)p;
+    global_kernel<<<(unsigned)grid, kGT, 0, st>>>(a, s);
+    ctx->launches++;
+    SWB_CUDA(cudaGetLastError());
+    return SWB_OK;
+}
+
+}  // namespace swb

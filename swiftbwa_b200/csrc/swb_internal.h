@@ -1,0 +1,113 @@
+// swb_internal.h -- declarations shared by the CUDA translation units of
+// libswb_cuda.so.  Not part of the public C ABI (include/swb_cuda.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/swb_cuda.h"
+
+namespace swb {
+
+// -------------------------------------------------------------- limits
+// Queries up to this length run in the shared-memory extension kernels;
+// longer ones (and scores that do not fit int16) use the global-scratch
+// int32 kernel.
+constexpr int kExtSmemMaxQ = 256;
+// Hard cap on any query or target length (the reference's extension target
+// window is capped at 10000 bases, ExtensionAligner.swift:214,277).
+constexpr int kMaxLen = 65535;
+
+// Device-side copy of swb_scoring plus derived constants.
+struct DevScoring {
+    int a, b, o_ins, e_ins, o_del, e_del, zdrop, pen_clip5, pen_clip3, band_width, min_seed_len;
+    int max_mat;        // max over the 5x5 matrix, starting from 0 (BandedSWScalar.swift:54-58)
+};
+
+inline DevScoring make_dev_scoring(const swb_scoring &s) {
+    DevScoring d{s.a, s.b, s.o_ins, s.e_ins, s.o_del, s.e_del, s.zdrop, s.pen_clip5, s.pen_clip3,
+                 s.band_width, s.min_seed_len, 0};
+    int m = 0;
+    // scoringMatrix(): a on the diagonal, -b off it, -1 for N (ScoringParameters.swift:65-73)
+    int vals[3] = {(int)(int8_t)s.a, (int)(int8_t)(-s.b), -1};
+    for (int v : vals) m = v > m ? v : m;
+    d.max_mat = m;
+    return d;
+}
+
+// ------------------------------------------------------------ a device arena
+// Grow-only device buffer owned by a context, counted against its budget.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+struct HostBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+}  // namespace swb
+
+// ------------------------------------------------------------------ context
+struct swb_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    size_t budget = 0;       // cap on bytes the context allocates on the device
+    size_t allocated = 0;    // bytes currently allocated
+    std::mutex mu;
+    // resident 2-bit reference (.pac layout)
+    uint8_t *d_pac = nullptr;
+    uint64_t ref_bases = 0;
+    size_t pac_bytes = 0;
+    // named scratch buffers (grow-only)
+    swb::DevBuf d_bases, d_tasks, d_out, d_keys, d_keys2, d_idx, d_idx2, d_sort_tmp, d_misc,
+        d_scratch, d_cigar, d_aux;
+    swb::HostBuf h_in, h_out;
+    unsigned long long launches = 0;
+    double last_ms = 0.0;
+    unsigned long long last_cells = 0;
+};
+
+namespace swb {
+
+// Error plumbing (thread-local message, set by every failing call).
+int set_error(int code, const std::string &msg);
+int check_cuda(cudaError_t e, const char *what);
+#define SWB_CUDA(call)                                               \
+    do {                                                             \
+        cudaError_t _e = (call);                                     \
+        if (_e != cudaSuccess) return ::swb::check_cuda(_e, #call);  \
+    } while (0)
+
+// Grow-only allocation against the context budget.
+int ensure_dev(swb_ctx *ctx, DevBuf &b, size_t bytes);
+int ensure_host(swb_ctx *ctx, HostBuf &b, size_t bytes);
+
+// -------------------------------------------------------- kernel launchers
+// All enqueue on `stream` and return SWB_OK or an error status.  `cells`
+// is a device counter (unsigned long long) the kernels add DP cells to.
+
+// Extension (kernel 1).  d_tasks/d_out are device arrays of n tasks/results.
+int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
+               const swb_ext_task *d_tasks, size_t n, swb_ext_result *d_out,
+               unsigned long long *d_cells, cudaStream_t stream, int max_q_hint);
+
+// Banded global + traceback (kernel 2).
+int launch_global(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
+                  const swb_global_task *d_tasks, size_t n, swb_global_result *d_res,
+                  uint32_t *d_cigar, unsigned long long *d_cells, cudaStream_t stream,
+                  int max_q, int max_t);
+
+// Local SW for mate rescue (kernel 3).
+int launch_local(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
+                 const swb_local_task *d_tasks, size_t n, swb_local_result *d_out,
+                 unsigned long long *d_cells, cudaStream_t stream, int max_q, int max_t);
+
+}  // namespace swb

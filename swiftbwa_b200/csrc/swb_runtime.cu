@@ -1,0 +1,448 @@
+// swb_runtime.cu -- context, device memory, staging and the C ABI of
+// libswb_cuda.so (include/swb_cuda.h).
+//
+// Synchronous batch calls: host arrays are packed into one pinned staging
+// buffer, copied to the device with a single cudaMemcpyAsync, processed on
+// the context's stream, and the results come back with one copy.  Device
+// buffers and pinned staging are grow-only and reused across calls; the
+// context's budget caps what it may hold on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "swb_internal.h"
+
+namespace swb {
+
+int ext_big_max_q(const swb_ext_task *tasks, size_t n, int max_mat);
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int check_cuda(cudaError_t e, const char *what) {
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        return set_error(SWB_ERR_OOM, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+    return set_error(SWB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int ensure_dev(swb_ctx *ctx, DevBuf &b, size_t bytes) {
+    if (bytes <= b.cap) return SWB_OK;
+    size_t want = std::max(bytes, b.cap + b.cap / 2);
+    want = (want + 4095) & ~(size_t)4095;
+    const size_t after = ctx->allocated - b.cap + want;
+    if (after > ctx->budget) {
+        want = (bytes + 4095) & ~(size_t)4095;
+        if (ctx->allocated - b.cap + want > ctx->budget)
+            return set_error(SWB_ERR_OOM, "device memory budget exceeded (" + std::to_string(ctx->allocated - b.cap + want) +
+                                              " > " + std::to_string(ctx->budget) + " bytes)");
+    }
+    if (b.p) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(b.p);
+        ctx->allocated -= b.cap;
+        b.p = nullptr;
+        b.cap = 0;
+    }
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        return check_cuda(e, "cudaMalloc");
+    }
+    b.cap = want;
+    ctx->allocated += want;
+    return SWB_OK;
+}
+
+int ensure_host(swb_ctx *ctx, HostBuf &b, size_t bytes) {
+    (void)ctx;
+    if (bytes <= b.cap) return SWB_OK;
+    size_t want = std::max(bytes, b.cap + b.cap / 2);
+    want = (want + 4095) & ~(size_t)4095;
+    if (b.p) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFreeHost(b.p);
+        b.p = nullptr;
+        b.cap = 0;
+    }
+    cudaError_t e = cudaMallocHost(&b.p, want);
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        return check_cuda(e, "cudaMallocHost");
+    }
+    b.cap = want;
+    return SWB_OK;
+}
+
+static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static void free_buf(swb_ctx *ctx, DevBuf &b) {
+    if (b.p) cudaFree(b.p);
+    ctx->allocated -= b.cap;
+    b.p = nullptr;
+    b.cap = 0;
+}
+
+static int validate_scoring(const swb_scoring *sc) {
+    if (!sc) return set_error(SWB_ERR_INVALID_ARG, "scoring is NULL");
+    if (sc->e_ins <= 0 || sc->e_del <= 0 || sc->o_ins < 0 || sc->o_del < 0 || sc->a < 0 || sc->b < 0 ||
+        sc->a > 127 || sc->b > 128)
+        return set_error(SWB_ERR_INVALID_ARG,
+                         "scoring: need e_ins, e_del > 0, o_* >= 0 and 0 <= a <= 127, 0 <= b <= 128");
+    return SWB_OK;
+}
+
+// Checks spans against the bases buffer / reference and lengths against the caps.
+template <class Task>
+static int validate_spans(const swb_ctx *ctx, const Task *tasks, size_t n, size_t n_bases,
+                          int *max_q, int *max_t) {
+    int mq = 0, mt = 0;
+    for (size_t i = 0; i < n; ++i) {
+        const Task &t = tasks[i];
+        if (t.qlen < 0 || t.tlen < 0) return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": negative length");
+        if (t.qlen > kMaxLen || t.tlen > kMaxLen)
+            return set_error(SWB_ERR_TOO_LARGE, "task " + std::to_string(i) + ": length above 65535");
+        if (t.qlen > 0 && (t.q_off > n_bases || t.q_off + (uint64_t)t.qlen > n_bases))
+            return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": query span outside bases");
+        if (t.tlen > 0) {
+            if (t.flags & SWB_T_FROM_REF) {
+                if (!ctx->d_pac) return set_error(SWB_ERR_NO_REFERENCE, "task reads the reference but none is uploaded");
+                if (t.t_off > ctx->ref_bases || t.t_off + (uint64_t)t.tlen > ctx->ref_bases)
+                    return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": target span outside reference");
+            } else if (t.t_off > n_bases || t.t_off + (uint64_t)t.tlen > n_bases) {
+                return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": target span outside bases");
+            }
+        }
+        mq = std::max(mq, t.qlen);
+        mt = std::max(mt, t.tlen);
+    }
+    if (max_q) *max_q = mq;
+    if (max_t) *max_t = mt;
+    return SWB_OK;
+}
+
+// Stages `parts` into one pinned buffer and copies it to d_in; returns
+// device pointers to each part.
+struct Part {
+    const void *src;
+    size_t bytes;
+    void **dev;
+};
+
+static int stage_in(swb_ctx *ctx, std::initializer_list<Part> parts) {
+    size_t total = 0;
+    for (const Part &p : parts) total += align256(p.bytes);
+    int rc;
+    if ((rc = ensure_host(ctx, ctx->h_in, total + 256)) || (rc = ensure_dev(ctx, ctx->d_bases, total + 256))) return rc;
+    size_t off = 0;
+    for (const Part &p : parts) {
+        if (p.bytes) std::memcpy((char *)ctx->h_in.p + off, p.src, p.bytes);
+        *p.dev = (char *)ctx->d_bases.p + off;
+        off += align256(p.bytes);
+    }
+    SWB_CUDA(cudaMemcpyAsync(ctx->d_bases.p, ctx->h_in.p, std::max<size_t>(off, 1), cudaMemcpyHostToDevice, ctx->stream));
+    return SWB_OK;
+}
+
+struct Timer {
+    swb_ctx *ctx;
+    unsigned long long *d_cells;
+    int begin() {
+        int rc;
+        if ((rc = ensure_dev(ctx, ctx->d_aux, 64))) return rc;
+        d_cells = (unsigned long long *)ctx->d_aux.p;
+        SWB_CUDA(cudaMemsetAsync(d_cells, 0, sizeof(unsigned long long), ctx->stream));
+        SWB_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
+        return SWB_OK;
+    }
+    int end() {
+        SWB_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
+        return SWB_OK;
+    }
+    // After the stream synchronised.
+    void collect() {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) ctx->last_ms = ms;
+        unsigned long long c = 0;
+        if (cudaMemcpy(&c, d_cells, sizeof(c), cudaMemcpyDeviceToHost) == cudaSuccess) ctx->last_cells = c;
+    }
+};
+
+}  // namespace swb
+
+using namespace swb;
+
+extern "C" {
+
+void swb_scoring_default(swb_scoring *s) {
+    if (!s) return;
+    *s = swb_scoring{1, 4, 6, 1, 6, 1, 100, 5, 5, 100, 19};
+}
+
+const char *swb_strerror(int status) {
+    switch (status) {
+    case SWB_OK: return "ok";
+    case SWB_ERR_INVALID_ARG: return "invalid argument";
+    case SWB_ERR_NO_DEVICE: return "no usable CUDA device";
+    case SWB_ERR_CUDA: return "CUDA runtime error";
+    case SWB_ERR_OOM: return "out of device memory or over budget";
+    case SWB_ERR_TOO_LARGE: return "task exceeds the supported size";
+    case SWB_ERR_NO_REFERENCE: return "no resident reference uploaded";
+    case SWB_ERR_TIMEOUT: return "device wait timed out";
+    case SWB_ERR_NOT_FOUND: return "unknown ticket";
+    case SWB_ERR_KERNEL: return "kernel reported an internal check failure";
+    default: return "unknown status";
+    }
+}
+
+const char *swb_last_error_message(void) { return g_last_error.c_str(); }
+
+int swb_init(int device, size_t mem_budget_bytes, swb_ctx **out) {
+    if (!out) return set_error(SWB_ERR_INVALID_ARG, "out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return set_error(SWB_ERR_NO_DEVICE, "no CUDA device visible");
+    }
+    if (device < 0 || device >= ndev) return set_error(SWB_ERR_INVALID_ARG, "device index out of range");
+    cudaDeviceProp prop;
+    SWB_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+        return set_error(SWB_ERR_NO_DEVICE, std::string("device ") + prop.name + " is not sm_100 (built for sm_100a)");
+    SWB_CUDA(cudaSetDevice(device));
+    swb_ctx *ctx = new swb_ctx();
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    ctx->budget = mem_budget_bytes ? mem_budget_bytes : free_b / 4 * 3;
+    cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_start);
+    if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_stop);
+    if (e != cudaSuccess) {
+        swb_destroy(ctx);
+        return check_cuda(e, "stream/event create");
+    }
+    *out = ctx;
+    return SWB_OK;
+}
+
+void swb_destroy(swb_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    DevBuf *bufs[] = {&ctx->d_bases, &ctx->d_tasks, &ctx->d_out, &ctx->d_keys, &ctx->d_keys2, &ctx->d_idx,
+                      &ctx->d_idx2, &ctx->d_sort_tmp, &ctx->d_misc, &ctx->d_scratch, &ctx->d_cigar, &ctx->d_aux};
+    for (DevBuf *b : bufs) free_buf(ctx, *b);
+    if (ctx->d_pac) cudaFree(ctx->d_pac);
+    if (ctx->h_in.p) cudaFreeHost(ctx->h_in.p);
+    if (ctx->h_out.p) cudaFreeHost(ctx->h_out.p);
+    if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
+    if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+int swb_upload_reference(swb_ctx *ctx, const uint8_t *pac, uint64_t n_bases) {
+    if (!ctx || (!pac && n_bases)) return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    SWB_CUDA(cudaSetDevice(ctx->device));
+    const size_t bytes = (size_t)((n_bases + 3) / 4);
+    if (ctx->d_pac) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->d_pac);
+        ctx->allocated -= ctx->pac_bytes;
+        ctx->d_pac = nullptr;
+        ctx->pac_bytes = 0;
+        ctx->ref_bases = 0;
+    }
+    if (n_bases == 0) return SWB_OK;
+    if (ctx->allocated + bytes + 16 > ctx->budget) return set_error(SWB_ERR_OOM, "reference exceeds the memory budget");
+    SWB_CUDA(cudaMalloc(&ctx->d_pac, bytes + 16));
+    ctx->pac_bytes = bytes + 16;
+    ctx->allocated += ctx->pac_bytes;
+    SWB_CUDA(cudaMemcpy(ctx->d_pac, pac, bytes, cudaMemcpyHostToDevice));
+    ctx->ref_bases = n_bases;
+    return SWB_OK;
+}
+
+int swb_ext_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, size_t n_bases,
+                  const swb_ext_task *tasks, size_t n_tasks, swb_ext_result *out) {
+    if (!ctx || (!tasks && n_tasks) || (!out && n_tasks) || (!bases && n_bases))
+        return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
+    int rc;
+    if ((rc = validate_scoring(sc))) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->last_ms = 0;
+    ctx->last_cells = 0;
+    if (n_tasks == 0) return SWB_OK;
+    if ((rc = validate_spans(ctx, tasks, n_tasks, n_bases, nullptr, nullptr))) return rc;
+    SWB_CUDA(cudaSetDevice(ctx->device));
+    const DevScoring dsc = make_dev_scoring(*sc);
+    const int big_q = ext_big_max_q(tasks, n_tasks, dsc.max_mat);
+    void *d_b = nullptr, *d_t = nullptr;
+    if ((rc = stage_in(ctx, {Part{bases, n_bases, &d_b}, Part{tasks, n_tasks * sizeof(swb_ext_task), &d_t}}))) return rc;
+    if ((rc = ensure_dev(ctx, ctx->d_out, n_tasks * sizeof(swb_ext_result)))) return rc;
+    Timer tm{ctx, nullptr};
+    if ((rc = tm.begin())) return rc;
+    if ((rc = launch_ext(ctx, dsc, (const uint8_t *)d_b, (const swb_ext_task *)d_t, n_tasks,
+                         (swb_ext_result *)ctx->d_out.p, tm.d_cells, ctx->stream, big_q)))
+        return rc;
+    if ((rc = tm.end())) return rc;
+    SWB_CUDA(cudaMemcpyAsync(out, ctx->d_out.p, n_tasks * sizeof(swb_ext_result), cudaMemcpyDeviceToHost, ctx->stream));
+    SWB_CUDA(cudaStreamSynchronize(ctx->stream));
+    tm.collect();
+    return SWB_OK;
+}
+
+int swb_ext_batch_device(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *d_bases,
+                         const swb_ext_task *d_tasks, size_t n_tasks, swb_ext_result *d_out,
+                         void *stream) {
+    if (!ctx || (!d_tasks && n_tasks) || (!d_out && n_tasks)) return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
+    int rc;
+    if ((rc = validate_scoring(sc))) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (n_tasks == 0) return SWB_OK;
+    SWB_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    if ((rc = ensure_dev(ctx, ctx->d_aux, 64))) return rc;
+    unsigned long long *d_cells = (unsigned long long *)ctx->d_aux.p;
+    SWB_CUDA(cudaMemsetAsync(d_cells, 0, sizeof(unsigned long long), s));
+    return launch_ext(ctx, make_dev_scoring(*sc), d_bases, d_tasks, n_tasks, d_out, d_cells, s, -1);
+}
+
+int swb_global_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, size_t n_bases,
+                     const swb_global_task *tasks, size_t n_tasks, swb_global_result *results,
+                     uint32_t *cigar_out, size_t cigar_cap) {
+    if (!ctx || (!tasks && n_tasks) || (!results && n_tasks) || (!bases && n_bases) || (!cigar_out && n_tasks))
+        return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
+    int rc;
+    if ((rc = validate_scoring(sc))) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->last_ms = 0;
+    ctx->last_cells = 0;
+    if (n_tasks == 0) return SWB_OK;
+    int max_q = 0, max_t = 0;
+    if ((rc = validate_spans(ctx, tasks, n_tasks, n_bases, &max_q, &max_t))) return rc;
+    size_t need = 0;
+    for (size_t i = 0; i < n_tasks; ++i) {
+        need += (size_t)tasks[i].qlen + (size_t)tasks[i].tlen;
+        const swb_global_task &t = tasks[i];
+        if (t.qlen > 0 && t.tlen > 0 && std::max(t.w, std::abs(t.qlen - t.tlen)) < 1)
+            return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": band width below 1 with equal lengths");
+    }
+    if (need > cigar_cap) return set_error(SWB_ERR_INVALID_ARG, "cigar_cap below sum of (qlen + tlen)");
+    SWB_CUDA(cudaSetDevice(ctx->device));
+    const DevScoring dsc = make_dev_scoring(*sc);
+    void *d_b = nullptr, *d_t = nullptr;
+    if ((rc = stage_in(ctx, {Part{bases, n_bases, &d_b}, Part{tasks, n_tasks * sizeof(swb_global_task), &d_t}}))) return rc;
+    if ((rc = ensure_dev(ctx, ctx->d_out, n_tasks * sizeof(swb_global_result)))) return rc;
+    if ((rc = ensure_dev(ctx, ctx->d_cigar, std::max<size_t>(need, 1) * sizeof(uint32_t)))) return rc;
+    Timer tm{ctx, nullptr};
+    if ((rc = tm.begin())) return rc;
+    if ((rc = launch_global(ctx, dsc, (const uint8_t *)d_b, (const swb_global_task *)d_t, n_tasks,
+                            (swb_global_result *)ctx->d_out.p, (uint32_t *)ctx->d_cigar.p, tm.d_cells,
+                            ctx->stream, max_q, max_t)))
+        return rc;
+    if ((rc = tm.end())) return rc;
+    SWB_CUDA(cudaMemcpyAsync(results, ctx->d_out.p, n_tasks * sizeof(swb_global_result), cudaMemcpyDeviceToHost, ctx->stream));
+    SWB_CUDA(cudaMemcpyAsync(cigar_out, ctx->d_cigar.p, std::max<size_t>(need, 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    SWB_CUDA(cudaStreamSynchronize(ctx->stream));
+    tm.collect();
+    return SWB_OK;
+}
+
+int swb_local_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, size_t n_bases,
+                    const swb_local_task *tasks, size_t n_tasks, swb_local_result *out) {
+    if (!ctx || (!tasks && n_tasks) || (!out && n_tasks) || (!bases && n_bases))
+        return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
+    int rc;
+    if ((rc = validate_scoring(sc))) return rc;
+    if (sc->o_ins + sc->e_ins > 255 || sc->e_ins > 255)
+        return set_error(SWB_ERR_INVALID_ARG, "local SW: gap penalties must fit in 8 bits (UInt8(gapOE))");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->last_ms = 0;
+    ctx->last_cells = 0;
+    if (n_tasks == 0) return SWB_OK;
+    int max_q = 0, max_t = 0;
+    if ((rc = validate_spans(ctx, tasks, n_tasks, n_bases, &max_q, &max_t))) return rc;
+    SWB_CUDA(cudaSetDevice(ctx->device));
+    const DevScoring dsc = make_dev_scoring(*sc);
+    void *d_b = nullptr, *d_t = nullptr;
+    if ((rc = stage_in(ctx, {Part{bases, n_bases, &d_b}, Part{tasks, n_tasks * sizeof(swb_local_task), &d_t}}))) return rc;
+    if ((rc = ensure_dev(ctx, ctx->d_out, n_tasks * sizeof(swb_local_result)))) return rc;
+    Timer tm{ctx, nullptr};
+    if ((rc = tm.begin())) return rc;
+    if ((rc = launch_local(ctx, dsc, (const uint8_t *)d_b, (const swb_local_task *)d_t, n_tasks,
+                           (swb_local_result *)ctx->d_out.p, tm.d_cells, ctx->stream, max_q, max_t)))
+        return rc;
+    if ((rc = tm.end())) return rc;
+    SWB_CUDA(cudaMemcpyAsync(out, ctx->d_out.p, n_tasks * sizeof(swb_local_result), cudaMemcpyDeviceToHost, ctx->stream));
+    SWB_CUDA(cudaStreamSynchronize(ctx->stream));
+    tm.collect();
+    return SWB_OK;
+}
+
+int swb_banded_sw_align(swb_ctx *ctx, const uint8_t *query, int32_t qlen, const uint8_t *target,
+                        int32_t tlen, const swb_scoring *sc, int32_t w, int32_t h0, int32_t end_bonus,
+                        swb_ext_result *out) {
+    if (!out || qlen < 0 || tlen < 0 || (!query && qlen) || (!target && tlen))
+        return set_error(SWB_ERR_INVALID_ARG, "bad argument");
+    std::string buf((size_t)qlen + (size_t)tlen + 1, '\0');
+    if (qlen) std::memcpy(&buf[0], query, (size_t)qlen);
+    if (tlen) std::memcpy(&buf[(size_t)qlen], target, (size_t)tlen);
+    swb_ext_task t{0, (uint64_t)qlen, qlen, tlen, w, h0, end_bonus, 0u};
+    return swb_ext_batch(ctx, sc, (const uint8_t *)buf.data(), buf.size(), &t, 1, out);
+}
+
+int swb_global_align(swb_ctx *ctx, const uint8_t *query, int32_t qlen, const uint8_t *target, int32_t tlen,
+                     const swb_scoring *sc, int32_t w, int32_t *score, uint32_t *cigar, int32_t *n_cigar) {
+    if (!score || !n_cigar || qlen < 0 || tlen < 0 || (!query && qlen) || (!target && tlen))
+        return set_error(SWB_ERR_INVALID_ARG, "bad argument");
+    if (*n_cigar < qlen + tlen || (!cigar && *n_cigar))
+        return set_error(SWB_ERR_INVALID_ARG, "cigar capacity below qlen + tlen");
+    std::string buf((size_t)qlen + (size_t)tlen + 1, '\0');
+    if (qlen) std::memcpy(&buf[0], query, (size_t)qlen);
+    if (tlen) std::memcpy(&buf[(size_t)qlen], target, (size_t)tlen);
+    swb_global_task t{0, (uint64_t)qlen, qlen, tlen, w, 0, 0u, 0};
+    swb_global_result r{};
+    std::vector<uint32_t> tmp((size_t)qlen + (size_t)tlen + 1);
+    int rc = swb_global_batch(ctx, sc, (const uint8_t *)buf.data(), buf.size(), &t, 1, &r, tmp.data(), tmp.size());
+    if (rc) return rc;
+    *score = r.score;
+    std::copy(tmp.begin(), tmp.begin() + r.n_cigar, cigar);
+    *n_cigar = r.n_cigar;
+    return SWB_OK;
+}
+
+int swb_local_align(swb_ctx *ctx, const uint8_t *query, int32_t qlen, const uint8_t *target, int32_t tlen,
+                    const swb_scoring *sc, int32_t min_sub_score, swb_local_result *out) {
+    if (!out || qlen < 0 || tlen < 0 || (!query && qlen) || (!target && tlen))
+        return set_error(SWB_ERR_INVALID_ARG, "bad argument");
+    std::string buf((size_t)qlen + (size_t)tlen + 1, '\0');
+    if (qlen) std::memcpy(&buf[0], query, (size_t)qlen);
+    if (tlen) std::memcpy(&buf[(size_t)qlen], target, (size_t)tlen);
+    swb_local_task t{0, (uint64_t)qlen, qlen, tlen, min_sub_score, 0u};
+    return swb_local_batch(ctx, sc, (const uint8_t *)buf.data(), buf.size(), &t, 1, out);
+}
+
+uint64_t swb_kernel_launches(const swb_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int swb_last_batch_stats(const swb_ctx *ctx, double *kernel_ms, uint64_t *cells) {
+    if (!ctx) return set_error(SWB_ERR_INVALID_ARG, "ctx is NULL");
+    if (kernel_ms) *kernel_ms = ctx->last_ms;
+    if (cells) *cells = ctx->last_cells;
+    return SWB_OK;
+}
+
+}  // extern "C"

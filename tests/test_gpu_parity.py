@@ -1,0 +1,128 @@
+"""CUDA kernels vs the oracle, through the C ABI: known answers, the
+reference's GPU-vs-CPU differential shapes, and seeded fuzz sets.  Every
+field must match bit for bit."""
+import numpy as np
+import pytest
+
+import gen
+import known
+from swiftbwa_b200.abi import Scoring
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def engine():
+    from swiftbwa_b200.alignment import Engine
+    from swiftbwa_b200.build import build
+    build()
+    e = Engine(0)
+    yield e
+    e.close()
+
+
+class GpuBackend:
+    def __init__(self, e, o):
+        self.e, self.o = e, o
+
+    def ext(self, q, t, sc, w, h0, eb):
+        return self.e.banded_sw_align(q, t, sc, w, h0, eb).as_tuple()
+
+    def global_(self, q, t, sc, w):
+        r = self.e.global_align(q, t, sc, w)
+        return r.score, list(r.cigar)
+
+    def compute_nm(self, cigar, q, t):
+        return self.o.compute_nm(cigar, q, t)
+
+    def cigar(self, q, r, qb, qe, rl, rev, ts, iw, sc, pos):
+        return self.e.cigar_generate(q, r, qb, qe, rl, rev, ts, iw, sc, pos)
+
+    def local(self, q, t, sc, ms):
+        r = self.e.local_align(q, t, sc, ms)
+        return None if r is None else r.as_tuple()
+
+
+CASES = known.load()["known_answers"]
+
+
+@pytest.mark.parametrize("case", [c for c in CASES if c["fn"] in ("ext", "global", "global_w_pair", "local")],
+                         ids=lambda c: c["name"])
+def test_known_answer_on_gpu(case, engine, oracle_mod):
+    fails = known.evaluate(case, GpuBackend(engine, oracle_mod))
+    assert fails is not None and not fails, "\n".join(fails or [])
+
+
+def test_differential_shapes(engine, oracle_mod):
+    for d in known.load()["differential_shapes"]:
+        sc = Scoring.default(**d["scoring"])
+        if d["kind"] == "ext":
+            g = engine.banded_sw_align(d["q"], d["t"], sc, d["w"], d["h0"]).as_tuple()
+            o = oracle_mod.banded_sw_scalar(d["q"], d["t"], sc, d["w"], d["h0"])[0]
+        else:
+            r = engine.local_align(d["q"], d["t"], sc, 0)
+            g = None if r is None else r.as_tuple()
+            o = oracle_mod.local_align(d["q"], d["t"], sc, 0)[0]
+        assert g == o, (d["source"], g, o)
+
+
+SCORINGS = [
+    dict(),
+    dict(zdrop=0),
+    dict(zdrop=10),
+    dict(a=2, b=3, o_ins=5, e_ins=2, o_del=4, e_del=3),
+    dict(a=1, b=1, o_ins=1, e_ins=1, o_del=1, e_del=1, zdrop=5),
+    dict(a=8),
+]
+
+
+def _cmp_struct(got, exp, fields):
+    bad = np.nonzero(np.any(np.stack([got[f] != exp[f] for f in fields]), axis=0))[0]
+    return bad
+
+
+@pytest.mark.parametrize("si", range(len(SCORINGS)))
+def test_ext_fuzz(engine, oracle_mod, si):
+    sc = Scoring.default(**SCORINGS[si])
+    d = gen.ext_tasks(1000 + si, 3000, qmax=300, ref_len=5000)
+    engine.upload_reference(d["pac"], d["ref_bases"])
+    got = engine.ext_batch(sc, d["bases"], d["tasks"])
+    exp, cells = oracle_mod.ext_batch(sc, d["bases"], d["tasks"], pac=d["pac"], ref_bases=d["ref_bases"],
+                                      n_threads=8)
+    bad = _cmp_struct(got, exp, got.dtype.names)
+    assert bad.size == 0, f"{bad.size} mismatches, first {bad[:5]}: {got[bad[:3]]} vs {exp[bad[:3]]} tasks {d['tasks'][bad[:3]]}"
+    ms, gcells = engine.last_batch_stats()
+    assert gcells == cells
+
+
+def test_ext_fuzz_int32_path(engine, oracle_mod):
+    sc = Scoring.default()
+    d = gen.ext_tasks(77, 500, qmax=120, big_scores=True)
+    got = engine.ext_batch(sc, d["bases"], d["tasks"])
+    exp, _ = oracle_mod.ext_batch(sc, d["bases"], d["tasks"], n_threads=8)
+    bad = _cmp_struct(got, exp, got.dtype.names)
+    assert bad.size == 0, f"{bad.size} mismatches: {got[bad[:3]]} vs {exp[bad[:3]]}"
+
+
+@pytest.mark.parametrize("si", [0, 3, 4])
+def test_global_fuzz(engine, oracle_mod, si):
+    sc = Scoring.default(**SCORINGS[si])
+    d = gen.global_tasks(2000 + si, 1500)
+    res, cig = engine.global_batch(sc, d["bases"], d["tasks"])
+    eres, ecig, _ = oracle_mod.global_batch(sc, d["bases"], d["tasks"], n_threads=8)
+    for k in range(len(res)):
+        assert res["score"][k] == eres["score"][k], k
+        assert res["n_cigar"][k] == eres["n_cigar"][k], k
+        o, n = int(res["cigar_off"][k]), int(res["n_cigar"][k])
+        eo = int(eres["cigar_off"][k])
+        assert np.array_equal(cig[o:o + n], ecig[eo:eo + n]), k
+
+
+@pytest.mark.parametrize("si", [0, 3, 4, 5])
+def test_local_fuzz(engine, oracle_mod, si):
+    sc = Scoring.default(**SCORINGS[si])
+    d = gen.local_tasks(3000 + si, 1200)
+    got = engine.local_batch(sc, d["bases"], d["tasks"])
+    exp, _ = oracle_mod.local_batch(sc, d["bases"], d["tasks"], n_threads=8)
+    bad = _cmp_struct(got, exp, got.dtype.names)
+    assert bad.size == 0, f"{bad.size} mismatches, first {bad[:5]}: {got[bad[:3]]} vs {exp[bad[:3]]} tasks {d['tasks'][bad[:3]]}"
