@@ -216,6 +216,23 @@ int swb_local_align(swb_ctx *ctx, const uint8_t *query, int32_t qlen,
                     swb_local_result *out);
 
 /* ------------------------------------------------------- library introspection */
+/* Per-kernel accounting.  With profiling on, every kernel launch is
+ * bracketed by CUDA events on its stream; swb_profile_read synchronises the
+ * context's streams and returns, per kernel name, the launches, summed
+ * device time and DP cells since the last swb_profile_reset. */
+typedef struct swb_kernel_stat {
+    char     name[40];
+    uint32_t launches;
+    double   total_ms;
+    uint64_t cells;
+} swb_kernel_stat;
+int swb_profile(swb_ctx *ctx, int enable);
+int swb_profile_reset(swb_ctx *ctx);
+int swb_profile_read(swb_ctx *ctx, swb_kernel_stat *stats, int cap, int *n_stats);
+/* Measured int32 add+max issue rate of the context's GPU (ops/s): the
+ * denominator of the kernels' integer-ALU roofline. */
+int swb_int_alu_peak(swb_ctx *ctx, double *ops_per_s);
+
 /* Kernel launches issued by this context so far (for launch accounting). */
 uint64_t swb_kernel_launches(const swb_ctx *ctx);
 /* Device time (ms, CUDA events on the context's stream) of the last

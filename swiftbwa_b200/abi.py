@@ -117,8 +117,14 @@ EXPORTED_SYMBOLS = (
     "swb_last_error_message", "swb_upload_reference", "swb_ext_batch",
     "swb_global_batch", "swb_local_batch", "swb_ext_batch_device",
     "swb_banded_sw_align", "swb_global_align", "swb_local_align",
-    "swb_kernel_launches", "swb_last_batch_stats",
+    "swb_kernel_launches", "swb_last_batch_stats", "swb_profile", "swb_profile_reset",
+    "swb_profile_read", "swb_int_alu_peak",
 )
+
+
+class KernelStat(C.Structure):
+    _fields_ = [("name", C.c_char * 40), ("launches", C.c_uint32), ("total_ms", C.c_double),
+                ("cells", C.c_uint64)]
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "libswb_cuda.so")
@@ -170,6 +176,14 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.swb_kernel_launches.restype = C.c_uint64
     lib.swb_last_batch_stats.argtypes = [vp, P(C.c_double), P(C.c_uint64)]
     lib.swb_last_batch_stats.restype = C.c_int
+    lib.swb_profile.argtypes = [vp, C.c_int]
+    lib.swb_profile.restype = C.c_int
+    lib.swb_profile_reset.argtypes = [vp]
+    lib.swb_profile_reset.restype = C.c_int
+    lib.swb_profile_read.argtypes = [vp, P(KernelStat), C.c_int, P(C.c_int)]
+    lib.swb_profile_read.restype = C.c_int
+    lib.swb_int_alu_peak.argtypes = [vp, P(C.c_double)]
+    lib.swb_int_alu_peak.restype = C.c_int
     return lib
 
 

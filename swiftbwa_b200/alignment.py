@@ -115,9 +115,12 @@ class Engine:
         _check(self.lib.swb_upload_reference(self.h, ptr(pac), n_bases), "swb_upload_reference")
 
     # ------------------------------------------------------------- batches
-    def ext_batch(self, sc: Scoring, bases: np.ndarray, tasks: np.ndarray) -> np.ndarray:
+    def ext_batch(self, sc: Scoring, bases: np.ndarray, tasks: np.ndarray,
+                  out: Optional[np.ndarray] = None) -> np.ndarray:
         assert tasks.dtype == EXT_TASK_DTYPE
-        out = np.zeros(len(tasks), EXT_RESULT_DTYPE)
+        if out is None:
+            out = np.zeros(len(tasks), EXT_RESULT_DTYPE)
+        assert out.dtype == EXT_RESULT_DTYPE and len(out) >= len(tasks)
         bases = np.ascontiguousarray(bases, dtype=np.uint8)
         _check(self.lib.swb_ext_batch(self.h, C.byref(sc), ptr(bases), bases.size,
                                       tasks.ctypes.data, len(tasks), out.ctypes.data),
@@ -151,6 +154,32 @@ class Engine:
 
     def kernel_launches(self) -> int:
         return int(self.lib.swb_kernel_launches(self.h))
+
+    # ------------------------------------------------------------ profiling
+    def profile(self, enable: bool = True):
+        _check(self.lib.swb_profile(self.h, int(enable)), "swb_profile")
+
+    def profile_reset(self):
+        _check(self.lib.swb_profile_reset(self.h), "swb_profile_reset")
+
+    def profile_read(self) -> dict:
+        """{kernel name: (launches, total_ms, cells)} since the last reset."""
+        cap = 64
+        arr = (abi.KernelStat * cap)()
+        n = C.c_int()
+        _check(self.lib.swb_profile_read(self.h, arr, cap, C.byref(n)), "swb_profile_read")
+        return {arr[k].name.decode(): (arr[k].launches, arr[k].total_ms, arr[k].cells)
+                for k in range(min(n.value, cap))}
+
+    def int_alu_peak(self) -> float:
+        v = C.c_double()
+        _check(self.lib.swb_int_alu_peak(self.h, C.byref(v)), "swb_int_alu_peak")
+        return v.value
+
+    def ext_batch_device(self, sc: Scoring, d_bases: int, d_tasks: int, n: int, d_out: int, stream: int = 0):
+        """swb_ext_batch_device on device pointers (HBM-resident inputs)."""
+        _check(self.lib.swb_ext_batch_device(self.h, C.byref(sc), C.c_void_p(d_bases), C.c_void_p(d_tasks), n,
+                                             C.c_void_p(d_out), C.c_void_p(stream)), "swb_ext_batch_device")
 
     # --------------------------------------------------- single-call forms
     def banded_sw_align(self, query, target, scoring: Scoring, w: int, h0: int,

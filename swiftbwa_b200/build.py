@@ -16,7 +16,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libswb_cuda.so")
-SOURCES = ["swb_runtime.cu", "swb_ext.cu", "swb_global.cu", "swb_local.cu"]
+SOURCES = ["swb_runtime.cu", "swb_ext.cu", "swb_global.cu", "swb_local.cu", "swb_probe.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -27,7 +27,24 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
+WORKLOAD_SRC = os.path.join(CSRC, "swb_workload.cpp")
+WORKLOAD_OUT = os.path.join(HERE, "libswb_workload.so")
+
+
+def build_workload() -> str:
+    """Host-only synthetic workload generator (g++)."""
+    deps = [WORKLOAD_SRC, os.path.join(HERE, "..", "include", "swb_cuda.h")]
+    if os.path.exists(WORKLOAD_OUT) and all(os.path.getmtime(d) <= os.path.getmtime(WORKLOAD_OUT) for d in deps):
+        return WORKLOAD_OUT
+    cxx = shutil.which("g++") or "g++"
+    subprocess.run([cxx, "-O3", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-shared", "-pthread",
+                    "-o", WORKLOAD_OUT + ".tmp", WORKLOAD_SRC], check=True)
+    os.replace(WORKLOAD_OUT + ".tmp", WORKLOAD_OUT)
+    return WORKLOAD_OUT
+
+
 def build(debug: bool = False, verbose: bool = False, ptxas_v: bool = False) -> str:
+    build_workload()
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     deps.append(os.path.join(HERE, "..", "include", "swb_cuda.h"))

@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(T) ext_smem_kernel(ExtArgs a, int bin) {
             a.out[ti] = r;
         }
     }
-    add_cells(a.cells, cells);
+    add_cells(a.cells + kCntExtBin0 + bin, cells);
 }
 
 __global__ void __launch_bounds__(kBigT) ext_global_kernel(ExtArgs a, int *h, int *e, uint8_t *q,
@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(kBigT) ext_global_kernel(ExtArgs a, int *h, in
             a.out[ti] = r;
         }
     }
-    add_cells(a.cells, cells);
+    add_cells(a.cells + kCntExtBin0 + kBigBin, cells);
 }
 
 template <int QMAX>
@@ -308,6 +308,8 @@ int launch_bin(swb_ctx *ctx, const ExtArgs &a, int bin, size_t n, cudaStream_t s
     const size_t need = (n + kSmemT - 1) / kSmemT;
     const size_t grid = std::min<size_t>(need, (size_t)ctx->sm_count * occ);
     if (grid == 0) return SWB_OK;
+    static const char *names[4] = {"ext_smem_q32", "ext_smem_q64", "ext_smem_q128", "ext_smem_q256"};
+    ProfScope ps(ctx, s, names[bin], kCntExtBin0 + bin);
     ext_smem_kernel<QMAX, kSmemT><<<(unsigned)grid, kSmemT, smem, s>>>(a, bin);
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
@@ -332,15 +334,24 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     int *big_max_q = (int *)((char *)ctx->d_misc.p + 64);
     SWB_CUDA(cudaMemsetAsync(big_max_q, 0, sizeof(int), s));
     const unsigned tb = 256;
-    ext_keys_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(d_tasks, n, sc.max_mat, keys, idx, big_max_q);
+    {
+        ProfScope ps(ctx, s, "ext_keys", -1);
+        ext_keys_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(d_tasks, n, sc.max_mat, keys, idx, big_max_q);
+    }
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
     size_t tmp_bytes = 0;
     SWB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys, keys2, idx, idx2, (int)n, 0, 32, s));
     if ((rc = ensure_dev(ctx, ctx->d_sort_tmp, tmp_bytes))) return rc;
-    SWB_CUDA(cub::DeviceRadixSort::SortPairs(ctx->d_sort_tmp.p, tmp_bytes, keys, keys2, idx, idx2,
-                                             (int)n, 0, 32, s));
-    bin_bounds_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(keys2, n, bin_start, kNumBins);
+    {
+        ProfScope ps(ctx, s, "cub_radix_sort", -1);
+        SWB_CUDA(cub::DeviceRadixSort::SortPairs(ctx->d_sort_tmp.p, tmp_bytes, keys, keys2, idx, idx2,
+                                                 (int)n, 0, 32, s));
+    }
+    {
+        ProfScope ps(ctx, s, "bin_bounds", -1);
+        bin_bounds_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(keys2, n, bin_start, kNumBins);
+    }
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
 
@@ -365,6 +376,7 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
         int *hbuf = (int *)ctx->d_scratch.p;
         int *ebuf = hbuf + cols * nslots;
         uint8_t *qbuf = (uint8_t *)(ebuf + cols * nslots);
+        ProfScope ps(ctx, s, "ext_global_i32", kCntExtBin0 + kBigBin);
         ext_global_kernel<<<(unsigned)(nslots / kBigT), kBigT, 0, s>>>(a, hbuf, ebuf, qbuf, nslots);
         ctx->launches++;
         SWB_CUDA(cudaGetLastError());

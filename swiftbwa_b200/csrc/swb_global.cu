@@ -243,7 +243,7 @@ int launch_global(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     s.t = (uint8_t *)p;
     p += (size_t)tmax * nslots;
     s.z = (uint8_t *)p;
-    GlobalArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_res, d_cigar, offs, d_cells, n};
+    GlobalArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_res, d_cigar, offs, d_cells + kCntGlobal, n};
     const size_t grid = std::min(nslots / kGT, (n + kGT - 1) / kGT);
     s.nslots = grid * kGT;   // fewer tasks than slots: pack the layout tighter
     // Re-derive pointers for the tighter layout so strides match nslots.
@@ -257,6 +257,7 @@ int launch_global(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     s.t = (uint8_t *)p;
     p += (size_t)tmax * s.nslots;
     s.z = (uint8_t *)p;
+    ProfScope ps(ctx, st, "global_nw_traceback", kCntGlobal);
     global_kernel<<<(unsigned)grid, kGT, 0, st>>>(a, s);
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());

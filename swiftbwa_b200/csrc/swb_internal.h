@@ -39,6 +39,15 @@ inline DevScoring make_dev_scoring(const swb_scoring &s) {
     return d;
 }
 
+// Cell counters: one per kernel family (indices below) in ctx->d_counters.
+enum CounterIdx {
+    kCntExtBin0 = 0,      // ext bins 0..4 -> 0..4
+    kCntGlobal = 8,
+    kCntLocalStriped = 9,
+    kCntLocalScalar = 10,
+    kNumCounters = 16
+};
+
 // ------------------------------------------------------------ a device arena
 // Grow-only device buffer owned by a context, counted against its budget.
 struct DevBuf {
@@ -73,6 +82,17 @@ struct swb_ctx {
     unsigned long long launches = 0;
     double last_ms = 0.0;
     unsigned long long last_cells = 0;
+    // per-kernel profiling
+    unsigned long long *d_counters = nullptr;   // swb::kNumCounters cells counters
+    bool prof_on = false;
+    struct ProfRec {
+        const char *name;
+        int counter;          // counter index or -1
+        cudaEvent_t a, b;
+    };
+    std::vector<ProfRec> prof;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
 };
 
 namespace swb {
@@ -85,6 +105,15 @@ int check_cuda(cudaError_t e, const char *what);
         cudaError_t _e = (call);                                     \
         if (_e != cudaSuccess) return ::swb::check_cuda(_e, #call);  \
     } while (0)
+
+// Brackets one kernel launch with events when profiling is on.
+struct ProfScope {
+    swb_ctx *ctx;
+    cudaStream_t s;
+    int idx = -1;
+    ProfScope(swb_ctx *c, cudaStream_t st, const char *name, int counter);
+    ~ProfScope();
+};
 
 // Grow-only allocation against the context budget.
 int ensure_dev(swb_ctx *ctx, DevBuf &b, size_t bytes);

@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(kLT) local_striped_kernel(LocalArgs a, int bin
         __syncwarp();
     }
     for (int o = 16; o > 0; o >>= 1) cells += __shfl_down_sync(kFull, cells, o);
-    if ((threadIdx.x & 31) == 0 && cells) atomicAdd(a.cells, cells);
+    if ((threadIdx.x & 31) == 0 && cells) atomicAdd(a.cells + kCntLocalStriped, cells);
 }
 
 // scalarSWPass (:383-492) over spans read through span_base.
@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(kST) local_scalar_kernel(LocalArgs a, int *hbu
         a.out[ti] = r;
     }
     for (int o = 16; o > 0; o >>= 1) cells += __shfl_down_sync(kFull, cells, o);
-    if ((threadIdx.x & 31) == 0 && cells) atomicAdd(a.cells, cells);
+    if ((threadIdx.x & 31) == 0 && cells) atomicAdd(a.cells + kCntLocalScalar, cells);
 }
 
 // Bin: 0 = scalar (qLen*A > 250 or empty), else the stripe count.
@@ -378,6 +378,13 @@ int launch_sn(swb_ctx *ctx, const LocalArgs &a, cudaStream_t st, uint32_t *peaks
     const size_t halves = std::min(halves_cap, n_bin);
     const size_t grid = (halves + kLT / 16 - 1) / (kLT / 16);
     if (grid == 0) return SWB_OK;
+    static const char *names[17] = {"", "local_striped_sn1", "local_striped_sn2", "local_striped_sn3",
+                                    "local_striped_sn4", "local_striped_sn5", "local_striped_sn6",
+                                    "local_striped_sn7", "local_striped_sn8", "local_striped_sn9",
+                                    "local_striped_sn10", "local_striped_sn11", "local_striped_sn12",
+                                    "local_striped_sn13", "local_striped_sn14", "local_striped_sn15",
+                                    "local_striped_sn16"};
+    ProfScope ps(ctx, st, names[SN], kCntLocalStriped);
     local_striped_kernel<SN><<<(unsigned)grid, kLT, 0, st>>>(a, SN, peaks, peak_stride);
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
@@ -437,7 +444,10 @@ int launch_local(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases, con
                               launch_sn<12>,  launch_sn<13>, launch_sn<14>, launch_sn<15>, launch_sn<16>};
     for (int sn = 1; sn <= max_sn; ++sn)
         if ((rc = fns[sn](ctx, a, st, peaks, peak_stride, halves_cap, n))) return rc;
-    local_scalar_kernel<<<(unsigned)(nsl / kST), kST, 0, st>>>(a, hbuf, ebuf, pbuf, nsl);
+    {
+        ProfScope ps(ctx, st, "local_scalar_i32", kCntLocalScalar);
+        local_scalar_kernel<<<(unsigned)(nsl / kST), kST, 0, st>>>(a, hbuf, ebuf, pbuf, nsl);
+    }
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
     return SWB_OK;

@@ -1,17 +1,19 @@
 // swb_runtime.cu -- context, device memory, staging and the C ABI of
 // libswb_cuda.so (include/swb_cuda.h).
 //
-// Synchronous batch calls: host arrays are packed into one pinned staging
-// buffer, copied to the device with a single cudaMemcpyAsync, processed on
-// the context's stream, and the results come back with one copy.  Device
-// buffers and pinned staging are grow-only and reused across calls; the
-// context's budget caps what it may hold on the device.
+// Synchronous batch calls: each host array (bases, tasks) is copied straight
+// from the caller's buffer with one cudaMemcpyAsync (full PCIe rate when the
+// caller's memory is pinned), processed on the context's stream, and the
+// results come back with one copy into the caller's output array.  Device
+// buffers are grow-only and reused across calls; the context's budget caps
+// what it may hold on the device.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 
 #include "swb_internal.h"
 
@@ -100,37 +102,77 @@ static int validate_scoring(const swb_scoring *sc) {
     return SWB_OK;
 }
 
-// Checks spans against the bases buffer / reference and lengths against the caps.
+// Checks spans against the bases buffer / reference and lengths against the
+// caps; large batches are checked by several host threads.
 template <class Task>
-static int validate_spans(const swb_ctx *ctx, const Task *tasks, size_t n, size_t n_bases,
-                          int *max_q, int *max_t) {
+static int validate_range(const swb_ctx *ctx, const Task *tasks, size_t lo, size_t hi, size_t n_bases,
+                          int *max_q, int *max_t, std::string *err, int *code) {
     int mq = 0, mt = 0;
-    for (size_t i = 0; i < n; ++i) {
+    for (size_t i = lo; i < hi; ++i) {
         const Task &t = tasks[i];
-        if (t.qlen < 0 || t.tlen < 0) return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": negative length");
-        if (t.qlen > kMaxLen || t.tlen > kMaxLen)
-            return set_error(SWB_ERR_TOO_LARGE, "task " + std::to_string(i) + ": length above 65535");
-        if (t.qlen > 0 && (t.q_off > n_bases || t.q_off + (uint64_t)t.qlen > n_bases))
-            return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": query span outside bases");
-        if (t.tlen > 0) {
+        const char *why = nullptr;
+        int c = SWB_ERR_INVALID_ARG;
+        if (t.qlen < 0 || t.tlen < 0) {
+            why = "negative length";
+        } else if (t.qlen > kMaxLen || t.tlen > kMaxLen) {
+            why = "length above 65535";
+            c = SWB_ERR_TOO_LARGE;
+        } else if (t.qlen > 0 && (t.q_off > n_bases || t.q_off + (uint64_t)t.qlen > n_bases)) {
+            why = "query span outside bases";
+        } else if (t.tlen > 0) {
             if (t.flags & SWB_T_FROM_REF) {
-                if (!ctx->d_pac) return set_error(SWB_ERR_NO_REFERENCE, "task reads the reference but none is uploaded");
-                if (t.t_off > ctx->ref_bases || t.t_off + (uint64_t)t.tlen > ctx->ref_bases)
-                    return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": target span outside reference");
+                if (!ctx->d_pac) {
+                    why = "task reads the reference but none is uploaded";
+                    c = SWB_ERR_NO_REFERENCE;
+                } else if (t.t_off > ctx->ref_bases || t.t_off + (uint64_t)t.tlen > ctx->ref_bases) {
+                    why = "target span outside reference";
+                }
             } else if (t.t_off > n_bases || t.t_off + (uint64_t)t.tlen > n_bases) {
-                return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": target span outside bases");
+                why = "target span outside bases";
             }
+        }
+        if (why) {
+            *err = "task " + std::to_string(i) + ": " + why;
+            *code = c;
+            return c;
         }
         mq = std::max(mq, t.qlen);
         mt = std::max(mt, t.tlen);
     }
-    if (max_q) *max_q = mq;
-    if (max_t) *max_t = mt;
+    *max_q = mq;
+    *max_t = mt;
     return SWB_OK;
 }
 
-// Stages `parts` into one pinned buffer and copies it to d_in; returns
-// device pointers to each part.
+template <class Task>
+static int validate_spans(const swb_ctx *ctx, const Task *tasks, size_t n, size_t n_bases, int *max_q,
+                          int *max_t) {
+    const size_t kChunk = 1 << 18;
+    const size_t nth = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), (n + kChunk - 1) / kChunk);
+    std::vector<int> mq(nth, 0), mt(nth, 0), codes(nth, 0);
+    std::vector<std::string> errs(nth);
+    if (nth <= 1) {
+        codes[0] = validate_range(ctx, tasks, 0, n, n_bases, &mq[0], &mt[0], &errs[0], &codes[0]);
+    } else {
+        std::vector<std::thread> th;
+        const size_t per = (n + nth - 1) / nth;
+        for (size_t k = 0; k < nth; ++k)
+            th.emplace_back([&, k] {
+                const size_t lo = k * per, hi = std::min(n, lo + per);
+                if (lo < hi) codes[k] = validate_range(ctx, tasks, lo, hi, n_bases, &mq[k], &mt[k], &errs[k], &codes[k]);
+            });
+        for (auto &t : th) t.join();
+    }
+    for (size_t k = 0; k < nth; ++k)
+        if (codes[k]) return set_error(codes[k], errs[k]);
+    if (max_q) *max_q = *std::max_element(mq.begin(), mq.end());
+    if (max_t) *max_t = *std::max_element(mt.begin(), mt.end());
+    return SWB_OK;
+}
+
+// Copies each part straight from the caller's buffer (pinned or pageable)
+// into one device region, one cudaMemcpyAsync per part; returns the device
+// pointer of each part.
 struct Part {
     const void *src;
     size_t bytes;
@@ -141,14 +183,13 @@ static int stage_in(swb_ctx *ctx, std::initializer_list<Part> parts) {
     size_t total = 0;
     for (const Part &p : parts) total += align256(p.bytes);
     int rc;
-    if ((rc = ensure_host(ctx, ctx->h_in, total + 256)) || (rc = ensure_dev(ctx, ctx->d_bases, total + 256))) return rc;
+    if ((rc = ensure_dev(ctx, ctx->d_bases, total + 256))) return rc;
     size_t off = 0;
     for (const Part &p : parts) {
-        if (p.bytes) std::memcpy((char *)ctx->h_in.p + off, p.src, p.bytes);
         *p.dev = (char *)ctx->d_bases.p + off;
+        if (p.bytes) SWB_CUDA(cudaMemcpyAsync(*p.dev, p.src, p.bytes, cudaMemcpyHostToDevice, ctx->stream));
         off += align256(p.bytes);
     }
-    SWB_CUDA(cudaMemcpyAsync(ctx->d_bases.p, ctx->h_in.p, std::max<size_t>(off, 1), cudaMemcpyHostToDevice, ctx->stream));
     return SWB_OK;
 }
 
@@ -156,10 +197,8 @@ struct Timer {
     swb_ctx *ctx;
     unsigned long long *d_cells;
     int begin() {
-        int rc;
-        if ((rc = ensure_dev(ctx, ctx->d_aux, 64))) return rc;
-        d_cells = (unsigned long long *)ctx->d_aux.p;
-        SWB_CUDA(cudaMemsetAsync(d_cells, 0, sizeof(unsigned long long), ctx->stream));
+        d_cells = ctx->d_counters;
+        SWB_CUDA(cudaMemsetAsync(d_cells, 0, sizeof(unsigned long long) * kNumCounters, ctx->stream));
         SWB_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
         return SWB_OK;
     }
@@ -171,10 +210,36 @@ struct Timer {
     void collect() {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) ctx->last_ms = ms;
-        unsigned long long c = 0;
-        if (cudaMemcpy(&c, d_cells, sizeof(c), cudaMemcpyDeviceToHost) == cudaSuccess) ctx->last_cells = c;
+        unsigned long long c[kNumCounters] = {0};
+        if (cudaMemcpy(c, d_cells, sizeof(c), cudaMemcpyDeviceToHost) == cudaSuccess) {
+            unsigned long long sum = 0;
+            for (int k = 0; k < kNumCounters; ++k) sum += c[k];
+            ctx->last_cells = sum;
+        }
     }
 };
+
+static cudaEvent_t pooled_event(swb_ctx *ctx) {
+    if (ctx->ev_used == ctx->ev_pool.size()) {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        ctx->ev_pool.push_back(e);
+    }
+    return ctx->ev_pool[ctx->ev_used++];
+}
+
+ProfScope::ProfScope(swb_ctx *c, cudaStream_t st, const char *name, int counter) : ctx(c), s(st) {
+    if (!ctx->prof_on) return;
+    cudaEvent_t a = pooled_event(ctx), b = pooled_event(ctx);
+    if (!a || !b) return;
+    ctx->prof.push_back(swb_ctx::ProfRec{name, counter, a, b});
+    idx = (int)ctx->prof.size() - 1;
+    cudaEventRecord(a, s);
+}
+
+ProfScope::~ProfScope() {
+    if (idx >= 0) cudaEventRecord(ctx->prof[idx].b, s);
+}
 
 }  // namespace swb
 
@@ -226,6 +291,8 @@ int swb_init(int device, size_t mem_budget_bytes, swb_ctx **out) {
     cudaMemGetInfo(&free_b, &total_b);
     ctx->budget = mem_budget_bytes ? mem_budget_bytes : free_b / 4 * 3;
     cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&ctx->d_counters, sizeof(unsigned long long) * kNumCounters);
+    if (e == cudaSuccess) e = cudaMemset(ctx->d_counters, 0, sizeof(unsigned long long) * kNumCounters);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_start);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_stop);
     if (e != cudaSuccess) {
@@ -244,6 +311,8 @@ void swb_destroy(swb_ctx *ctx) {
                       &ctx->d_idx2, &ctx->d_sort_tmp, &ctx->d_misc, &ctx->d_scratch, &ctx->d_cigar, &ctx->d_aux};
     for (DevBuf *b : bufs) free_buf(ctx, *b);
     if (ctx->d_pac) cudaFree(ctx->d_pac);
+    if (ctx->d_counters) cudaFree(ctx->d_counters);
+    for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     if (ctx->h_in.p) cudaFreeHost(ctx->h_in.p);
     if (ctx->h_out.p) cudaFreeHost(ctx->h_out.p);
     if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
@@ -314,10 +383,7 @@ int swb_ext_batch_device(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *d_b
     if (n_tasks == 0) return SWB_OK;
     SWB_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-    if ((rc = ensure_dev(ctx, ctx->d_aux, 64))) return rc;
-    unsigned long long *d_cells = (unsigned long long *)ctx->d_aux.p;
-    SWB_CUDA(cudaMemsetAsync(d_cells, 0, sizeof(unsigned long long), s));
-    return launch_ext(ctx, make_dev_scoring(*sc), d_bases, d_tasks, n_tasks, d_out, d_cells, s, -1);
+    return launch_ext(ctx, make_dev_scoring(*sc), d_bases, d_tasks, n_tasks, d_out, ctx->d_counters, s, -1);
 }
 
 int swb_global_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, size_t n_bases,
@@ -437,6 +503,54 @@ int swb_local_align(swb_ctx *ctx, const uint8_t *query, int32_t qlen, const uint
 }
 
 uint64_t swb_kernel_launches(const swb_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int swb_profile(swb_ctx *ctx, int enable) {
+    if (!ctx) return set_error(SWB_ERR_INVALID_ARG, "ctx is NULL");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->prof_on = enable != 0;
+    return SWB_OK;
+}
+
+int swb_profile_reset(swb_ctx *ctx) {
+    if (!ctx) return set_error(SWB_ERR_INVALID_ARG, "ctx is NULL");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    SWB_CUDA(cudaSetDevice(ctx->device));
+    SWB_CUDA(cudaDeviceSynchronize());
+    ctx->prof.clear();
+    ctx->ev_used = 0;
+    SWB_CUDA(cudaMemset(ctx->d_counters, 0, sizeof(unsigned long long) * kNumCounters));
+    return SWB_OK;
+}
+
+int swb_profile_read(swb_ctx *ctx, swb_kernel_stat *stats, int cap, int *n_stats) {
+    if (!ctx || !n_stats || (!stats && cap > 0)) return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    SWB_CUDA(cudaSetDevice(ctx->device));
+    SWB_CUDA(cudaDeviceSynchronize());
+    unsigned long long c[kNumCounters] = {0};
+    SWB_CUDA(cudaMemcpy(c, ctx->d_counters, sizeof(c), cudaMemcpyDeviceToHost));
+    std::vector<swb_kernel_stat> out;
+    std::vector<int> counters;
+    for (const auto &r : ctx->prof) {
+        float ms = 0.f;
+        SWB_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+        int k = 0;
+        while (k < (int)out.size() && std::strcmp(out[k].name, r.name) != 0) ++k;
+        if (k == (int)out.size()) {
+            swb_kernel_stat st{};
+            std::strncpy(st.name, r.name, sizeof(st.name) - 1);
+            out.push_back(st);
+            counters.push_back(r.counter);
+        }
+        out[k].launches++;
+        out[k].total_ms += ms;
+    }
+    for (size_t k = 0; k < out.size(); ++k)
+        out[k].cells = counters[k] >= 0 ? c[counters[k]] : 0;
+    *n_stats = (int)out.size();
+    for (int k = 0; k < (int)out.size() && k < cap; ++k) stats[k] = out[k];
+    return SWB_OK;
+}
 
 int swb_last_batch_stats(const swb_ctx *ctx, double *kernel_ms, uint64_t *cells) {
     if (!ctx) return set_error(SWB_ERR_INVALID_ARG, "ctx is NULL");

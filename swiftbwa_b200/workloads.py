@@ -1,0 +1,174 @@
+"""Seeded synthetic workloads for the five benchmark configurations
+(libswb_workload.so, built from csrc/swb_workload.cpp).
+
+The reference publishes no dataset for this path; every config is a seeded
+synthetic stand-in with the shapes, sizes and error rates the configs
+state.  Seeds are 0x5EED0000 + config (+ rank for multi-GPU shards).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from .abi import EXT_TASK_DTYPE, GLOBAL_TASK_DTYPE, LOCAL_TASK_DTYPE, SWB_GLB_RETRY
+from .build import WORKLOAD_OUT, build_workload
+
+SEED_BASE = 0x5EED0000
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(WORKLOAD_OUT):
+            build_workload()
+        L = C.CDLL(WORKLOAD_OUT)
+        vp, i64, u64, dbl, i32 = C.c_void_p, C.c_int64, C.c_uint64, C.c_double, C.c_int
+        L.swbw_reference.argtypes = [u64, u64, dbl, vp, vp, vp, i64]
+        L.swbw_reference.restype = i64
+        L.swbw_ext_tasks.argtypes = [u64, vp, i64, vp, i64, dbl, i64, i32, dbl, dbl, dbl, i32, i32, i32, i32,
+                                     i32, i32, i32, vp, vp, vp]
+        L.swbw_ext_tasks.restype = i64
+        L.swbw_uneven_tasks.argtypes = [u64, vp, i64, i64, i32, i32, vp, i32, i32, i32, i32, i32, dbl, dbl, i32,
+                                        vp, vp]
+        L.swbw_uneven_tasks.restype = i64
+        L.swbw_rescue_tasks.argtypes = [u64, vp, i64, i64, i32, i32, dbl, dbl, dbl, dbl, i32, vp, vp]
+        L.swbw_rescue_tasks.restype = None
+        _lib = L
+    return _lib
+
+
+@dataclass
+class Reference:
+    codes: np.ndarray          # one byte per base, 0-3
+    pac: np.ndarray            # .pac layout
+    blocks: np.ndarray         # (n, 2) tandem blocks [start, len]
+
+    @property
+    def n(self) -> int:
+        return int(self.codes.size)
+
+
+def reference(seed: int, n: int, tandem_frac: float = 0.0, max_blocks: int = 1 << 16) -> Reference:
+    codes = np.empty(n, np.uint8)
+    pac = np.empty((n + 3) // 4 + 16, np.uint8)
+    blocks = np.zeros((max_blocks, 2), np.int64)
+    nb = lib().swbw_reference(seed, n, tandem_frac, codes.ctypes.data, pac.ctypes.data, blocks.ctypes.data,
+                              max_blocks)
+    return Reference(codes, pac, blocks[:nb].copy())
+
+
+@dataclass
+class ExtWorkload:
+    ref: Reference
+    bases: np.ndarray                  # reads (or queries), one byte per base
+    tasks: np.ndarray                  # EXT_TASK_DTYPE
+    read_info: Optional[np.ndarray] = None   # (n_reads, 4): ref_start, ref_end, n_sub, indel_bases
+    read_len: int = 0
+    name: str = ""
+    meta: dict = field(default_factory=dict)
+
+
+def ext_from_reads(ref: Reference, seed: int, n_reads: int, read_len: int, *, sub=0.01, indel=0.001,
+                   n_rate=0.005, w=100, h0=19, end_bonus5=5, end_bonus3=5, left=True, random_seed_pos=True,
+                   tandem_read_frac=0.0, bases_out: Optional[np.ndarray] = None,
+                   tasks_out: Optional[np.ndarray] = None) -> ExtWorkload:
+    per = 2 if left else 1
+    reads = bases_out if bases_out is not None else np.empty(n_reads * read_len, np.uint8)
+    tasks = tasks_out if tasks_out is not None else np.empty(n_reads * per, EXT_TASK_DTYPE)
+    info = np.empty((n_reads, 4), np.int64)
+    nt = lib().swbw_ext_tasks(seed, ref.codes.ctypes.data, ref.n, ref.blocks.ctypes.data, len(ref.blocks),
+                              tandem_read_frac, n_reads, read_len, sub, indel, n_rate, 19, int(random_seed_pos),
+                              w, h0, end_bonus5, end_bonus3, int(left), reads.ctypes.data, tasks.ctypes.data,
+                              info.ctypes.data)
+    return ExtWorkload(ref, reads, tasks[:nt], info, read_len)
+
+
+def config0(rank: int = 0) -> ExtWorkload:
+    """10,000 right extensions: 100 bp reads off a 50 kbp reference, 1% subs,
+    0.1% 1-3 bp indels, 0.5% N; query = suffix after the first exact 19-mer,
+    target = qlen + w window; w=100, h0=19, end bonus 5."""
+    ref = reference(SEED_BASE + 0 + 1000 * rank, 50_000)
+    wl = ext_from_reads(ref, SEED_BASE + 0 + 1000 * rank + 1, 10_000, 100, left=False, random_seed_pos=False)
+    wl.name = "config0: 10k right extensions, 100 bp reads, 50 kbp reference"
+    return wl
+
+
+def config1(rank: int = 0, n_reads: int = 5_000_000, ref_len: int = 100_000_000) -> ExtWorkload:
+    """10M extension tasks (left on reversed prefixes + right) from 150 bp
+    reads off a 100 Mbp reference in which 20% of reads come from inserted
+    tandem-repeat blocks (period 2-6, 1-5 kbp); error rates as config 0."""
+    ref = reference(SEED_BASE + 1 + 1000 * rank, ref_len, tandem_frac=0.02)
+    wl = ext_from_reads(ref, SEED_BASE + 1 + 1000 * rank + 1, n_reads, 150, left=True, random_seed_pos=True,
+                        tandem_read_frac=0.2)
+    wl.name = f"config1: {len(wl.tasks)} left+right extensions, {n_reads} x 150 bp reads, {ref_len // 10**6} Mbp reference, 20% tandem-repeat reads"
+    return wl
+
+
+def global_from_reads(wl: ExtWorkload, scoring_a: int = 1, w: int = 100, only_non_fast_path: bool = True):
+    """Banded NW + CIGAR task per read hit span (config 1): query = read,
+    target = the reference span the read was drawn from.  With
+    only_non_fast_path, reads CIGARGenerator would answer with its pure-M
+    fast path (equal lengths, no indel, deficit < open+extend of both gaps,
+    CIGARGenerator.swift:59-80) are left out, as the reference skips their DP."""
+    info = wl.read_info
+    L = wl.read_len
+    rs, re_, nsub, nind = info[:, 0], info[:, 1], info[:, 2], info[:, 3]
+    rlen = np.minimum(re_ - rs, 10_000).astype(np.int64)
+    est = L * scoring_a - nsub * 5 - nind * 2
+    fast = (rlen == L) & (nind == 0) & (L * scoring_a - est < 14)
+    keep = ~fast if only_non_fast_path else np.ones(len(info), bool)
+    idx = np.nonzero(keep & (rlen > 0))[0]
+    t = np.zeros(len(idx), GLOBAL_TASK_DTYPE)
+    t["q_off"] = idx.astype(np.uint64) * L
+    t["t_off"] = rs[idx].astype(np.uint64)
+    t["qlen"] = L
+    t["tlen"] = rlen[idx]
+    t["w"] = w
+    t["true_score"] = est[idx]
+    t["flags"] = SWB_GLB_RETRY | 0x8    # SWB_T_FROM_REF
+    return t
+
+
+def config2(rank: int = 0, n: int = 20_000_000, ref_len: int = 100_000_000) -> ExtWorkload:
+    """20M uneven extensions: qlen log-uniform 30-250, w uniform 10-100,
+    target qlen + w, h0 uniform 19-60, 2% subs, 0.3% indels."""
+    ref = reference(SEED_BASE + 2 + 1000 * rank, ref_len)
+    return uneven(ref, SEED_BASE + 2 + 1000 * rank + 1, n, name=f"config2: {n} uneven extensions")
+
+
+def uneven(ref: Reference, seed: int, n: int, qmin=30, qmax=250, mix=None, wmin=10, wmax=100, h0min=19, h0max=60,
+           sub=0.02, indel=0.003, end_bonus=5, name="uneven") -> ExtWorkload:
+    bases = np.empty(n * qmax, np.uint8)
+    tasks = np.empty(n, EXT_TASK_DTYPE)
+    mix_arr = np.asarray(mix or [], np.int32)
+    used = lib().swbw_uneven_tasks(seed, ref.codes.ctypes.data, ref.n, n, qmin, qmax,
+                                   mix_arr.ctypes.data if mix_arr.size else None, int(mix_arr.size),
+                                   wmin, wmax, h0min, h0max, sub, indel, end_bonus, bases.ctypes.data,
+                                   tasks.ctypes.data)
+    return ExtWorkload(ref, bases[:used], tasks, None, 0, name)
+
+
+@dataclass
+class RescueWorkload:
+    ref: Reference
+    bases: np.ndarray
+    tasks: np.ndarray
+    name: str = ""
+
+
+def config3(rank: int = 0, n: int = 2_000_000, ref_len: int = 100_000_000) -> RescueWorkload:
+    """2M mate-rescue local SW: 150 bp mate (2% subs) vs a ~700 bp window
+    (insert 400 +- 50, window = mean +- 4 SD plus the mate), 10% no hit,
+    minSubScore = 19."""
+    ref = reference(SEED_BASE + 3 + 1000 * rank, ref_len)
+    bases = np.empty(n * 150, np.uint8)
+    tasks = np.empty(n, LOCAL_TASK_DTYPE)
+    lib().swbw_rescue_tasks(SEED_BASE + 3 + 1000 * rank + 1, ref.codes.ctypes.data, ref.n, n, 150, 700, 400.0,
+                            50.0, 0.02, 0.10, 19, bases.ctypes.data, tasks.ctypes.data)
+    return RescueWorkload(ref, bases, tasks, f"config3: {n} mate-rescue local SW, 150 bp vs 700 bp")
