@@ -197,6 +197,29 @@ int swb_ext_batch_device(swb_ctx *ctx, const swb_scoring *sc,
                          const uint8_t *d_bases, const swb_ext_task *d_tasks,
                          size_t n_tasks, swb_ext_result *d_out, void *stream);
 
+/* Allocation-free variant of swb_ext_batch_device.  It has no counterpart
+ * in the reference.  It is for callers that cannot let a library call
+ * cudaMalloc: a server whose own arena already holds the free HBM (the
+ * resident reference and admitted request buffers), or a continuous-batching
+ * loop that cannot afford cudaMalloc/cudaFree stalling its other streams.
+ * It needs no context: it runs on the calling thread's current device and
+ * on `stream` (a cudaStream_t, NULL = the legacy default stream); every
+ * pointer is a device pointer the caller owns (d_pac: the .pac reference
+ * for SWB_T_FROM_REF spans, may be NULL otherwise; spans are trusted, as in
+ * swb_ext_batch_device).  Its only working memory is one static device
+ * array of 18.9 MB that every GPU loading the library holds until the
+ * process exits.  Limit: a task that needs the int32 path (query above 256
+ * bases, or h0 + qlen*maxScore above 32000) may have at most 1024 query
+ * bases; a longer one gets an all-zero result and the call returns
+ * SWB_ERR_TOO_LARGE naming the first such task.  The first call on a device
+ * does a one-time set-up (looks up the array's address, sizes a kernel);
+ * make that first call before any stream capture.  The call waits for its
+ * stream to finish.  Calls share the array, so calls that overlap on the
+ * GPU (other threads or streams) race; serialise them. */
+int swb_ext_batch_static(const swb_scoring *sc, const uint8_t *d_bases, const uint8_t *d_pac,
+                         const swb_ext_task *d_tasks, size_t n_tasks, swb_ext_result *d_out,
+                         void *stream);
+
 /* --------------------------------------------- single-call Swift signatures */
 /* BandedSWScalar.align (BandedSWScalar.swift:21-28). */
 int swb_banded_sw_align(swb_ctx *ctx, const uint8_t *query, int32_t qlen,

@@ -118,7 +118,7 @@ EXPORTED_SYMBOLS = (
     "swb_global_batch", "swb_local_batch", "swb_ext_batch_device",
     "swb_banded_sw_align", "swb_global_align", "swb_local_align",
     "swb_kernel_launches", "swb_last_batch_stats", "swb_profile", "swb_profile_reset",
-    "swb_profile_read", "swb_int_alu_peak",
+    "swb_profile_read", "swb_int_alu_peak", "swb_ext_batch_static",
 )
 
 
@@ -184,6 +184,8 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.swb_profile_read.restype = C.c_int
     lib.swb_int_alu_peak.argtypes = [vp, P(C.c_double)]
     lib.swb_int_alu_peak.restype = C.c_int
+    lib.swb_ext_batch_static.argtypes = [P(Scoring), vp, vp, vp, C.c_size_t, vp, vp]
+    lib.swb_ext_batch_static.restype = C.c_int
     return lib
 
 
