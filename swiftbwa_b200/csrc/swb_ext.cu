@@ -2,21 +2,33 @@
 // BandedSWScalar.align (Sources/Alignment/BandedSWScalar.swift:21-191).
 //
 // Layout and schedule
-//   * One thread owns one extension.  Its DP row (H and E per query column)
-//     lives in shared memory as one 32-bit word per column, int16 H in the
-//     low half and int16 E in the high half, interleaved across the block's
-//     threads ([column][thread]) so every access is bank-conflict free.  The
-//     query is staged beside it, 4 codes per word.  This keeps the
-//     reference's storage semantics exactly: cells outside the current band
-//     keep their stale values, h[end] receives the last H of the row, and
-//     narrowing scans the same words the Swift loop scans.
-//   * Tasks are binned on the device by query length (<=32, 64, 128, 256)
-//     and radix-sorted by (bin, qlen, tlen) so a warp's threads walk rows of
-//     similar shape; each bin runs a kernel instantiated for its row size
-//     with a grid-stride loop over its slice of the sorted order.
+//   * One thread owns one extension and walks the Swift row loop literally,
+//     so the reference's storage semantics hold as written: cells outside
+//     the current band keep their stale values, h[end] receives the last H
+//     of the row, e[end] = 0, and band narrowing scans the words the Swift
+//     loop scans.
+//   * The DP row lives in shared memory as one 32-bit word per query column
+//     (H in the low half, E in the high half; both are >= 0 and below 32768
+//     for the tasks routed here), interleaved [column][thread] so that every
+//     access is bank-conflict free.  Beside it each column keeps the 16-bit
+//     prmt selector of its query base, so the score of a cell is one byte
+//     permute of the row's 8-byte score table with sign replication.
+//   * Per cell the recurrence is five fused integer ops:
+//         d   = relu(min(M + s, M << 7))   -- M ? M + s : 0, clamped at 0 (*)
+//         H   = max3(d, E, F)
+//         E'  = relu(max(E - eDel, d - oeDel))
+//         F'  = relu(max(F - eIns, d - oeIns))
+//         key = max(key, H << 16 | j)      -- row max, last j on ties
+//     (*) Clamping the diagonal at 0 changes no output: E and F are >= 0, so
+//     H = max(diag, E, F) is unchanged, and E', F' clamp at 0 anyway.
+//     M << 7 >= M + s for every M >= 1 because s <= a <= 127.
+//   * Tasks are binned on the device by query length (10 bins from 32 to
+//     256 columns) and radix-sorted by (bin, qlen, tlen) so a warp's threads
+//     walk rows of similar shape; each bin's kernel is instantiated for its
+//     row size and launched on its own stream, so the bins overlap on the GPU.
 //   * Tasks whose scores could leave int16 (h0 + qlen*maxScore > 32000) or
-//     whose query exceeds 256 run in an int32 kernel with the row in global
-//     scratch, same code path.
+//     whose query exceeds 256 run the generic device function over int32
+//     rows in global scratch (swb_ext_dp.cuh).
 #include <cub/device/device_radix_sort.cuh>
 
 #include "swb_device.cuh"
@@ -26,15 +38,19 @@
 namespace swb {
 namespace {
 
-constexpr int kNumBins = 5;           // 4 shared-memory bins + 1 global-scratch bin
-constexpr int kBigBin = 4;
-constexpr int kSmemT = 64;            // threads per block in the shared-memory kernels
+constexpr int kFastBins = 10;
+__device__ __constant__ int kFastQDev[kFastBins] = {32, 48, 64, 80, 96, 112, 128, 160, 192, 256};
+constexpr int kBigBin = kFastBins;        // global-scratch int32 bin
+constexpr int kNumBins = kFastBins + 1;
+constexpr int kFastT = 32;                // threads per block in the shared-memory kernels
 constexpr int kBigT = 64;
 
 __device__ __forceinline__ int ext_bin(const swb_ext_task &t, int max_mat) {
     if (t.qlen <= 0 || t.tlen <= 0) return 0;
     if (t.qlen > kExtSmemMaxQ || !fits16(t.qlen, t.h0, max_mat)) return kBigBin;
-    return t.qlen <= 32 ? 0 : t.qlen <= 64 ? 1 : t.qlen <= 128 ? 2 : 3;
+    int b = 0;
+    while (t.qlen > kFastQDev[b]) ++b;
+    return b;
 }
 
 // Sort key: bin in bits 28-31, query length in 16-27, target length in 0-15.
@@ -68,14 +84,123 @@ __global__ void bin_bounds_kernel(const uint32_t *__restrict__ sorted_keys, size
         for (int bb = b + 1; bb <= nbins; ++bb) bin_start[bb] = (uint32_t)n;
 }
 
+// One extension over the shared-memory row of this thread.
+//   he: this thread's column-0 word; column j is he[j*T]
+//   qs: this thread's column-0 selector; column j is qs[j*T]
+template <int T>
+__device__ __forceinline__ void ext_fast_one(const ExtArgs &a, const swb_ext_task &tk, uint32_t *__restrict__ he,
+                                             uint16_t *__restrict__ qs, swb_ext_result &res,
+                                             unsigned long long &cells) {
+    res = swb_ext_result{0, 0, 0, 0, 0, 0};
+    const int qlen = tk.qlen, tlen = tk.tlen;
+    if (!(qlen > 0 && tlen > 0)) return;                                   // :33-35
+    const DevScoring &sc = a.sc;
+    const int oDel = sc.o_del, eDel = sc.e_del, oIns = sc.o_ins, eIns = sc.e_ins;
+    const int oeDel = oDel + eDel, oeIns = oIns + eIns;
+    const int zDrop = sc.zdrop;
+    const int h0 = tk.h0;
+
+    // Query profile: the prmt selector of each column's base (:44-50).
+    for (int j = 0; j < qlen; ++j) {
+        const uint32_t q = span_base(a.bases, a.pac, tk.q_off, j, qlen, tk.flags, false);
+        qs[j * T] = (uint16_t)(q * 0x1111u + 0x8880u);
+    }
+    int w = tk.w;                                                          // :52-62
+    {
+        const int maxIns = (int)((double)(qlen * sc.max_mat + tk.end_bonus - oIns) / (double)eIns + 1.0);
+        w = imin(w, imax(1, maxIns));
+        const int maxDel = (int)((double)(qlen * sc.max_mat + tk.end_bonus - oDel) / (double)eDel + 1.0);
+        w = imin(w, imax(1, maxDel));
+    }
+    {                                                                      // :65-77
+        int j = 1;
+        he[0] = (uint32_t)h0;
+        if (h0 > oIns + eIns) {
+            int hv = h0 - oIns - eIns;
+            he[T] = (uint32_t)hv;
+            j = 2;
+            while (j <= qlen && hv > eIns) {
+                hv -= eIns;
+                he[j * T] = (uint32_t)hv;
+                ++j;
+            }
+        }
+        for (; j <= qlen; ++j) he[j * T] = 0u;
+    }
+    // Target reader: forward or reversed, bases or resident .pac, optional complement.
+    const bool tref = (tk.flags & SWB_T_FROM_REF) != 0;
+    const bool tcomp = (tk.flags & SWB_T_COMPLEMENT) != 0;
+    const long long tstep = (tk.flags & SWB_T_REVERSE) ? -1 : 1;
+    const long long tbase = (tk.flags & SWB_T_REVERSE) ? (long long)tk.t_off + tlen - 1 : (long long)tk.t_off;
+
+    int maxScore = h0, maxI = -1, maxJ = -1, gScore = -1, gTle = -1, maxOff = 0;
+    int beg = 0, end = qlen;
+    for (int i = 0; i < tlen; ++i) {                                       // :90
+        const unsigned long long idx = (unsigned long long)(tbase + tstep * i);
+        uint32_t tb = tref ? (a.pac[idx >> 2] >> ((3u - (uint32_t)(idx & 3)) << 1)) & 3u : a.bases[idx];
+        if (tcomp && tb < 4u) tb = 3u - tb;
+        const RowTable rt = row_table(sc, tb);
+        if (beg < i - w) beg = i - w;                                      // :95-97
+        if (end > i + w + 1) end = i + w + 1;
+        if (end > qlen) end = qlen;
+        int f = 0;
+        int h1 = beg == 0 ? imax(h0 - (oDel + eDel * (i + 1)), 0) : 0;    // :99-107
+        uint32_t key = 0;
+        if (end > beg) cells += (unsigned long long)(end - beg);
+        uint32_t *hp = he + beg * T;
+        const uint16_t *qp = qs + beg * T;
+#pragma unroll 4
+        for (int j = beg; j < end; ++j, hp += T, qp += T) {               // :112-143
+            const uint32_t wd = *hp;
+            const int M = (int)(wd & 0xFFFFu), e = (int)(wd >> 16);
+            const int s = (int)prmt(rt.lo, rt.hi, (uint32_t)*qp);
+            const int d = __viaddmin_s32_relu(M, s, M << 7);
+            const int H = __vimax3_s32(d, e, f);
+            const int nE = __viaddmax_s32_relu(e, -eDel, d - oeDel);
+            *hp = __byte_perm((uint32_t)h1, (uint32_t)nE, 0x5410);
+            h1 = H;
+            key = max(key, ((uint32_t)H << 16) | (uint32_t)j);
+            f = __viaddmax_s32_relu(f, -eIns, d - oeIns);
+        }
+        he[end * T] = (uint32_t)h1 & 0xFFFFu;                              // :145-146
+        const int rowMax = end > beg ? (int)(key >> 16) : 0;
+        const int rowMaxJ = (int)(key & 0xFFFFu);
+        if (end == qlen) {                                                 // :149-152
+            gTle = gScore > h1 ? gTle : i;
+            gScore = gScore > h1 ? gScore : h1;
+        }
+        if (rowMax == 0) break;                                            // :155
+        if (rowMax > maxScore) {                                           // :158-172
+            maxScore = rowMax;
+            maxI = i;
+            maxJ = rowMaxJ;
+            const int off = abs(rowMaxJ - i);
+            if (off > maxOff) maxOff = off;
+        } else if (zDrop > 0) {
+            const int dI = i - maxI, dJ = rowMaxJ - maxJ;
+            if (dI > dJ) {
+                if (maxScore - rowMax - (dI - dJ) * eDel > zDrop) break;
+            } else {
+                if (maxScore - rowMax - (dJ - dI) * eIns > zDrop) break;
+            }
+        }
+        int nb = beg;                                                      // :175-180
+        while (nb < end && he[nb * T] == 0u) ++nb;
+        beg = nb;
+        int ne = end;
+        while (ne >= beg && he[ne * T] == 0u) --ne;
+        end = imin(ne + 2, qlen);
+    }
+    res = swb_ext_result{maxScore, maxJ + 1, maxI + 1, gTle + 1, gScore, maxOff};   // :183-190
+}
+
 template <int QMAX, int T>
-__global__ void __launch_bounds__(T) ext_smem_kernel(ExtArgs a, int bin) {
+__global__ void __launch_bounds__(T) ext_fast_kernel(ExtArgs a, int bin) {
     extern __shared__ uint32_t sm[];
-    Smem16<T> st{sm, sm + (QMAX + 1) * T, (int)threadIdx.x};
+    uint32_t *he = sm + threadIdx.x;
+    uint16_t *qs = (uint16_t *)(sm + (QMAX + 1) * T) + threadIdx.x;
     const uint32_t lo = a.bin_start[bin], hi = a.bin_start[bin + 1];
     unsigned long long cells = 0;
-    // Every thread of the block runs the same number of iterations, so the
-    // warp-level reduction below sees all 32 lanes.
     const uint32_t span = hi - lo;
     const uint32_t per_iter = gridDim.x * (uint32_t)T;
     const uint32_t iters = (span + per_iter - 1) / per_iter;
@@ -85,7 +210,7 @@ __global__ void __launch_bounds__(T) ext_smem_kernel(ExtArgs a, int bin) {
             const uint32_t ti = a.order[pos];
             const swb_ext_task tk = a.tasks[ti];
             swb_ext_result r;
-            ext_one(a, tk, st, r, cells);
+            ext_fast_one<T>(a, tk, he, qs, r, cells);
             a.out[ti] = r;
         }
     }
@@ -114,29 +239,38 @@ __global__ void __launch_bounds__(kBigT) ext_global_kernel(ExtArgs a, int *h, in
 }
 
 template <int QMAX>
-size_t smem_bytes() { return (size_t)((QMAX + 1) + QMAX / 4) * kSmemT * sizeof(uint32_t); }
+constexpr size_t fast_smem_bytes() {
+    return (size_t)(QMAX + 1) * kFastT * sizeof(uint32_t) + (size_t)QMAX * kFastT * sizeof(uint16_t);
+}
+
+const char *const kBinNames[kNumBins] = {"ext_fast_q32",  "ext_fast_q48",  "ext_fast_q64",  "ext_fast_q80",
+                                         "ext_fast_q96",  "ext_fast_q112", "ext_fast_q128", "ext_fast_q160",
+                                         "ext_fast_q192", "ext_fast_q256", "ext_global_i32"};
 
 template <int QMAX>
-int launch_bin(swb_ctx *ctx, const ExtArgs &a, int bin, size_t n, cudaStream_t s) {
+int launch_fast(swb_ctx *ctx, const ExtArgs &a, int bin, size_t n, cudaStream_t s) {
     static int occ = -1;
-    const size_t smem = smem_bytes<QMAX>();
+    constexpr size_t smem = fast_smem_bytes<QMAX>();
     if (occ < 0) {
-        SWB_CUDA(cudaFuncSetAttribute(ext_smem_kernel<QMAX, kSmemT>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        SWB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ext_smem_kernel<QMAX, kSmemT>,
-                                                               kSmemT, smem));
+        SWB_CUDA(cudaFuncSetAttribute(ext_fast_kernel<QMAX, kFastT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        SWB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ext_fast_kernel<QMAX, kFastT>, kFastT, smem));
         if (occ < 1) occ = 1;
     }
-    const size_t need = (n + kSmemT - 1) / kSmemT;
+    const size_t need = (n + kFastT - 1) / kFastT;
     const size_t grid = std::min<size_t>(need, (size_t)ctx->sm_count * occ);
     if (grid == 0) return SWB_OK;
-    static const char *names[4] = {"ext_smem_q32", "ext_smem_q64", "ext_smem_q128", "ext_smem_q256"};
-    ProfScope ps(ctx, s, names[bin], kCntExtBin0 + bin);
-    ext_smem_kernel<QMAX, kSmemT><<<(unsigned)grid, kSmemT, smem, s>>>(a, bin);
+    ProfScope ps(ctx, s, kBinNames[bin], kCntExtBin0 + bin);
+    ext_fast_kernel<QMAX, kFastT><<<(unsigned)grid, kFastT, smem, s>>>(a, bin);
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
     return SWB_OK;
 }
+
+using FastLauncher = int (*)(swb_ctx *, const ExtArgs &, int, size_t, cudaStream_t);
+const FastLauncher kFastLaunch[kFastBins] = {launch_fast<32>,  launch_fast<48>,  launch_fast<64>,  launch_fast<80>,
+                                             launch_fast<96>,  launch_fast<112>, launch_fast<128>, launch_fast<160>,
+                                             launch_fast<192>, launch_fast<256>};
 
 }  // namespace
 
@@ -153,7 +287,7 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     uint32_t *keys = (uint32_t *)ctx->d_keys.p, *keys2 = (uint32_t *)ctx->d_keys2.p;
     uint32_t *idx = (uint32_t *)ctx->d_idx.p, *idx2 = (uint32_t *)ctx->d_idx2.p;
     uint32_t *bin_start = (uint32_t *)ctx->d_misc.p;          // kNumBins+1 words
-    int *big_max_q = (int *)((char *)ctx->d_misc.p + 64);
+    int *big_max_q = (int *)((char *)ctx->d_misc.p + 128);
     SWB_CUDA(cudaMemsetAsync(big_max_q, 0, sizeof(int), s));
     const unsigned tb = 256;
     {
@@ -177,31 +311,39 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
 
-    ExtArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_out, idx2, bin_start, d_cells};
-    if ((rc = launch_bin<32>(ctx, a, 0, n, s))) return rc;
-    if ((rc = launch_bin<64>(ctx, a, 1, n, s))) return rc;
-    if ((rc = launch_bin<128>(ctx, a, 2, n, s))) return rc;
-    if ((rc = launch_bin<256>(ctx, a, 3, n, s))) return rc;
-
     // Global-scratch bin: size its scratch from the longest query in it.
     int max_q = max_q_hint;
     if (max_q < 0) {
         SWB_CUDA(cudaMemcpyAsync(&max_q, big_max_q, sizeof(int), cudaMemcpyDeviceToHost, s));
         SWB_CUDA(cudaStreamSynchronize(s));
     }
+    if (max_q > kMaxLen) return set_error(SWB_ERR_TOO_LARGE, "query longer than 65535 bases");
+    const size_t nslots = (size_t)ctx->sm_count * 4 * kBigT;
+    const size_t cols = (size_t)max_q + 1;
     if (max_q > 0) {
-        if (max_q > kMaxLen) return set_error(SWB_ERR_TOO_LARGE, "query longer than 65535 bases");
-        const size_t nslots = (size_t)ctx->sm_count * 4 * kBigT;
-        const size_t cols = (size_t)max_q + 1;
         const size_t bytes = cols * nslots * (2 * sizeof(int) + 1) + 256;
         if ((rc = ensure_dev(ctx, ctx->d_scratch, bytes))) return rc;
-        int *hbuf = (int *)ctx->d_scratch.p;
-        int *ebuf = hbuf + cols * nslots;
-        uint8_t *qbuf = (uint8_t *)(ebuf + cols * nslots);
-        ProfScope ps(ctx, s, "ext_global_i32", kCntExtBin0 + kBigBin);
-        ext_global_kernel<<<(unsigned)(nslots / kBigT), kBigT, 0, s>>>(a, hbuf, ebuf, qbuf, nslots);
-        ctx->launches++;
-        SWB_CUDA(cudaGetLastError());
+    }
+
+    // Fork: every bin runs on its own stream after the sort, then joins back.
+    ExtArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_out, idx2, bin_start, d_cells};
+    SWB_CUDA(cudaEventRecord(ctx->fork_ev, s));
+    for (int b = 0; b < kNumBins; ++b) {
+        cudaStream_t sb = ctx->side[b];
+        SWB_CUDA(cudaStreamWaitEvent(sb, ctx->fork_ev, 0));
+        if (b < kFastBins) {
+            if ((rc = kFastLaunch[b](ctx, a, b, n, sb))) return rc;
+        } else if (max_q > 0) {
+            int *hbuf = (int *)ctx->d_scratch.p;
+            int *ebuf = hbuf + cols * nslots;
+            uint8_t *qbuf = (uint8_t *)(ebuf + cols * nslots);
+            ProfScope ps(ctx, sb, kBinNames[kBigBin], kCntExtBin0 + kBigBin);
+            ext_global_kernel<<<(unsigned)(nslots / kBigT), kBigT, 0, sb>>>(a, hbuf, ebuf, qbuf, nslots);
+            ctx->launches++;
+            SWB_CUDA(cudaGetLastError());
+        }
+        SWB_CUDA(cudaEventRecord(ctx->join_ev[b], sb));
+        SWB_CUDA(cudaStreamWaitEvent(s, ctx->join_ev[b], 0));
     }
     return SWB_OK;
 }

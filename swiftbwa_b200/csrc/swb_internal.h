@@ -41,12 +41,14 @@ inline DevScoring make_dev_scoring(const swb_scoring &s) {
 
 // Cell counters: one per kernel family (indices below) in ctx->d_counters.
 enum CounterIdx {
-    kCntExtBin0 = 0,      // ext bins 0..4 -> 0..4
-    kCntGlobal = 8,
-    kCntLocalStriped = 9,
-    kCntLocalScalar = 10,
+    kCntExtBin0 = 0,      // extension bins 0..10 -> 0..10
+    kCntGlobal = 12,
+    kCntLocalStriped = 13,
+    kCntLocalScalar = 14,
     kNumCounters = 16
 };
+
+constexpr int kSideStreams = 12;   // concurrent bin launches per context
 
 // ------------------------------------------------------------ a device arena
 // Grow-only device buffer owned by a context, counted against its budget.
@@ -68,6 +70,10 @@ struct swb_ctx {
     int sm_count = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    // fork/join of the per-bin kernels
+    cudaStream_t side[swb::kSideStreams] = {};
+    cudaEvent_t fork_ev = nullptr;
+    cudaEvent_t join_ev[swb::kSideStreams] = {};
     size_t budget = 0;       // cap on bytes the context allocates on the device
     size_t allocated = 0;    // bytes currently allocated
     std::mutex mu;

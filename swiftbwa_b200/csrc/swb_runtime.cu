@@ -293,6 +293,11 @@ int swb_init(int device, size_t mem_budget_bytes, swb_ctx **out) {
     cudaError_t e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&ctx->d_counters, sizeof(unsigned long long) * kNumCounters);
     if (e == cudaSuccess) e = cudaMemset(ctx->d_counters, 0, sizeof(unsigned long long) * kNumCounters);
+    for (int k = 0; k < kSideStreams && e == cudaSuccess; ++k) {
+        e = cudaStreamCreateWithFlags(&ctx->side[k], cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->join_ev[k], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_start);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_stop);
     if (e != cudaSuccess) {
@@ -317,6 +322,14 @@ void swb_destroy(swb_ctx *ctx) {
     if (ctx->h_out.p) cudaFreeHost(ctx->h_out.p);
     if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
     if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+    for (int k = 0; k < kSideStreams; ++k) {
+        if (ctx->side[k]) {
+            cudaStreamSynchronize(ctx->side[k]);
+            cudaStreamDestroy(ctx->side[k]);
+        }
+        if (ctx->join_ev[k]) cudaEventDestroy(ctx->join_ev[k]);
+    }
+    if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
