@@ -22,14 +22,25 @@
 //     (*) Clamping the diagonal at 0 changes no output: E and F are >= 0, so
 //     H = max(diag, E, F) is unchanged, and E', F' clamp at 0 anyway.
 //     M << 7 >= M + s for every M >= 1 because s <= a <= 127.
-//   * Tasks are binned on the device by query length (10 bins from 32 to
-//     256 columns) and radix-sorted by (bin, qlen, tlen) so a warp's threads
-//     walk rows of similar shape; each bin's kernel is instantiated for its
-//     row size and launched on its own stream, so the bins overlap on the GPU.
+//   * Tasks whose score bound h0 + qlen*maxScore is at most 255 (all
+//     short-read extensions with the default scoring) use int8 rows instead:
+//     one word per column holding the selector (low half), H and E (one
+//     byte each), so a cell needs one shared load and the row takes 4 bytes
+//     per column.  The bound is static, so the int8 rows never saturate and
+//     nothing is re-run.
+//   * Tasks are binned on the device by row width (int8 / int16) and query
+//     length (10 classes from 32 to 256 columns) and radix-sorted by
+//     (bin, qlen, tlen) so a warp's threads walk rows of similar shape; each
+//     bin's kernel is instantiated for its row size and launched on its own
+//     stream, so the bins overlap on the GPU.
 //   * Tasks whose scores could leave int16 (h0 + qlen*maxScore > 32000) or
 //     whose query exceeds 256 run the generic device function over int32
 //     rows in global scratch (swb_ext_dp.cuh).
 #include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <thread>
+#include <vector>
 
 #include "swb_device.cuh"
 #include "swb_ext_dp.cuh"
@@ -38,22 +49,30 @@
 namespace swb {
 namespace {
 
-constexpr int kFastBins = 10;
-__device__ __constant__ int kFastQDev[kFastBins] = {32, 48, 64, 80, 96, 112, 128, 160, 192, 256};
-constexpr int kBigBin = kFastBins;        // global-scratch int32 bin
+// Bins 0-9: int8 rows (score bound <= 255), 10-19: int16 rows, by query
+// length class; bin 20: int32 rows in global scratch.
+constexpr int kLenClasses = 10;
+__device__ __constant__ int kFastQDev[kLenClasses] = {32, 48, 64, 80, 96, 112, 128, 160, 192, 256};
+constexpr int kFastBins = 2 * kLenClasses;
+constexpr int kBigBin = kFastBins;
 constexpr int kNumBins = kFastBins + 1;
 constexpr int kFastT = 32;                // threads per block in the shared-memory kernels
 constexpr int kBigT = 64;
+
+// True when every H/E of the task fits one byte: H <= h0 + qlen*maxMat.
+__device__ __forceinline__ bool fits8(int qlen, int h0, int max_mat) {
+    return h0 >= 0 && (long long)h0 + (long long)qlen * (max_mat > 0 ? max_mat : 0) <= 255;
+}
 
 __device__ __forceinline__ int ext_bin(const swb_ext_task &t, int max_mat) {
     if (t.qlen <= 0 || t.tlen <= 0) return 0;
     if (t.qlen > kExtSmemMaxQ || !fits16(t.qlen, t.h0, max_mat)) return kBigBin;
     int b = 0;
     while (t.qlen > kFastQDev[b]) ++b;
-    return b;
+    return fits8(t.qlen, t.h0, max_mat) ? b : kLenClasses + b;
 }
 
-// Sort key: bin in bits 28-31, query length in 16-27, target length in 0-15.
+// Sort key: bin in bits 27-31, query length in 15-26, target length in 0-14.
 __global__ void ext_keys_kernel(const swb_ext_task *__restrict__ tasks, size_t n, int max_mat,
                                 uint32_t *__restrict__ keys, uint32_t *__restrict__ idx,
                                 int *__restrict__ big_max_q) {
@@ -62,8 +81,8 @@ __global__ void ext_keys_kernel(const swb_ext_task *__restrict__ tasks, size_t n
     const swb_ext_task t = tasks[i];
     const int b = ext_bin(t, max_mat);
     const uint32_t q = (uint32_t)min(max(t.qlen, 0), 4095);
-    const uint32_t tl = (uint32_t)min(max(t.tlen, 0), 65535);
-    keys[i] = ((uint32_t)b << 28) | (q << 16) | tl;
+    const uint32_t tl = (uint32_t)min(max(t.tlen, 0), 32767);
+    keys[i] = ((uint32_t)b << 27) | (q << 15) | tl;
     idx[i] = (uint32_t)i;
     if (b == kBigBin) atomicMax(big_max_q, t.qlen);
 }
@@ -77,17 +96,17 @@ __global__ void bin_bounds_kernel(const uint32_t *__restrict__ sorted_keys, size
         return;
     }
     if (p >= n) return;
-    const int b = (int)(sorted_keys[p] >> 28);
-    const int bprev = p == 0 ? -1 : (int)(sorted_keys[p - 1] >> 28);
+    const int b = (int)(sorted_keys[p] >> 27);
+    const int bprev = p == 0 ? -1 : (int)(sorted_keys[p - 1] >> 27);
     for (int bb = bprev + 1; bb <= b; ++bb) bin_start[bb] = (uint32_t)p;
     if (p == n - 1)
         for (int bb = b + 1; bb <= nbins; ++bb) bin_start[bb] = (uint32_t)n;
 }
 
 // One extension over the shared-memory row of this thread.
-//   he: this thread's column-0 word; column j is he[j*T]
-//   qs: this thread's column-0 selector; column j is qs[j*T]
-template <int T>
+//   U8 = false: he[j*T] = H | E << 16, qs[j*T] = the column's prmt selector.
+//   U8 = true : he[j*T] = selector | H << 16 | E << 24 (scores <= 255); qs unused.
+template <int T, bool U8>
 __device__ __forceinline__ void ext_fast_one(const ExtArgs &a, const swb_ext_task &tk, uint32_t *__restrict__ he,
                                              uint16_t *__restrict__ qs, swb_ext_result &res,
                                              unsigned long long &cells) {
@@ -100,10 +119,33 @@ __device__ __forceinline__ void ext_fast_one(const ExtArgs &a, const swb_ext_tas
     const int zDrop = sc.zdrop;
     const int h0 = tk.h0;
 
-    // Query profile: the prmt selector of each column's base (:44-50).
-    for (int j = 0; j < qlen; ++j) {
-        const uint32_t q = span_base(a.bases, a.pac, tk.q_off, j, qlen, tk.flags, false);
-        qs[j * T] = (uint16_t)(q * 0x1111u + 0x8880u);
+    // Query profile: the prmt selector of each column's base (:44-50), and
+    // the first row from h0 (:65-77).
+    {
+        int hv = h0;
+        bool ramp = h0 > oIns + eIns;
+        for (int j = 0; j <= qlen; ++j) {
+            int hj = 0;
+            if (j == 0) {
+                hj = h0;
+            } else if (j == 1) {
+                if (ramp) hj = hv = h0 - oIns - eIns;
+            } else if (ramp && hv > eIns) {
+                hj = hv -= eIns;
+            } else {
+                ramp = false;
+            }
+            if (U8) {
+                const uint32_t q = j < qlen ? span_base(a.bases, a.pac, tk.q_off, j, qlen, tk.flags, false) : 5u;
+                he[j * T] = ((q * 0x1111u + 0x8880u) & 0xFFFFu) | ((uint32_t)hj << 16);
+            } else {
+                if (j < qlen) {
+                    const uint32_t q = span_base(a.bases, a.pac, tk.q_off, j, qlen, tk.flags, false);
+                    qs[j * T] = (uint16_t)(q * 0x1111u + 0x8880u);
+                }
+                he[j * T] = (uint32_t)hj;
+            }
+        }
     }
     int w = tk.w;                                                          // :52-62
     {
@@ -112,26 +154,13 @@ __device__ __forceinline__ void ext_fast_one(const ExtArgs &a, const swb_ext_tas
         const int maxDel = (int)((double)(qlen * sc.max_mat + tk.end_bonus - oDel) / (double)eDel + 1.0);
         w = imin(w, imax(1, maxDel));
     }
-    {                                                                      // :65-77
-        int j = 1;
-        he[0] = (uint32_t)h0;
-        if (h0 > oIns + eIns) {
-            int hv = h0 - oIns - eIns;
-            he[T] = (uint32_t)hv;
-            j = 2;
-            while (j <= qlen && hv > eIns) {
-                hv -= eIns;
-                he[j * T] = (uint32_t)hv;
-                ++j;
-            }
-        }
-        for (; j <= qlen; ++j) he[j * T] = 0u;
-    }
     // Target reader: forward or reversed, bases or resident .pac, optional complement.
     const bool tref = (tk.flags & SWB_T_FROM_REF) != 0;
     const bool tcomp = (tk.flags & SWB_T_COMPLEMENT) != 0;
     const long long tstep = (tk.flags & SWB_T_REVERSE) ? -1 : 1;
     const long long tbase = (tk.flags & SWB_T_REVERSE) ? (long long)tk.t_off + tlen - 1 : (long long)tk.t_off;
+    // A column is all-zero (h == 0 and e == 0) when its H|E bits are zero.
+    const uint32_t nzmask = U8 ? 0xFFFF0000u : 0xFFFFFFFFu;
 
     int maxScore = h0, maxI = -1, maxJ = -1, gScore = -1, gTle = -1, maxOff = 0;
     int beg = 0, end = qlen;
@@ -148,21 +177,39 @@ __device__ __forceinline__ void ext_fast_one(const ExtArgs &a, const swb_ext_tas
         uint32_t key = 0;
         if (end > beg) cells += (unsigned long long)(end - beg);
         uint32_t *hp = he + beg * T;
-        const uint16_t *qp = qs + beg * T;
+        if (U8) {
 #pragma unroll 4
-        for (int j = beg; j < end; ++j, hp += T, qp += T) {               // :112-143
-            const uint32_t wd = *hp;
-            const int M = (int)(wd & 0xFFFFu), e = (int)(wd >> 16);
-            const int s = (int)prmt(rt.lo, rt.hi, (uint32_t)*qp);
-            const int d = __viaddmin_s32_relu(M, s, M << 7);
-            const int H = __vimax3_s32(d, e, f);
-            const int nE = __viaddmax_s32_relu(e, -eDel, d - oeDel);
-            *hp = __byte_perm((uint32_t)h1, (uint32_t)nE, 0x5410);
-            h1 = H;
-            key = max(key, ((uint32_t)H << 16) | (uint32_t)j);
-            f = __viaddmax_s32_relu(f, -eIns, d - oeIns);
+            for (int j = beg; j < end; ++j, hp += T) {                    // :112-143
+                const uint32_t wd = *hp;
+                const int s = (int)prmt(rt.lo, rt.hi, wd);
+                const int M = (int)__byte_perm(wd, 0u, 0x4442);
+                const int e = (int)(wd >> 24);
+                const int d = __viaddmin_s32_relu(M, s, M << 7);
+                const int H = __vimax3_s32(d, e, f);
+                const int nE = __viaddmax_s32_relu(e, -eDel, d - oeDel);
+                *hp = __byte_perm(wd, __byte_perm((uint32_t)h1, (uint32_t)nE, 0x0040), 0x5410);
+                h1 = H;
+                key = max(key, ((uint32_t)H << 16) | (uint32_t)j);
+                f = __viaddmax_s32_relu(f, -eIns, d - oeIns);
+            }
+            he[end * T] = (he[end * T] & 0xFFFFu) | ((uint32_t)h1 << 16);  // :145-146
+        } else {
+            const uint16_t *qp = qs + beg * T;
+#pragma unroll 4
+            for (int j = beg; j < end; ++j, hp += T, qp += T) {           // :112-143
+                const uint32_t wd = *hp;
+                const int M = (int)(wd & 0xFFFFu), e = (int)(wd >> 16);
+                const int s = (int)prmt(rt.lo, rt.hi, (uint32_t)*qp);
+                const int d = __viaddmin_s32_relu(M, s, M << 7);
+                const int H = __vimax3_s32(d, e, f);
+                const int nE = __viaddmax_s32_relu(e, -eDel, d - oeDel);
+                *hp = __byte_perm((uint32_t)h1, (uint32_t)nE, 0x5410);
+                h1 = H;
+                key = max(key, ((uint32_t)H << 16) | (uint32_t)j);
+                f = __viaddmax_s32_relu(f, -eIns, d - oeIns);
+            }
+            he[end * T] = (uint32_t)h1 & 0xFFFFu;                          // :145-146
         }
-        he[end * T] = (uint32_t)h1 & 0xFFFFu;                              // :145-146
         const int rowMax = end > beg ? (int)(key >> 16) : 0;
         const int rowMaxJ = (int)(key & 0xFFFFu);
         if (end == qlen) {                                                 // :149-152
@@ -185,20 +232,20 @@ __device__ __forceinline__ void ext_fast_one(const ExtArgs &a, const swb_ext_tas
             }
         }
         int nb = beg;                                                      // :175-180
-        while (nb < end && he[nb * T] == 0u) ++nb;
+        while (nb < end && (he[nb * T] & nzmask) == 0u) ++nb;
         beg = nb;
         int ne = end;
-        while (ne >= beg && he[ne * T] == 0u) --ne;
+        while (ne >= beg && (he[ne * T] & nzmask) == 0u) --ne;
         end = imin(ne + 2, qlen);
     }
     res = swb_ext_result{maxScore, maxJ + 1, maxI + 1, gTle + 1, gScore, maxOff};   // :183-190
 }
 
-template <int QMAX, int T>
+template <int QMAX, int T, bool U8>
 __global__ void __launch_bounds__(T) ext_fast_kernel(ExtArgs a, int bin) {
     extern __shared__ uint32_t sm[];
     uint32_t *he = sm + threadIdx.x;
-    uint16_t *qs = (uint16_t *)(sm + (QMAX + 1) * T) + threadIdx.x;
+    uint16_t *qs = U8 ? nullptr : (uint16_t *)(sm + (QMAX + 1) * T) + threadIdx.x;
     const uint32_t lo = a.bin_start[bin], hi = a.bin_start[bin + 1];
     unsigned long long cells = 0;
     const uint32_t span = hi - lo;
@@ -210,7 +257,7 @@ __global__ void __launch_bounds__(T) ext_fast_kernel(ExtArgs a, int bin) {
             const uint32_t ti = a.order[pos];
             const swb_ext_task tk = a.tasks[ti];
             swb_ext_result r;
-            ext_fast_one<T>(a, tk, he, qs, r, cells);
+            ext_fast_one<T, U8>(a, tk, he, qs, r, cells);
             a.out[ti] = r;
         }
     }
@@ -238,39 +285,44 @@ __global__ void __launch_bounds__(kBigT) ext_global_kernel(ExtArgs a, int *h, in
     add_cells(a.cells + kCntExtBin0 + kBigBin, cells);
 }
 
-template <int QMAX>
+template <int QMAX, bool U8>
 constexpr size_t fast_smem_bytes() {
-    return (size_t)(QMAX + 1) * kFastT * sizeof(uint32_t) + (size_t)QMAX * kFastT * sizeof(uint16_t);
+    return (size_t)(QMAX + 1) * kFastT * sizeof(uint32_t) + (U8 ? 0 : (size_t)QMAX * kFastT * sizeof(uint16_t));
 }
 
-const char *const kBinNames[kNumBins] = {"ext_fast_q32",  "ext_fast_q48",  "ext_fast_q64",  "ext_fast_q80",
-                                         "ext_fast_q96",  "ext_fast_q112", "ext_fast_q128", "ext_fast_q160",
-                                         "ext_fast_q192", "ext_fast_q256", "ext_global_i32"};
+const char *const kBinNames[kNumBins] = {
+    "ext_u8_q32",  "ext_u8_q48",  "ext_u8_q64",  "ext_u8_q80",  "ext_u8_q96",  "ext_u8_q112",  "ext_u8_q128",
+    "ext_u8_q160", "ext_u8_q192", "ext_u8_q256", "ext_i16_q32", "ext_i16_q48", "ext_i16_q64",  "ext_i16_q80",
+    "ext_i16_q96", "ext_i16_q112", "ext_i16_q128", "ext_i16_q160", "ext_i16_q192", "ext_i16_q256",
+    "ext_global_i32"};
 
-template <int QMAX>
+template <int QMAX, bool U8>
 int launch_fast(swb_ctx *ctx, const ExtArgs &a, int bin, size_t n, cudaStream_t s) {
     static int occ = -1;
-    constexpr size_t smem = fast_smem_bytes<QMAX>();
+    constexpr size_t smem = fast_smem_bytes<QMAX, U8>();
     if (occ < 0) {
-        SWB_CUDA(cudaFuncSetAttribute(ext_fast_kernel<QMAX, kFastT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        SWB_CUDA(cudaFuncSetAttribute(ext_fast_kernel<QMAX, kFastT, U8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
-        SWB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ext_fast_kernel<QMAX, kFastT>, kFastT, smem));
+        SWB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ext_fast_kernel<QMAX, kFastT, U8>, kFastT, smem));
         if (occ < 1) occ = 1;
     }
     const size_t need = (n + kFastT - 1) / kFastT;
     const size_t grid = std::min<size_t>(need, (size_t)ctx->sm_count * occ);
     if (grid == 0) return SWB_OK;
     ProfScope ps(ctx, s, kBinNames[bin], kCntExtBin0 + bin);
-    ext_fast_kernel<QMAX, kFastT><<<(unsigned)grid, kFastT, smem, s>>>(a, bin);
+    ext_fast_kernel<QMAX, kFastT, U8><<<(unsigned)grid, kFastT, smem, s>>>(a, bin);
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
     return SWB_OK;
 }
 
 using FastLauncher = int (*)(swb_ctx *, const ExtArgs &, int, size_t, cudaStream_t);
-const FastLauncher kFastLaunch[kFastBins] = {launch_fast<32>,  launch_fast<48>,  launch_fast<64>,  launch_fast<80>,
-                                             launch_fast<96>,  launch_fast<112>, launch_fast<128>, launch_fast<160>,
-                                             launch_fast<192>, launch_fast<256>};
+const FastLauncher kFastLaunch[kFastBins] = {
+    launch_fast<32, true>,   launch_fast<48, true>,   launch_fast<64, true>,  launch_fast<80, true>,
+    launch_fast<96, true>,   launch_fast<112, true>,  launch_fast<128, true>, launch_fast<160, true>,
+    launch_fast<192, true>,  launch_fast<256, true>,  launch_fast<32, false>, launch_fast<48, false>,
+    launch_fast<64, false>,  launch_fast<80, false>,  launch_fast<96, false>, launch_fast<112, false>,
+    launch_fast<128, false>, launch_fast<160, false>, launch_fast<192, false>, launch_fast<256, false>};
 
 }  // namespace
 
@@ -327,6 +379,7 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
 
     // Fork: every bin runs on its own stream after the sort, then joins back.
     ExtArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_out, idx2, bin_start, d_cells};
+    ProfScope pass(ctx, s, "ext_pass", -1);   // fork to join, on the launching stream
     SWB_CUDA(cudaEventRecord(ctx->fork_ev, s));
     for (int b = 0; b < kNumBins; ++b) {
         cudaStream_t sb = ctx->side[b];
@@ -348,15 +401,28 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     return SWB_OK;
 }
 
-// Host-side twin of the device bin test, used to size the scratch bin.
+// Host-side twin of the device bin test, used to size the scratch bin
+// (several host threads for large batches).
 int ext_big_max_q(const swb_ext_task *tasks, size_t n, int max_mat) {
-    int m = 0;
-    for (size_t i = 0; i < n; ++i) {
-        const swb_ext_task &t = tasks[i];
-        if (t.qlen <= 0 || t.tlen <= 0) continue;
-        if (t.qlen > kExtSmemMaxQ || !fits16(t.qlen, t.h0, max_mat)) m = t.qlen > m ? t.qlen : m;
-    }
-    return m;
+    auto range = [&](size_t lo, size_t hi) {
+        int m = 0;
+        for (size_t i = lo; i < hi; ++i) {
+            const swb_ext_task &t = tasks[i];
+            if (t.qlen <= 0 || t.tlen <= 0) continue;
+            if (t.qlen > kExtSmemMaxQ || !fits16(t.qlen, t.h0, max_mat)) m = t.qlen > m ? t.qlen : m;
+        }
+        return m;
+    };
+    const size_t kChunk = 1 << 18;
+    const size_t nth = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), (n + kChunk - 1) / kChunk);
+    if (nth <= 1) return range(0, n);
+    std::vector<int> part(nth, 0);
+    std::vector<std::thread> th;
+    const size_t per = (n + nth - 1) / nth;
+    for (size_t k = 0; k < nth; ++k)
+        th.emplace_back([&, k] { part[k] = range(k * per, std::min(n, (k + 1) * per)); });
+    for (auto &t : th) t.join();
+    return *std::max_element(part.begin(), part.end());
 }
 
 }  // namespace swb

@@ -41,14 +41,14 @@ inline DevScoring make_dev_scoring(const swb_scoring &s) {
 
 // Cell counters: one per kernel family (indices below) in ctx->d_counters.
 enum CounterIdx {
-    kCntExtBin0 = 0,      // extension bins 0..10 -> 0..10
-    kCntGlobal = 12,
-    kCntLocalStriped = 13,
-    kCntLocalScalar = 14,
-    kNumCounters = 16
+    kCntExtBin0 = 0,      // extension bins 0..20 -> 0..20
+    kCntGlobal = 24,
+    kCntLocalStriped = 25,
+    kCntLocalScalar = 26,
+    kNumCounters = 32
 };
 
-constexpr int kSideStreams = 12;   // concurrent bin launches per context
+constexpr int kSideStreams = 24;   // concurrent bin launches per context
 
 // ------------------------------------------------------------ a device arena
 // Grow-only device buffer owned by a context, counted against its budget.
