@@ -49,6 +49,7 @@ enum CounterIdx {
 };
 
 constexpr int kSideStreams = 24;   // concurrent bin launches per context
+constexpr int kMaxChunks = 16;     // pipelined chunks of one synchronous batch call
 
 // ------------------------------------------------------------ a device arena
 // Grow-only device buffer owned by a context, counted against its budget.
@@ -74,6 +75,9 @@ struct swb_ctx {
     cudaStream_t side[swb::kSideStreams] = {};
     cudaEvent_t fork_ev = nullptr;
     cudaEvent_t join_ev[swb::kSideStreams] = {};
+    // host<->device copy streams and per-chunk events of the pipelined batch calls
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t chunk_in[swb::kMaxChunks] = {}, chunk_done[swb::kMaxChunks] = {};
     size_t budget = 0;       // cap on bytes the context allocates on the device
     size_t allocated = 0;    // bytes currently allocated
     std::mutex mu;

@@ -298,6 +298,12 @@ int swb_init(int device, size_t mem_budget_bytes, swb_ctx **out) {
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->join_ev[k], cudaEventDisableTiming);
     }
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking);
+    for (int k = 0; k < kMaxChunks && e == cudaSuccess; ++k) {
+        e = cudaEventCreateWithFlags(&ctx->chunk_in[k], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->chunk_done[k], cudaEventDisableTiming);
+    }
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_start);
     if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev_stop);
     if (e != cudaSuccess) {
@@ -330,6 +336,15 @@ void swb_destroy(swb_ctx *ctx) {
         if (ctx->join_ev[k]) cudaEventDestroy(ctx->join_ev[k]);
     }
     if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+    for (cudaStream_t st : {ctx->h2d, ctx->d2h})
+        if (st) {
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
+    for (int k = 0; k < kMaxChunks; ++k) {
+        if (ctx->chunk_in[k]) cudaEventDestroy(ctx->chunk_in[k]);
+        if (ctx->chunk_done[k]) cudaEventDestroy(ctx->chunk_done[k]);
+    }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -371,16 +386,57 @@ int swb_ext_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, siz
     SWB_CUDA(cudaSetDevice(ctx->device));
     const DevScoring dsc = make_dev_scoring(*sc);
     const int big_q = ext_big_max_q(tasks, n_tasks, dsc.max_mat);
-    void *d_b = nullptr, *d_t = nullptr;
-    if ((rc = stage_in(ctx, {Part{bases, n_bases, &d_b}, Part{tasks, n_tasks * sizeof(swb_ext_task), &d_t}}))) return rc;
+
+    // Chunks of at least 1M tasks, at most kMaxChunks; chunk k may start once
+    // the prefix of `bases` its tasks (and all earlier ones) reference is on
+    // the device.
+    const size_t kMinChunk = 1u << 20;
+    const size_t nchunks = std::min<size_t>(kMaxChunks, std::max<size_t>(1, n_tasks / kMinChunk));
+    const size_t per = (n_tasks + nchunks - 1) / nchunks;
+    std::vector<size_t> need(nchunks, 0);
+    {
+        std::vector<std::thread> th;
+        for (size_t k = 0; k < nchunks; ++k)
+            th.emplace_back([&, k] {
+                size_t m = 0;
+                for (size_t i = k * per; i < std::min(n_tasks, (k + 1) * per); ++i) {
+                    const swb_ext_task &t = tasks[i];
+                    if (t.qlen > 0) m = std::max<size_t>(m, t.q_off + (size_t)t.qlen);
+                    if (t.tlen > 0 && !(t.flags & SWB_T_FROM_REF)) m = std::max<size_t>(m, t.t_off + (size_t)t.tlen);
+                }
+                need[k] = m;
+            });
+        for (auto &t : th) t.join();
+        for (size_t k = 1; k < nchunks; ++k) need[k] = std::max(need[k], need[k - 1]);
+    }
+    const size_t bases_bytes = align256(std::max<size_t>(n_bases, 1));
+    if ((rc = ensure_dev(ctx, ctx->d_bases, bases_bytes + align256(n_tasks * sizeof(swb_ext_task)) + 256))) return rc;
     if ((rc = ensure_dev(ctx, ctx->d_out, n_tasks * sizeof(swb_ext_result)))) return rc;
+    uint8_t *d_b = (uint8_t *)ctx->d_bases.p;
+    swb_ext_task *d_t = (swb_ext_task *)((char *)ctx->d_bases.p + bases_bytes);
+    swb_ext_result *d_o = (swb_ext_result *)ctx->d_out.p;
     Timer tm{ctx, nullptr};
     if ((rc = tm.begin())) return rc;
-    if ((rc = launch_ext(ctx, dsc, (const uint8_t *)d_b, (const swb_ext_task *)d_t, n_tasks,
-                         (swb_ext_result *)ctx->d_out.p, tm.d_cells, ctx->stream, big_q)))
-        return rc;
+    // Copies must not overtake work still using these buffers.
+    SWB_CUDA(cudaEventRecord(ctx->fork_ev, ctx->stream));
+    SWB_CUDA(cudaStreamWaitEvent(ctx->h2d, ctx->fork_ev, 0));
+    size_t copied = 0;
+    for (size_t k = 0; k < nchunks; ++k) {
+        const size_t lo = k * per, hi = std::min(n_tasks, lo + per);
+        if (need[k] > copied) {
+            SWB_CUDA(cudaMemcpyAsync(d_b + copied, bases + copied, need[k] - copied, cudaMemcpyHostToDevice, ctx->h2d));
+            copied = need[k];
+        }
+        SWB_CUDA(cudaMemcpyAsync(d_t + lo, tasks + lo, (hi - lo) * sizeof(swb_ext_task), cudaMemcpyHostToDevice, ctx->h2d));
+        SWB_CUDA(cudaEventRecord(ctx->chunk_in[k], ctx->h2d));
+        SWB_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->chunk_in[k], 0));
+        if ((rc = launch_ext(ctx, dsc, d_b, d_t + lo, hi - lo, d_o + lo, tm.d_cells, ctx->stream, big_q))) return rc;
+        SWB_CUDA(cudaEventRecord(ctx->chunk_done[k], ctx->stream));
+        SWB_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->chunk_done[k], 0));
+        SWB_CUDA(cudaMemcpyAsync(out + lo, d_o + lo, (hi - lo) * sizeof(swb_ext_result), cudaMemcpyDeviceToHost, ctx->d2h));
+    }
     if ((rc = tm.end())) return rc;
-    SWB_CUDA(cudaMemcpyAsync(out, ctx->d_out.p, n_tasks * sizeof(swb_ext_result), cudaMemcpyDeviceToHost, ctx->stream));
+    SWB_CUDA(cudaStreamSynchronize(ctx->d2h));
     SWB_CUDA(cudaStreamSynchronize(ctx->stream));
     tm.collect();
     return SWB_OK;

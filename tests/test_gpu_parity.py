@@ -126,3 +126,19 @@ def test_local_fuzz(engine, oracle_mod, si):
     exp, _ = oracle_mod.local_batch(sc, d["bases"], d["tasks"], n_threads=8)
     bad = _cmp_struct(got, exp, got.dtype.names)
     assert bad.size == 0, f"{bad.size} mismatches, first {bad[:5]}: {got[bad[:3]]} vs {exp[bad[:3]]} tasks {d['tasks'][bad[:3]]}"
+
+
+def test_ext_config_workloads_chunked(engine, oracle_mod):
+    """Config-0 and a 2.6M-task config-1 shard through the host entry point
+    (the latter runs as pipelined chunks), every task against the oracle."""
+    import os
+    from swiftbwa_b200 import workloads as W
+    sc = Scoring.default()
+    for wl in (W.config0(), W.config1(n_reads=1_300_000, ref_len=10_000_000)):
+        engine.upload_reference(wl.ref.pac, wl.ref.n)
+        got = engine.ext_batch(sc, wl.bases, wl.tasks)
+        exp, cells = oracle_mod.ext_batch(sc, wl.bases, wl.tasks, pac=wl.ref.pac, ref_bases=wl.ref.n,
+                                          n_threads=os.cpu_count() or 8)
+        bad = _cmp_struct(got, exp, got.dtype.names)
+        assert bad.size == 0, f"{wl.name}: {bad.size} mismatches, first {bad[:5]}"
+        assert engine.last_batch_stats()[1] == cells
