@@ -127,6 +127,40 @@ typedef struct swb_global_result {
     uint64_t cigar_off;   /* offset (in ops) of this task's CIGAR in the output      */
 } swb_global_result;
 
+/* One call of CIGARGenerator.generate(querySegment:refSegment:qb:qe:readLength:
+ * isReverse:trueScore:initialW:scoring:refPos:) (CIGARGenerator.swift:30-111):
+ * band inference, the pure-M fast path, banded global alignment with the
+ * band-doubling retry, leading/trailing deletion squeeze, NM, MD and soft
+ * clips.  q_off/qlen is the query segment, t_off/rlen the reference segment
+ * (spans as for the other tasks; SWB_T_* flags apply to the segment). */
+typedef struct swb_cigar_task {
+    uint64_t q_off, t_off;
+    int32_t  qlen, rlen;
+    int32_t  qb, qe;          /* alignment bounds in read coordinates        */
+    int32_t  read_len;
+    int32_t  is_reverse;
+    int32_t  true_score;
+    int32_t  initial_w;
+    int64_t  ref_pos;
+    uint32_t flags;
+    int32_t  reserved;
+} swb_cigar_task;             /* 64 bytes */
+
+/* CIGARResult (Sources/Alignment/GlobalAlignResult.swift:20-44).  The CIGAR
+ * (soft clips included) is at cigar_out[cigar_off .. +n_cigar), the MD
+ * string (NUL-terminated) at md_out[md_off]. */
+typedef struct swb_cigar_result {
+    int32_t  score;
+    int32_t  nm;
+    int32_t  n_cigar;
+    int32_t  md_len;
+    int64_t  pos;
+    uint64_t cigar_off;       /* sum over earlier tasks of (qlen + rlen + 2)       */
+    uint64_t md_off;          /* sum over earlier tasks of (6 * (qlen + rlen) + 8) */
+    int32_t  used_dp;         /* 0 = pure-M fast path (:59-80), 1 = global DP      */
+    int32_t  reserved;
+} swb_cigar_result;           /* 48 bytes */
+
 /* ------------------------------------------------ kernel 3: local SW (rescue) */
 /* One call of LocalSWAligner.align(query:target:scoring:scoringMatrix:minSubScore:)
  * (Sources/Alignment/LocalSWAligner.swift:42-45). */
@@ -180,6 +214,16 @@ int swb_global_batch(swb_ctx *ctx, const swb_scoring *sc,
                      const swb_global_task *tasks, size_t n_tasks,
                      swb_global_result *results,
                      uint32_t *cigar_out, size_t cigar_cap);
+
+/* CIGARGenerator.generate for a batch (replaces the GlobalSWDispatcher +
+ * CIGARGenerator.postProcess pair of BWAMemAligner.swift:483-668).
+ * cigar_cap >= sum of (qlen + rlen + 2); md_cap >= sum of (6*(qlen+rlen)+8). */
+int swb_cigar_batch(swb_ctx *ctx, const swb_scoring *sc,
+                    const uint8_t *bases, size_t n_bases,
+                    const swb_cigar_task *tasks, size_t n_tasks,
+                    swb_cigar_result *results,
+                    uint32_t *cigar_out, size_t cigar_cap,
+                    char *md_out, size_t md_cap);
 
 /* Replaces LocalSWDispatcher.dispatchBatch (LocalSWDispatcher.swift:31),
  * with score2 computed on the device (the Metal path hard-codes it to 0,

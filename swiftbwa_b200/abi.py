@@ -118,8 +118,17 @@ EXPORTED_SYMBOLS = (
     "swb_global_batch", "swb_local_batch", "swb_ext_batch_device",
     "swb_banded_sw_align", "swb_global_align", "swb_local_align",
     "swb_kernel_launches", "swb_last_batch_stats", "swb_profile", "swb_profile_reset",
-    "swb_profile_read", "swb_int_alu_peak", "swb_ext_batch_static",
+    "swb_profile_read", "swb_int_alu_peak", "swb_ext_batch_static", "swb_cigar_batch",
 )
+
+CIGAR_TASK_DTYPE = np.dtype([("q_off", "<u8"), ("t_off", "<u8"), ("qlen", "<i4"), ("rlen", "<i4"),
+                             ("qb", "<i4"), ("qe", "<i4"), ("read_len", "<i4"), ("is_reverse", "<i4"),
+                             ("true_score", "<i4"), ("initial_w", "<i4"), ("ref_pos", "<i8"),
+                             ("flags", "<u4"), ("reserved", "<i4")])
+CIGAR_RESULT_DTYPE = np.dtype([("score", "<i4"), ("nm", "<i4"), ("n_cigar", "<i4"), ("md_len", "<i4"),
+                               ("pos", "<i8"), ("cigar_off", "<u8"), ("md_off", "<u8"),
+                               ("used_dp", "<i4"), ("reserved", "<i4")])
+assert CIGAR_TASK_DTYPE.itemsize == 64 and CIGAR_RESULT_DTYPE.itemsize == 48
 
 
 class KernelStat(C.Structure):
@@ -186,6 +195,9 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.swb_int_alu_peak.restype = C.c_int
     lib.swb_ext_batch_static.argtypes = [P(Scoring), vp, vp, vp, C.c_size_t, vp, vp]
     lib.swb_ext_batch_static.restype = C.c_int
+    lib.swb_cigar_batch.argtypes = [vp, P(Scoring), u8p, C.c_size_t, vp, C.c_size_t, vp, P(C.c_uint32),
+                                    C.c_size_t, C.c_char_p, C.c_size_t]
+    lib.swb_cigar_batch.restype = C.c_int
     return lib
 
 

@@ -147,6 +147,42 @@ class Engine:
                "swb_local_batch")
         return out
 
+    def cigar_batch(self, sc: Scoring, bases: np.ndarray, tasks: np.ndarray):
+        """CIGARGenerator.generate over CIGAR_TASK_DTYPE tasks -> list of dicts
+        (cigar, nm, md, score, pos, used_dp)."""
+        assert tasks.dtype == abi.CIGAR_TASK_DTYPE
+        ql = tasks["qlen"].astype(np.int64)
+        rl = tasks["rlen"].astype(np.int64)
+        ccap = int((ql + rl + 2).sum()) + 1
+        mcap = int((6 * (ql + rl) + 8).sum()) + 1
+        res = np.zeros(len(tasks), abi.CIGAR_RESULT_DTYPE)
+        cig = np.zeros(ccap, np.uint32)
+        md = C.create_string_buffer(mcap)
+        bases = np.ascontiguousarray(bases, dtype=np.uint8)
+        if bases.size == 0:
+            bases = np.zeros(1, np.uint8)
+        _check(self.lib.swb_cigar_batch(self.h, C.byref(sc), ptr(bases), bases.size, tasks.ctypes.data,
+                                        len(tasks), res.ctypes.data, ptr(cig, C.c_uint32), ccap, md, mcap),
+               "swb_cigar_batch")
+        raw = md.raw
+        out = []
+        for r in res:
+            o, n = int(r["cigar_off"]), int(r["n_cigar"])
+            mo, ml = int(r["md_off"]), int(r["md_len"])
+            out.append(dict(cigar=[int(x) for x in cig[o:o + n]], nm=int(r["nm"]), md=raw[mo:mo + ml].decode(),
+                            score=int(r["score"]), pos=int(r["pos"]), used_dp=bool(r["used_dp"])))
+        return out
+
+    def cigar_generate(self, query_segment, ref_segment, qb, qe, read_len, is_reverse, true_score,
+                       initial_w, scoring: Scoring, ref_pos) -> dict:
+        """CIGARGenerator.generate (Sources/Alignment/CIGARGenerator.swift:30-42)."""
+        q, r = _u8(query_segment), _u8(ref_segment)
+        bases = np.concatenate([q, r]) if q.size + r.size else np.zeros(1, np.uint8)
+        t = np.zeros(1, abi.CIGAR_TASK_DTYPE)
+        t[0] = (0, q.size, q.size, r.size, qb, qe, read_len, int(bool(is_reverse)), true_score, initial_w,
+                ref_pos, 0, 0)
+        return self.cigar_batch(scoring, bases, t)[0]
+
     def last_batch_stats(self):
         ms, cells = C.c_double(), C.c_uint64()
         _check(self.lib.swb_last_batch_stats(self.h, C.byref(ms), C.byref(cells)), "stats")

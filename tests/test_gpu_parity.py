@@ -46,7 +46,7 @@ class GpuBackend:
 CASES = known.load()["known_answers"]
 
 
-@pytest.mark.parametrize("case", [c for c in CASES if c["fn"] in ("ext", "global", "global_w_pair", "local")],
+@pytest.mark.parametrize("case", [c for c in CASES if c["fn"] in ("ext", "global", "global_w_pair", "local", "cigar")],
                          ids=lambda c: c["name"])
 def test_known_answer_on_gpu(case, engine, oracle_mod):
     fails = known.evaluate(case, GpuBackend(engine, oracle_mod))
@@ -142,3 +142,41 @@ def test_ext_config_workloads_chunked(engine, oracle_mod):
         bad = _cmp_struct(got, exp, got.dtype.names)
         assert bad.size == 0, f"{wl.name}: {bad.size} mismatches, first {bad[:5]}"
         assert engine.last_batch_stats()[1] == cells
+
+
+@pytest.mark.parametrize("si", [0, 3])
+def test_cigar_generate_fuzz(engine, oracle_mod, si):
+    """CIGARGenerator.generate: fast path, device DP with retries, squeeze,
+    NM, MD and soft clips against the oracle, task by task."""
+    from swiftbwa_b200.abi import CIGAR_TASK_DTYPE
+    sc = Scoring.default(**SCORINGS[si])
+    rng = np.random.default_rng(5000 + si)
+    chunks, rows, cases = [], [], []
+    off = 0
+    for k in range(1500):
+        rl_read = int(rng.integers(20, 200))
+        read = rng.integers(0, 4, rl_read).astype(np.uint8)
+        qb = int(rng.integers(0, rl_read // 3))
+        qe = int(rng.integers(max(qb + 1, rl_read - rl_read // 3), rl_read + 1))
+        qseg = read[qb:qe].copy()
+        rseg = gen.mutate(rng, qseg, sub=rng.choice([0.0, 0.01, 0.05]), indel=rng.choice([0.0, 0.0, 0.02, 0.05]))
+        if rng.random() < 0.2:   # leading/trailing reference bases -> squeezed deletions
+            rseg = np.concatenate([rng.integers(0, 4, int(rng.integers(0, 4))).astype(np.uint8), rseg,
+                                   rng.integers(0, 4, int(rng.integers(0, 4))).astype(np.uint8)])
+        if len(rseg) == 0:
+            rseg = np.array([2], np.uint8)
+        true_score = int(len(qseg) * sc.a - rng.integers(0, 30))
+        iw = int(rng.choice([1, 5, 20, 100]))
+        is_rev = bool(rng.random() < 0.5)
+        pos = int(rng.integers(0, 10**9))
+        chunks += [qseg, rseg]
+        rows.append((off, off + len(qseg), len(qseg), len(rseg), qb, qe, rl_read, int(is_rev), true_score, iw, pos, 0, 0))
+        cases.append((qseg, rseg, qb, qe, rl_read, is_rev, true_score, iw, pos))
+        off += len(qseg) + len(rseg)
+    tasks = np.array(rows, dtype=CIGAR_TASK_DTYPE)
+    got = engine.cigar_batch(sc, np.concatenate(chunks), tasks)
+    for k, c in enumerate(cases):
+        exp = oracle_mod.cigar_generate(c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], sc, c[8])
+        g = got[k]
+        assert (g["cigar"], g["nm"], g["md"], g["score"], g["pos"], g["used_dp"]) == \
+            (exp["cigar"], exp["nm"], exp["md"], exp["score"], exp["pos"], exp["used_dp"]), (k, g, exp)
