@@ -264,6 +264,47 @@ int swb_ext_batch_static(const swb_scoring *sc, const uint8_t *d_bases, const ui
                          const swb_ext_task *d_tasks, size_t n_tasks, swb_ext_result *d_out,
                          void *stream);
 
+/* ------------------------------------------------ serving (continuous batching) */
+/* A request loop over one context's GPU for extension batches of differing
+ * sizes that arrive concurrently (the actor loop of BWAMemAligner's
+ * read-chunk pipeline, main.swift:315-423, batching its extensions).
+ * Requests are queued and answered asynchronously by ticket.  A worker
+ * thread forms waves from the head of the queue (at most max_wave_tasks
+ * tasks, large requests split across waves so small ones do not wait behind
+ * them), stages each request's bases once into a device arena admitted
+ * against arena_bytes, sorts/bins every wave's tasks together, and
+ * alternates waves between two internal lanes so that one wave's copies
+ * overlap the other's kernels.  plain = 1 disables all of that: one
+ * request at a time, one launch sequence each (the baseline).  The caller
+ * keeps each request's buffers alive until its ticket completes; each
+ * task's result is the same as from swb_ext_batch. */
+typedef struct swb_server swb_server;
+typedef struct swb_server_opts {
+    size_t   arena_bytes;      /* device bytes for request bases (0 = 1 GiB)   */
+    size_t   max_wave_tasks;   /* tasks per wave (0 = 1M)                      */
+    int32_t  plain;            /* 1 = one request per launch, no overlap       */
+    int32_t  start_paused;     /* 1 = admit nothing until swb_server_resume    */
+} swb_server_opts;
+typedef struct swb_server_stats {
+    uint64_t submitted, completed, tasks_completed, waves;
+    uint64_t cells;            /* DP cells of completed waves                  */
+    double   busy_ms;          /* summed wave device time                      */
+} swb_server_stats;
+int swb_server_start(swb_ctx *ctx, const swb_scoring *sc, const swb_server_opts *opts, swb_server **out);
+int swb_server_submit(swb_server *srv, const uint8_t *bases, size_t n_bases,
+                      const swb_ext_task *tasks, size_t n_tasks, swb_ext_result *out, uint64_t *ticket);
+/* *done = 1 once the ticket completed; *status = its result status. */
+int swb_server_poll(swb_server *srv, uint64_t ticket, int *done, int *status);
+/* Waits at most timeout_ms (SWB_ERR_TIMEOUT after that).  On completion the
+ * ticket is released and its submit/completion times (steady-clock ns) are
+ * returned; *status is the request's own status. */
+int swb_server_wait(swb_server *srv, uint64_t ticket, int timeout_ms, int *status,
+                    uint64_t *submit_ns, uint64_t *done_ns);
+int swb_server_resume(swb_server *srv);
+int swb_server_stats_get(swb_server *srv, swb_server_stats *st);
+/* Drains the queue, stops the worker, frees the server's device memory. */
+int swb_server_stop(swb_server *srv);
+
 /* --------------------------------------------- single-call Swift signatures */
 /* BandedSWScalar.align (BandedSWScalar.swift:21-28). */
 int swb_banded_sw_align(swb_ctx *ctx, const uint8_t *query, int32_t qlen,

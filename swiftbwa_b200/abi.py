@@ -119,7 +119,19 @@ EXPORTED_SYMBOLS = (
     "swb_banded_sw_align", "swb_global_align", "swb_local_align",
     "swb_kernel_launches", "swb_last_batch_stats", "swb_profile", "swb_profile_reset",
     "swb_profile_read", "swb_int_alu_peak", "swb_ext_batch_static", "swb_cigar_batch",
+    "swb_server_start", "swb_server_submit", "swb_server_poll", "swb_server_wait", "swb_server_resume",
+    "swb_server_stats_get", "swb_server_stop",
 )
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("arena_bytes", C.c_size_t), ("max_wave_tasks", C.c_size_t), ("plain", C.c_int32),
+                ("start_paused", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("tasks_completed", C.c_uint64),
+                ("waves", C.c_uint64), ("cells", C.c_uint64), ("busy_ms", C.c_double)]
 
 CIGAR_TASK_DTYPE = np.dtype([("q_off", "<u8"), ("t_off", "<u8"), ("qlen", "<i4"), ("rlen", "<i4"),
                              ("qb", "<i4"), ("qe", "<i4"), ("read_len", "<i4"), ("is_reverse", "<i4"),
@@ -198,6 +210,16 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.swb_cigar_batch.argtypes = [vp, P(Scoring), u8p, C.c_size_t, vp, C.c_size_t, vp, P(C.c_uint32),
                                     C.c_size_t, C.c_char_p, C.c_size_t]
     lib.swb_cigar_batch.restype = C.c_int
+    lib.swb_server_start.argtypes = [vp, P(Scoring), P(ServerOpts), P(vp)]
+    lib.swb_server_submit.argtypes = [vp, u8p, C.c_size_t, vp, C.c_size_t, vp, P(C.c_uint64)]
+    lib.swb_server_poll.argtypes = [vp, C.c_uint64, P(C.c_int), P(C.c_int)]
+    lib.swb_server_wait.argtypes = [vp, C.c_uint64, C.c_int, P(C.c_int), P(C.c_uint64), P(C.c_uint64)]
+    lib.swb_server_resume.argtypes = [vp]
+    lib.swb_server_stats_get.argtypes = [vp, P(ServerStats)]
+    lib.swb_server_stop.argtypes = [vp]
+    for f in ("swb_server_start", "swb_server_submit", "swb_server_poll", "swb_server_wait", "swb_server_resume",
+              "swb_server_stats_get", "swb_server_stop"):
+        getattr(lib, f).restype = C.c_int
     return lib
 
 

@@ -321,7 +321,7 @@ void swb_destroy(swb_ctx *ctx) {
     DevBuf *bufs[] = {&ctx->d_bases, &ctx->d_tasks, &ctx->d_out, &ctx->d_keys, &ctx->d_keys2, &ctx->d_idx,
                       &ctx->d_idx2, &ctx->d_sort_tmp, &ctx->d_misc, &ctx->d_scratch, &ctx->d_cigar, &ctx->d_aux};
     for (DevBuf *b : bufs) free_buf(ctx, *b);
-    if (ctx->d_pac) cudaFree(ctx->d_pac);
+    if (ctx->d_pac && ctx->pac_owned) cudaFree(ctx->d_pac);
     if (ctx->d_counters) cudaFree(ctx->d_counters);
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     if (ctx->h_in.p) cudaFreeHost(ctx->h_in.p);

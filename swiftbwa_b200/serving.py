@@ -1,0 +1,149 @@
+"""Python side of the continuous-batching request loop (swb_server_* in
+include/swb_cuda.h) and the config-4 request-stream driver used by bench.py.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+import time
+from dataclasses import dataclass
+from typing import List, Optional
+
+import numpy as np
+
+from . import abi
+from .abi import EXT_RESULT_DTYPE, EXT_TASK_DTYPE, Scoring, ptr
+from .alignment import Engine, _check
+
+
+class Server:
+    """A request loop on one Engine's GPU.  Keeps every submitted request's
+    arrays alive until its ticket has been waited for."""
+
+    def __init__(self, engine: Engine, scoring: Scoring, arena_bytes: int = 0, max_wave_tasks: int = 0,
+                 plain: bool = False, start_paused: bool = False):
+        self.lib = engine.lib
+        self.engine = engine
+        opts = abi.ServerOpts(arena_bytes, max_wave_tasks, int(plain), int(start_paused))
+        h = C.c_void_p()
+        _check(self.lib.swb_server_start(engine.h, C.byref(scoring), C.byref(opts), C.byref(h)), "swb_server_start")
+        self.h = h
+        self._keep = {}
+        self._lock = threading.Lock()
+
+    def submit(self, bases: np.ndarray, tasks: np.ndarray, out: Optional[np.ndarray] = None) -> int:
+        assert tasks.dtype == EXT_TASK_DTYPE
+        bases = np.ascontiguousarray(bases, dtype=np.uint8)
+        if out is None:
+            out = np.zeros(len(tasks), EXT_RESULT_DTYPE)
+        t = C.c_uint64()
+        _check(self.lib.swb_server_submit(self.h, ptr(bases), bases.size, tasks.ctypes.data, len(tasks),
+                                          out.ctypes.data, C.byref(t)), "swb_server_submit")
+        with self._lock:
+            self._keep[t.value] = (bases, tasks, out)
+        return t.value
+
+    def poll(self, ticket: int):
+        done, status = C.c_int(), C.c_int()
+        _check(self.lib.swb_server_poll(self.h, ticket, C.byref(done), C.byref(status)), "swb_server_poll")
+        return bool(done.value), status.value
+
+    def wait(self, ticket: int, timeout_ms: int = 60_000):
+        """-> (results array, submit_ns, done_ns); raises SWBError on timeout."""
+        status, s_ns, d_ns = C.c_int(), C.c_uint64(), C.c_uint64()
+        _check(self.lib.swb_server_wait(self.h, ticket, timeout_ms, C.byref(status), C.byref(s_ns), C.byref(d_ns)),
+               "swb_server_wait")
+        _check(status.value, "request")
+        with self._lock:
+            _, _, out = self._keep.pop(ticket)
+        return out, s_ns.value, d_ns.value
+
+    def resume(self):
+        _check(self.lib.swb_server_resume(self.h), "swb_server_resume")
+
+    def stats(self) -> dict:
+        st = abi.ServerStats()
+        _check(self.lib.swb_server_stats_get(self.h, C.byref(st)), "swb_server_stats_get")
+        return {f: getattr(st, f) for f, _ in abi.ServerStats._fields_}
+
+    def stop(self):
+        if self.h:
+            _check(self.lib.swb_server_stop(self.h), "swb_server_stop")
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass
+
+
+@dataclass
+class Request:
+    lo: int          # task range in the pool
+    hi: int
+    at: float        # arrival time (s from start)
+
+
+def request_stream(seed: int, n_pool: int, rate: float, duration: float, min_tasks=1_000,
+                   max_tasks=1_000_000) -> List[Request]:
+    """Poisson arrivals at `rate`/s for `duration` s; sizes log-uniform in
+    [min_tasks, max_tasks]; each request is a random contiguous slice of a
+    task pool of n_pool tasks."""
+    rng = np.random.default_rng(seed)
+    out, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration:
+            break
+        n = int(np.exp(rng.uniform(np.log(min_tasks), np.log(max_tasks))))
+        n = min(n, n_pool)
+        lo = int(rng.integers(0, n_pool - n + 1))
+        out.append(Request(lo, lo + n, t))
+    return out
+
+
+def slice_request(bases: np.ndarray, tasks: np.ndarray, lo: int, hi: int):
+    """A request's own (bases, tasks): the pool slice with offsets rebased to
+    its own bases buffer (targets from the resident reference keep theirs)."""
+    t = tasks[lo:hi].copy()
+    explicit = (t["flags"] & abi.SWB_T_FROM_REF) == 0
+    starts = [t["q_off"]] + ([t["t_off"][explicit]] if explicit.any() else [])
+    ends = [t["q_off"] + t["qlen"].astype(np.uint64)]
+    if explicit.any():
+        ends.append(t["t_off"][explicit] + t["tlen"][explicit].astype(np.uint64))
+    b0 = int(min(int(x.min()) for x in starts))
+    b1 = int(max(int(x.max()) for x in ends))
+    t["q_off"] -= np.uint64(b0)
+    t["t_off"][explicit] -= np.uint64(b0)
+    return bases[b0:max(b1, b0 + 1)], t
+
+
+def run_stream(server: Server, bases: np.ndarray, tasks: np.ndarray, reqs: List[Request], open_loop: bool = True):
+    """Submits the requests (at their arrival times when open_loop, else all at
+    once) and waits for them; returns per-request (n_tasks, latency_s) and the
+    makespan in seconds."""
+    prepared = [slice_request(bases, tasks, r.lo, r.hi) for r in reqs]
+    tickets = [None] * len(reqs)
+    lat = [None] * len(reqs)
+    t0 = time.perf_counter()
+
+    def submitter():
+        for k, r in enumerate(reqs):
+            if open_loop:
+                delay = r.at - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+            b, t = prepared[k]
+            tickets[k] = server.submit(b, t)
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    for k in range(len(reqs)):
+        while tickets[k] is None:
+            time.sleep(0.0002)
+        _, s_ns, d_ns = server.wait(tickets[k], timeout_ms=600_000)
+        lat[k] = (d_ns - s_ns) * 1e-9
+    th.join()
+    makespan = time.perf_counter() - t0
+    return [(r.hi - r.lo, lat[k]) for k, r in enumerate(reqs)], makespan

@@ -1,0 +1,103 @@
+"""The continuous-batching request loop (swb_server_*): every request's
+results are the same alone and in the mix, in served and plain mode; waits
+are bounded; admission waits for arena space; oversized requests are
+rejected at submit."""
+import numpy as np
+import pytest
+
+import gen
+from swiftbwa_b200 import abi
+from swiftbwa_b200.abi import Scoring
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def engine():
+    from swiftbwa_b200.alignment import Engine
+    from swiftbwa_b200.build import build
+    build()
+    e = Engine(0)
+    yield e
+    e.close()
+
+
+def _pool(engine, seed=31, n=6000):
+    d = gen.ext_tasks(seed, n, qmax=280, ref_len=8000)
+    engine.upload_reference(d["pac"], d["ref_bases"])
+    return d["bases"], d["tasks"]
+
+
+def _requests(n_pool, seed=7, k=40):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(k):
+        n = int(np.exp(rng.uniform(np.log(1), np.log(1500))))
+        lo = int(rng.integers(0, n_pool - n + 1))
+        out.append((lo, lo + n))
+    return out
+
+
+@pytest.mark.parametrize("plain", [False, True])
+def test_same_alone_and_in_mix(engine, plain):
+    from swiftbwa_b200.serving import Server, slice_request
+    sc = Scoring.default()
+    bases, tasks = _pool(engine)
+    reqs = [slice_request(bases, tasks, lo, hi) for lo, hi in _requests(len(tasks))]
+    alone = [engine.ext_batch(sc, b, t) for b, t in reqs]
+    # Small waves force large requests across several waves and both lanes.
+    srv = Server(engine, sc, arena_bytes=1 << 24, max_wave_tasks=700, plain=plain)
+    try:
+        tickets = [srv.submit(b, t) for b, t in reqs]
+        for k, tk in enumerate(tickets):
+            out, s_ns, d_ns = srv.wait(tk)
+            assert d_ns >= s_ns
+            assert np.array_equal(out, alone[k]), f"request {k} differs in the mix"
+        st = srv.stats()
+        assert st["completed"] == len(reqs) and st["tasks_completed"] == sum(len(t) for _, t in reqs)
+    finally:
+        srv.stop()
+
+
+def test_bounded_wait_and_resume(engine):
+    from swiftbwa_b200.alignment import SWBError
+    from swiftbwa_b200.serving import Server, slice_request
+    sc = Scoring.default()
+    bases, tasks = _pool(engine, seed=32, n=500)
+    b, t = slice_request(bases, tasks, 0, 500)
+    srv = Server(engine, sc, arena_bytes=1 << 22, start_paused=True)
+    try:
+        tk = srv.submit(b, t)
+        with pytest.raises(SWBError) as ei:
+            srv.wait(tk, timeout_ms=50)
+        assert ei.value.status == abi.SWB_ERR_TIMEOUT
+        assert srv.poll(tk)[0] is False
+        srv.resume()
+        out, _, _ = srv.wait(tk)
+        assert np.array_equal(out, engine.ext_batch(sc, b, t))
+        with pytest.raises(SWBError) as ei:
+            srv.poll(tk)          # released by the successful wait
+        assert ei.value.status == abi.SWB_ERR_NOT_FOUND
+    finally:
+        srv.stop()
+
+
+def test_admission_waits_for_arena_space(engine):
+    from swiftbwa_b200.serving import Server, slice_request
+    sc = Scoring.default()
+    bases, tasks = _pool(engine, seed=33, n=3000)
+    reqs = [slice_request(bases, tasks, lo, lo + 300) for lo in range(0, 3000, 300)]
+    need = max(b.size for b, _ in reqs)
+    srv = Server(engine, sc, arena_bytes=((need + 255) // 256) * 256 * 2, max_wave_tasks=1000)
+    try:
+        tickets = [srv.submit(b, t) for b, t in reqs]
+        for k, tk in enumerate(tickets):
+            out, _, _ = srv.wait(tk)
+            assert np.array_equal(out, engine.ext_batch(sc, *reqs[k]))
+        big = np.zeros(4 * need + 1024, np.uint8)
+        from swiftbwa_b200.alignment import SWBError
+        with pytest.raises(SWBError) as ei:
+            srv.submit(big, tasks[:1].copy())
+        assert ei.value.status == abi.SWB_ERR_TOO_LARGE
+    finally:
+        srv.stop()
