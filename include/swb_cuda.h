@@ -264,6 +264,47 @@ int swb_ext_batch_static(const swb_scoring *sc, const uint8_t *d_bases, const ui
                          const swb_ext_task *d_tasks, size_t n_tasks, swb_ext_result *d_out,
                          void *stream);
 
+/* ------------------------------------------ extension driver (whole chains) */
+/* MemSeed (Sources/BWACore/Seed.swift): rbeg in BWT coordinates
+ * [0, 2*genome_len). */
+typedef struct swb_seed {
+    int64_t rbeg;
+    int32_t qbeg, len, score;
+    int32_t reserved;
+} swb_seed;                 /* 24 bytes */
+
+/* One chain: seeds[seed_off .. seed_off+n_seeds) of the read
+ * bases[read_off .. read_off+read_len). */
+typedef struct swb_chain {
+    uint64_t read_off;
+    int32_t  read_len;
+    int32_t  rid;
+    uint32_t seed_off, n_seeds;
+} swb_chain;                /* 24 bytes */
+
+/* MemAlnReg fields ExtensionAligner.extend sets (AlignmentRegion.swift:19-75). */
+typedef struct swb_region {
+    int64_t rb, re;
+    int32_t qb, qe;
+    int32_t rid, score, true_score, sub, sub_n, w, seed_cov, seed_len0;
+} swb_region;               /* 56 bytes */
+
+/* ExtensionAligner.extend for many chains at once
+ * (Sources/Alignment/ExtensionAligner.swift:114-346), with targets fetched
+ * from the resident reference as FMIndex.getReference does
+ * (Sources/FMIndex/FMIndex.swift:147-170; the uploaded reference is the
+ * forward strand of length genome_len).  Chains advance in rounds: each
+ * round extends the next pending seed of every active chain on the GPU
+ * (left, its band retry, right, its band retry), so the covered-region
+ * skip, the retries and the left-to-right h0 chaining are the reference's.
+ * Chain c's regions are out[seed_off .. seed_off + n_regions[c]) (at most
+ * one region per seed).  *rounds (optional) receives the GPU batches run. */
+int swb_extend_chains(swb_ctx *ctx, const swb_scoring *sc,
+                      const uint8_t *bases, size_t n_bases,
+                      const swb_seed *seeds, size_t n_seeds,
+                      const swb_chain *chains, size_t n_chains, uint64_t genome_len,
+                      swb_region *out, uint32_t *n_regions, uint32_t *rounds);
+
 /* ------------------------------------------------ serving (continuous batching) */
 /* A request loop over one context's GPU for extension batches of differing
  * sizes that arrive concurrently (the actor loop of BWAMemAligner's
@@ -282,7 +323,10 @@ typedef struct swb_server swb_server;
 typedef struct swb_server_opts {
     size_t   arena_bytes;      /* device bytes for request bases (0 = 1 GiB)   */
     size_t   max_wave_tasks;   /* tasks per wave (0 = 1M)                      */
-    int32_t  plain;            /* 1 = one request per launch, no overlap       */
+    int32_t  plain;            /* 0 = served (waves, two lanes); 1 = one request
+                                  at a time through the binned launch sequence;
+                                  2 = one request at a time through the plain
+                                  single-launch kernel (swb_ext_batch_static)  */
     int32_t  start_paused;     /* 1 = admit nothing until swb_server_resume    */
 } swb_server_opts;
 typedef struct swb_server_stats {
@@ -291,7 +335,13 @@ typedef struct swb_server_stats {
     double   busy_ms;          /* summed wave device time                      */
 } swb_server_stats;
 int swb_server_start(swb_ctx *ctx, const swb_scoring *sc, const swb_server_opts *opts, swb_server **out);
-int swb_server_submit(swb_server *srv, const uint8_t *bases, size_t n_bases,
+/* Task offsets (q_off, and t_off of spans not in the reference) are
+ * relative to bases - span_origin: the byte a task addresses as x is
+ * bases[x - span_origin], so a request can be a slice of a larger pool
+ * without rebasing.  Pinned (cudaHostAlloc/registered) bases, tasks and out
+ * are copied asynchronously with no host-side pass; pageable ones work too,
+ * through bounce buffers. */
+int swb_server_submit(swb_server *srv, const uint8_t *bases, size_t n_bases, uint64_t span_origin,
                       const swb_ext_task *tasks, size_t n_tasks, swb_ext_result *out, uint64_t *ticket);
 /* *done = 1 once the ticket completed; *status = its result status. */
 int swb_server_poll(swb_server *srv, uint64_t ticket, int *done, int *status);

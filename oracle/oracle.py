@@ -89,6 +89,9 @@ def lib() -> C.CDLL:
                                        C.c_void_p, P(C.c_uint32), C.c_size_t, C.c_int,
                                        P(C.c_uint64)]
         L.orc_local_batch.argtypes = L.orc_ext_batch.argtypes
+        L.orc_extend_batch.argtypes = [P(Scoring), u8p, u8p, C.c_int64, C.c_void_p, C.c_void_p, C.c_size_t,
+                                       C.c_void_p, P(C.c_uint32), C.c_int, P(C.c_uint64)]
+        L.orc_extend_batch.restype = C.c_int
         _lib = L
     return _lib
 
@@ -248,3 +251,19 @@ def local_batch(sc: Scoring, bases: np.ndarray, tasks: np.ndarray, pac=None, ref
                                len(tasks), out.ctypes.data, n_threads, C.byref(cells))
     assert rc == 0
     return out, cells.value
+
+
+def extend_batch(sc: Scoring, bases: np.ndarray, pac: np.ndarray, genome_len: int, seeds: np.ndarray,
+                 chains: np.ndarray, n_threads: int = 1):
+    """ExtensionAligner.extend (FMIndex.getReference targets) for every chain
+    -> (regions array laid out like swb_extend_chains' output, counts, cells)."""
+    from swiftbwa_b200.abi import REGION_DTYPE
+    out = np.zeros(max(len(seeds), 1), REGION_DTYPE)
+    counts = np.zeros(max(len(chains), 1), np.uint32)
+    cells = C.c_uint64()
+    rc = lib().orc_extend_batch(C.byref(sc), ptr(bases), ptr(pac), genome_len, seeds.ctypes.data,
+                                chains.ctypes.data, len(chains), out.ctypes.data, ptr(counts, C.c_uint32),
+                                n_threads, C.byref(cells))
+    if rc != 0:
+        raise ValueError("extend_batch failed")
+    return out, counts[:len(chains)], cells.value

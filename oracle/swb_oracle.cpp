@@ -13,6 +13,7 @@
 #include "swb_oracle.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -1315,3 +1316,26 @@ int orc_local_batch(const swb_scoring *sc, const uint8_t *bases, const uint8_t *
 }
 
 }  // extern "C"
+
+int orc_extend_batch(const swb_scoring *sc, const uint8_t *bases, const uint8_t *pac, int64_t genome_len,
+                     const swb_seed *seeds, const swb_chain *chains, size_t n_chains,
+                     swb_region *out, uint32_t *n_regions, int n_threads, uint64_t *cells) {
+    static_assert(sizeof(orc_region) == sizeof(swb_region), "region layouts differ");
+    static_assert(sizeof(orc_seed) == sizeof(swb_seed), "seed layouts differ");
+    std::vector<uint64_t> per(std::max(n_threads, 1), 0);
+    std::atomic<int> bad{0};
+    parallel_for(n_chains, n_threads, [&](size_t lo, size_t hi, int tid) {
+        for (size_t c = lo; c < hi; ++c) {
+            const swb_chain &ch = chains[c];
+            uint64_t calls = 0, cl = 0;
+            const int n = orc_extend(reinterpret_cast<const orc_seed *>(seeds + ch.seed_off), (int32_t)ch.n_seeds,
+                                     ch.rid, bases + ch.read_off, ch.read_len, pac, genome_len, 1, sc,
+                                     reinterpret_cast<orc_region *>(out + ch.seed_off), (int32_t)ch.n_seeds, &calls, &cl);
+            if (n < 0) bad = 1;
+            n_regions[c] = (uint32_t)std::max(n, 0);
+            per[tid] += cl;
+        }
+    });
+    if (cells) { *cells = 0; for (auto v : per) *cells += v; }
+    return bad ? -1 : 0;
+}

@@ -115,6 +115,12 @@ int orc_local_batch(const swb_scoring *sc, const uint8_t *bases, const uint8_t *
                     uint64_t ref_bases, const swb_local_task *tasks, size_t n,
                     swb_local_result *out, int n_threads, uint64_t *cells);
 
+/* orc_extend (FMIndex.getReference targets) over many chains, in parallel:
+ * chain c's regions go to out[seed_off ..] and their number to n_regions[c]. */
+int orc_extend_batch(const swb_scoring *sc, const uint8_t *bases, const uint8_t *pac, int64_t genome_len,
+                     const swb_seed *seeds, const swb_chain *chains, size_t n_chains,
+                     swb_region *out, uint32_t *n_regions, int n_threads, uint64_t *cells);
+
 #ifdef __cplusplus
 }
 #endif

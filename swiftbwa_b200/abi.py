@@ -104,6 +104,13 @@ LOCAL_TASK_DTYPE = np.dtype([("q_off", "<u8"), ("t_off", "<u8"), ("qlen", "<i4")
 LOCAL_RESULT_DTYPE = np.dtype([("score", "<i4"), ("qb", "<i4"), ("qe", "<i4"),
                                ("tb", "<i4"), ("te", "<i4"), ("score2", "<i4")])
 
+SEED_DTYPE = np.dtype([("rbeg", "<i8"), ("qbeg", "<i4"), ("len", "<i4"), ("score", "<i4"), ("reserved", "<i4")])
+CHAIN_DTYPE = np.dtype([("read_off", "<u8"), ("read_len", "<i4"), ("rid", "<i4"), ("seed_off", "<u4"),
+                        ("n_seeds", "<u4")])
+REGION_DTYPE = np.dtype([("rb", "<i8"), ("re", "<i8"), ("qb", "<i4"), ("qe", "<i4"), ("rid", "<i4"),
+                         ("score", "<i4"), ("true_score", "<i4"), ("sub", "<i4"), ("sub_n", "<i4"), ("w", "<i4"),
+                         ("seed_cov", "<i4"), ("seed_len0", "<i4")])
+assert SEED_DTYPE.itemsize == 24 and CHAIN_DTYPE.itemsize == 24 and REGION_DTYPE.itemsize == 56
 assert EXT_TASK_DTYPE.itemsize == C.sizeof(ExtTask) == 40
 assert GLOBAL_TASK_DTYPE.itemsize == C.sizeof(GlobalTask) == 40
 assert LOCAL_TASK_DTYPE.itemsize == C.sizeof(LocalTask) == 32
@@ -120,7 +127,7 @@ EXPORTED_SYMBOLS = (
     "swb_kernel_launches", "swb_last_batch_stats", "swb_profile", "swb_profile_reset",
     "swb_profile_read", "swb_int_alu_peak", "swb_ext_batch_static", "swb_cigar_batch",
     "swb_server_start", "swb_server_submit", "swb_server_poll", "swb_server_wait", "swb_server_resume",
-    "swb_server_stats_get", "swb_server_stop",
+    "swb_server_stats_get", "swb_server_stop", "swb_extend_chains",
 )
 
 
@@ -211,12 +218,15 @@ def declare(lib: C.CDLL) -> C.CDLL:
                                     C.c_size_t, C.c_char_p, C.c_size_t]
     lib.swb_cigar_batch.restype = C.c_int
     lib.swb_server_start.argtypes = [vp, P(Scoring), P(ServerOpts), P(vp)]
-    lib.swb_server_submit.argtypes = [vp, u8p, C.c_size_t, vp, C.c_size_t, vp, P(C.c_uint64)]
+    lib.swb_server_submit.argtypes = [vp, u8p, C.c_size_t, C.c_uint64, vp, C.c_size_t, vp, P(C.c_uint64)]
     lib.swb_server_poll.argtypes = [vp, C.c_uint64, P(C.c_int), P(C.c_int)]
     lib.swb_server_wait.argtypes = [vp, C.c_uint64, C.c_int, P(C.c_int), P(C.c_uint64), P(C.c_uint64)]
     lib.swb_server_resume.argtypes = [vp]
     lib.swb_server_stats_get.argtypes = [vp, P(ServerStats)]
     lib.swb_server_stop.argtypes = [vp]
+    lib.swb_extend_chains.argtypes = [vp, P(Scoring), u8p, C.c_size_t, vp, C.c_size_t, vp, C.c_size_t, C.c_uint64,
+                                      vp, P(C.c_uint32), P(C.c_uint32)]
+    lib.swb_extend_chains.restype = C.c_int
     for f in ("swb_server_start", "swb_server_submit", "swb_server_poll", "swb_server_wait", "swb_server_resume",
               "swb_server_stats_get", "swb_server_stop"):
         getattr(lib, f).restype = C.c_int

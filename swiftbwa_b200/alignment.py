@@ -183,6 +183,24 @@ class Engine:
                 ref_pos, 0, 0)
         return self.cigar_batch(scoring, bases, t)[0]
 
+    def extend_chains(self, sc: Scoring, bases: np.ndarray, seeds: np.ndarray, chains: np.ndarray,
+                      genome_len: int):
+        """ExtensionAligner.extend for every chain (SEED_DTYPE seeds, CHAIN_DTYPE
+        chains) against the uploaded forward strand -> (REGION_DTYPE array,
+        per-chain region counts, GPU rounds).  Chain c's regions are
+        regions[seed_off : seed_off + counts[c]]."""
+        assert seeds.dtype == abi.SEED_DTYPE and chains.dtype == abi.CHAIN_DTYPE
+        bases = np.ascontiguousarray(bases, dtype=np.uint8)
+        if bases.size == 0:
+            bases = np.zeros(1, np.uint8)
+        out = np.zeros(max(len(seeds), 1), abi.REGION_DTYPE)
+        counts = np.zeros(max(len(chains), 1), np.uint32)
+        rounds = C.c_uint32()
+        _check(self.lib.swb_extend_chains(self.h, C.byref(sc), ptr(bases), bases.size, seeds.ctypes.data, len(seeds),
+                                          chains.ctypes.data, len(chains), genome_len, out.ctypes.data,
+                                          ptr(counts, C.c_uint32), C.byref(rounds)), "swb_extend_chains")
+        return out, counts[:len(chains)], rounds.value
+
     def last_batch_stats(self):
         ms, cells = C.c_double(), C.c_uint64()
         _check(self.lib.swb_last_batch_stats(self.h, C.byref(ms), C.byref(cells)), "stats")

@@ -9,16 +9,20 @@
 //     their space;
 //   * forms waves of at most max_wave_tasks tasks from the head of the
 //     queue, splitting large requests across waves so that small ones do not
-//     wait behind them, and rebases each task's offsets into the arena;
+//     wait behind them;
+//   * copies each piece of a wave straight from the caller's buffers when
+//     they are pinned (the task offsets are then rebased into the arena by a
+//     small kernel), or through a pinned bounce buffer when they are not;
 //   * runs a wave as one sort + binned extension pass over all its tasks
-//     (the same launch sequence as swb_ext_batch), alternating between two
-//     lanes -- internal contexts with their own streams and buffers sharing
-//     the resident reference -- so that one wave's copies and host staging
-//     overlap the other wave's kernels;
-//   * copies each request's slice of a wave's results straight into the
-//     caller's output and completes the request when its last slice lands.
-// plain mode is the baseline: one whole request per launch sequence, copy in,
-// compute, copy out, synchronise, next request.
+//     (the launch sequence of swb_ext_batch), alternating between two lanes
+//     -- internal contexts with their own streams and buffers sharing the
+//     resident reference -- so one wave's copies overlap the other's kernels;
+//   * copies each request's slice of a wave's results back (directly into a
+//     pinned output, through a bounce buffer otherwise) and completes the
+//     request when its last slice has landed.
+// plain = 1 is the baseline of the same kernels: one request at a time, copy
+// in, compute, copy out, synchronise.  plain = 2 also swaps the binned pass
+// for the plain single-launch kernel of swb_ext_batch_static.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -31,13 +35,14 @@
 
 #include "swb_internal.h"
 
-namespace swb {
-int ext_big_max_q(const swb_ext_task *tasks, size_t n, int max_mat);
-}
+extern "C" int swb_ext_batch_static(const swb_scoring *sc, const uint8_t *d_bases, const uint8_t *d_pac,
+                                    const swb_ext_task *d_tasks, size_t n_tasks, swb_ext_result *d_out, void *stream);
 
 using namespace swb;
 
 namespace {
+
+constexpr int kMaxPieces = 4096;   // pieces (request slices) per wave
 
 inline size_t align_up256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -47,13 +52,26 @@ uint64_t now_ns() {
         .count();
 }
 
+bool is_pinned(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 struct Req {
     uint64_t ticket = 0;
     const uint8_t *bases = nullptr;
     size_t n_bases = 0;
+    uint64_t origin = 0;
     const swb_ext_task *tasks = nullptr;
     size_t n = 0;
     swb_ext_result *out = nullptr;
+    bool tasks_pinned = false, out_pinned = false;
+    int max_q = 0;                       // longest query (sizes the int32 bin's scratch)
     size_t dispatched = 0, completed = 0;
     bool staged = false;
     size_t arena_off = 0, arena_len = 0;
@@ -67,6 +85,21 @@ struct Piece {
     size_t lo, hi, woff;
 };
 
+// Device-side rebase of one piece of a wave: q_off and explicit t_off += delta.
+struct RebasePiece {
+    unsigned long long woff, n, delta;
+};
+
+__global__ void rebase_kernel(swb_ext_task *__restrict__ t, const RebasePiece *__restrict__ pieces) {
+    const RebasePiece p = pieces[blockIdx.y];
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < p.n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        swb_ext_task &x = t[p.woff + i];
+        x.q_off += p.delta;
+        if (!(x.flags & SWB_T_FROM_REF)) x.t_off += p.delta;
+    }
+}
+
 // First-fit allocator over the device arena (offsets, 256-byte granules).
 struct Arena {
     size_t cap = 0;
@@ -77,7 +110,7 @@ struct Arena {
         free_[0] = c;
     }
     bool alloc(size_t len, size_t *off) {
-        len = (len + 255) & ~(size_t)255;
+        len = align_up256(len);
         for (auto it = free_.begin(); it != free_.end(); ++it)
             if (it->second >= len) {
                 *off = it->first;
@@ -89,7 +122,7 @@ struct Arena {
         return false;
     }
     void release(size_t off, size_t len) {
-        len = (len + 255) & ~(size_t)255;
+        len = align_up256(len);
         auto it = free_.emplace(off, len).first;
         auto nx = std::next(it);
         if (nx != free_.end() && it->first + it->second == nx->first) {
@@ -108,8 +141,11 @@ struct Arena {
 
 struct Lane {
     swb_ctx *ctx = nullptr;
-    swb_ext_task *h_stage = nullptr;              // pinned staging of the wave's tasks
-    unsigned long long *h_cells = nullptr;         // pinned copy of the wave's cell counters
+    swb_ext_task *h_stage = nullptr;        // pinned bounce buffer for pageable tasks
+    swb_ext_result *h_out = nullptr;        // pinned bounce buffer for pageable outputs
+    RebasePiece *h_pieces = nullptr;        // pinned piece table
+    RebasePiece *d_pieces = nullptr;
+    unsigned long long *h_cells = nullptr;  // pinned copy of the wave's cell counters
     cudaEvent_t ev_done = nullptr, ev_t0 = nullptr, ev_t1 = nullptr;
     bool busy = false;
     std::vector<Piece> pieces;
@@ -122,7 +158,7 @@ struct swb_server {
     swb_ctx *parent = nullptr;
     swb_scoring sc{};
     DevScoring dsc{};
-    bool plain = false;
+    int plain = 0;
     size_t max_wave = 1u << 20;
     uint8_t *d_arena = nullptr;
     Arena arena;
@@ -131,7 +167,7 @@ struct swb_server {
     std::thread worker;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
-    std::deque<Req *> queue;                        // admitted order; not yet fully dispatched or staged
+    std::deque<Req *> queue;
     std::unordered_map<uint64_t, Req *> reqs;
     uint64_t next_ticket = 1;
     bool stopping = false, paused = false;
@@ -153,6 +189,8 @@ void complete_wave(swb_server *s, Lane &L) {
     for (const Piece &p : L.pieces) {
         Req *r = p.r;
         if (L.launch_rc != SWB_OK) r->status = L.launch_rc;
+        if (!r->out_pinned && L.launch_rc == SWB_OK)
+            std::memcpy(r->out + p.lo, L.h_out + p.woff, (p.hi - p.lo) * sizeof(swb_ext_result));
         r->completed += p.hi - p.lo;
         s->stats.tasks_completed += p.hi - p.lo;
         if (r->completed == r->n) {
@@ -171,14 +209,21 @@ void complete_wave(swb_server *s, Lane &L) {
 // Forms and launches one wave on lane L.  Called with s->mu held; returns
 // false when nothing could be dispatched.
 bool launch_wave(swb_server *s, Lane &L) {
-    size_t wn = 0;
+    swb_ctx *c = L.ctx;
     // One copy stream for both lanes: a request split across waves on both
     // lanes has its bases copied once, and every later wave's task copy (and
     // so its kernels) is ordered after that copy.
-    cudaStream_t h2d = s->lanes[0].ctx->h2d, st = L.ctx->stream, d2h = L.ctx->d2h;
-    // Stage bases and tasks in arrival order.
+    cudaStream_t h2d = s->lanes[0].ctx->h2d, st = c->stream, d2h = c->d2h;
+    if (ensure_dev(c, c->d_tasks, s->max_wave * sizeof(swb_ext_task)) ||
+        ensure_dev(c, c->d_out, s->max_wave * sizeof(swb_ext_result)))
+        return false;
+    swb_ext_task *d_tasks = (swb_ext_task *)c->d_tasks.p;
+    swb_ext_result *d_out = (swb_ext_result *)c->d_out.p;
+    size_t wn = 0;
+    int npin = 0;
+    bool host_staged = false;
     for (Req *r : s->queue) {
-        if (wn >= s->max_wave) break;
+        if (wn >= s->max_wave || (int)L.pieces.size() >= kMaxPieces) break;
         if (r->dispatched == r->n) continue;
         if (!r->staged) {
             size_t off = 0;
@@ -186,15 +231,21 @@ bool launch_wave(swb_server *s, Lane &L) {
             r->arena_off = off;
             r->arena_len = std::max<size_t>(r->n_bases, 1);
             r->staged = true;
-            if (r->n_bases)
-                cudaMemcpyAsync(s->d_arena + off, r->bases, r->n_bases, cudaMemcpyHostToDevice, h2d);
+            if (r->n_bases) cudaMemcpyAsync(s->d_arena + off, r->bases, r->n_bases, cudaMemcpyHostToDevice, h2d);
         }
         const size_t take = std::min(r->n - r->dispatched, s->max_wave - wn);
-        for (size_t k = 0; k < take; ++k) {
-            swb_ext_task t = r->tasks[r->dispatched + k];
-            t.q_off += r->arena_off;
-            if (!(t.flags & SWB_T_FROM_REF)) t.t_off += r->arena_off;
-            L.h_stage[wn + k] = t;
+        const unsigned long long delta = (unsigned long long)r->arena_off - (unsigned long long)r->origin;
+        if (r->tasks_pinned) {
+            cudaMemcpyAsync(d_tasks + wn, r->tasks + r->dispatched, take * sizeof(swb_ext_task), cudaMemcpyHostToDevice, h2d);
+            L.h_pieces[npin++] = RebasePiece{wn, take, delta};
+        } else {
+            for (size_t k = 0; k < take; ++k) {
+                swb_ext_task t = r->tasks[r->dispatched + k];
+                t.q_off += delta;
+                if (!(t.flags & SWB_T_FROM_REF)) t.t_off += delta;
+                L.h_stage[wn + k] = t;
+            }
+            host_staged = true;
         }
         L.pieces.push_back(Piece{r, r->dispatched, r->dispatched + take, wn});
         r->dispatched += take;
@@ -202,31 +253,49 @@ bool launch_wave(swb_server *s, Lane &L) {
         if (s->plain) break;
     }
     if (wn == 0) return false;
-    swb_ctx *c = L.ctx;
-    int rc = ensure_dev(c, c->d_tasks, wn * sizeof(swb_ext_task));
-    if (!rc) rc = ensure_dev(c, c->d_out, wn * sizeof(swb_ext_result));
-    if (!rc && cudaMemcpyAsync(c->d_tasks.p, L.h_stage, wn * sizeof(swb_ext_task), cudaMemcpyHostToDevice, h2d) != cudaSuccess)
-        rc = SWB_ERR_CUDA;
+    int rc = SWB_OK;
+    if (host_staged)
+        for (const Piece &p : L.pieces)
+            if (!p.r->tasks_pinned &&
+                cudaMemcpyAsync(d_tasks + p.woff, L.h_stage + p.woff, (p.hi - p.lo) * sizeof(swb_ext_task),
+                                cudaMemcpyHostToDevice, h2d) != cudaSuccess)
+                rc = SWB_ERR_CUDA;
+    if (!rc && npin) {
+        cudaMemcpyAsync(L.d_pieces, L.h_pieces, npin * sizeof(RebasePiece), cudaMemcpyHostToDevice, h2d);
+        size_t maxn = 0;
+        for (int k = 0; k < npin; ++k) maxn = std::max<size_t>(maxn, L.h_pieces[k].n);
+        const dim3 grid((unsigned)std::min<size_t>((maxn + 255) / 256, 1024), (unsigned)npin);
+        rebase_kernel<<<grid, 256, 0, h2d>>>(d_tasks, L.d_pieces);
+        c->launches++;
+        if (cudaGetLastError() != cudaSuccess) rc = SWB_ERR_CUDA;
+    }
     if (!rc && cudaEventRecord(c->chunk_in[0], h2d) != cudaSuccess) rc = SWB_ERR_CUDA;
     if (!rc && cudaStreamWaitEvent(st, c->chunk_in[0], 0) != cudaSuccess) rc = SWB_ERR_CUDA;
     if (!rc) cudaMemsetAsync(c->d_counters, 0, sizeof(unsigned long long) * kNumCounters, st);
     if (!rc) cudaEventRecord(L.ev_t0, st);
-    if (!rc)
-        rc = launch_ext(c, s->dsc, s->d_arena, (const swb_ext_task *)c->d_tasks.p, wn, (swb_ext_result *)c->d_out.p,
-                        c->d_counters, st, ext_big_max_q(L.h_stage, wn, s->dsc.max_mat));
+    if (!rc) {
+        if (s->plain == 2) {
+            rc = swb_ext_batch_static(&s->sc, s->d_arena, c->d_pac, d_tasks, wn, d_out, st);
+        } else {
+            // The int32 bin's scratch is sized from the longest query of the
+            // wave's requests (an upper bound of the bin's), known since submit.
+            int max_q = 0;
+            for (const Piece &p : L.pieces) max_q = std::max(max_q, p.r->max_q);
+            rc = launch_ext(c, s->dsc, s->d_arena, d_tasks, wn, d_out, c->d_counters, st, max_q);
+        }
+    }
     if (!rc) cudaEventRecord(L.ev_t1, st);
     if (!rc && cudaEventRecord(c->chunk_done[0], st) != cudaSuccess) rc = SWB_ERR_CUDA;
     if (!rc && cudaStreamWaitEvent(d2h, c->chunk_done[0], 0) != cudaSuccess) rc = SWB_ERR_CUDA;
     if (!rc) {
         for (const Piece &p : L.pieces)
-            cudaMemcpyAsync(p.r->out + p.lo, (swb_ext_result *)c->d_out.p + p.woff, (p.hi - p.lo) * sizeof(swb_ext_result),
-                            cudaMemcpyDeviceToHost, d2h);
+            cudaMemcpyAsync(p.r->out_pinned ? p.r->out + p.lo : L.h_out + p.woff, d_out + p.woff,
+                            (p.hi - p.lo) * sizeof(swb_ext_result), cudaMemcpyDeviceToHost, d2h);
         cudaMemcpyAsync(L.h_cells, c->d_counters, sizeof(unsigned long long) * kNumCounters, cudaMemcpyDeviceToHost, d2h);
     }
     L.launch_rc = rc;
     cudaEventRecord(L.ev_done, rc ? st : d2h);
     L.busy = true;
-    // Fully dispatched requests leave the queue (they complete through their pieces).
     while (!s->queue.empty() && s->queue.front()->dispatched == s->queue.front()->n) s->queue.pop_front();
     return true;
 }
@@ -282,11 +351,12 @@ int swb_server_start(swb_ctx *ctx, const swb_scoring *sc, const swb_server_opts 
     *out = nullptr;
     swb_server_opts o{};
     if (opts) o = *opts;
+    if (o.plain < 0 || o.plain > 2) return set_error(SWB_ERR_INVALID_ARG, "plain must be 0, 1 or 2");
     auto *s = new swb_server();
     s->parent = ctx;
     s->sc = *sc;
     s->dsc = make_dev_scoring(*sc);
-    s->plain = o.plain != 0;
+    s->plain = o.plain;
     s->paused = o.start_paused != 0;
     s->max_wave = o.max_wave_tasks ? o.max_wave_tasks : (1u << 20);
     const size_t arena = o.arena_bytes ? o.arena_bytes : ((size_t)1 << 30);
@@ -303,6 +373,9 @@ int swb_server_start(swb_ctx *ctx, const swb_scoring *sc, const swb_server_opts 
         L.ctx->pac_owned = false;
         L.ctx->ref_bases = ctx->ref_bases;
         if (cudaMallocHost(&L.h_stage, s->max_wave * sizeof(swb_ext_task)) != cudaSuccess ||
+            cudaMallocHost(&L.h_out, s->max_wave * sizeof(swb_ext_result)) != cudaSuccess ||
+            cudaMallocHost(&L.h_pieces, kMaxPieces * sizeof(RebasePiece)) != cudaSuccess ||
+            cudaMalloc(&L.d_pieces, kMaxPieces * sizeof(RebasePiece)) != cudaSuccess ||
             cudaMallocHost(&L.h_cells, sizeof(unsigned long long) * kNumCounters) != cudaSuccess ||
             cudaEventCreateWithFlags(&L.ev_done, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreate(&L.ev_t0) != cudaSuccess || cudaEventCreate(&L.ev_t1) != cudaSuccess)
@@ -311,6 +384,9 @@ int swb_server_start(swb_ctx *ctx, const swb_scoring *sc, const swb_server_opts 
     if (rc) {
         for (Lane &L : s->lanes) {
             if (L.h_stage) cudaFreeHost(L.h_stage);
+            if (L.h_out) cudaFreeHost(L.h_out);
+            if (L.h_pieces) cudaFreeHost(L.h_pieces);
+            if (L.d_pieces) cudaFree(L.d_pieces);
             if (L.h_cells) cudaFreeHost(L.h_cells);
             if (L.ctx) swb_destroy(L.ctx);
         }
@@ -323,28 +399,36 @@ int swb_server_start(swb_ctx *ctx, const swb_scoring *sc, const swb_server_opts 
     return SWB_OK;
 }
 
-int swb_server_submit(swb_server *s, const uint8_t *bases, size_t n_bases, const swb_ext_task *tasks, size_t n_tasks,
-                      swb_ext_result *out, uint64_t *ticket) {
+int swb_server_submit(swb_server *s, const uint8_t *bases, size_t n_bases, uint64_t span_origin,
+                      const swb_ext_task *tasks, size_t n_tasks, swb_ext_result *out, uint64_t *ticket) {
     if (!s || !ticket || (!bases && n_bases) || (!tasks && n_tasks) || (!out && n_tasks))
         return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
     if (align_up256(std::max<size_t>(n_bases, 1)) > s->arena.cap)
         return set_error(SWB_ERR_TOO_LARGE, "request bases exceed the server arena");
     // Span validation against the request's own buffer and the reference.
+    const uint64_t lo = span_origin, hi = span_origin + n_bases;
+    int max_q = 0;
     for (size_t i = 0; i < n_tasks; ++i) {
         const swb_ext_task &t = tasks[i];
+        max_q = std::max(max_q, t.qlen);
         const bool bad_len = t.qlen < 0 || t.tlen < 0 || t.qlen > kMaxLen || t.tlen > kMaxLen;
-        const bool bad_q = t.qlen > 0 && t.q_off + (uint64_t)t.qlen > n_bases;
-        const bool bad_t = t.tlen > 0 && ((t.flags & SWB_T_FROM_REF) ? (!s->parent->d_pac || t.t_off + (uint64_t)t.tlen > s->parent->ref_bases)
-                                                                   : t.t_off + (uint64_t)t.tlen > n_bases);
+        const bool bad_q = t.qlen > 0 && (t.q_off < lo || t.q_off + (uint64_t)t.qlen > hi);
+        const bool bad_t = t.tlen > 0 && ((t.flags & SWB_T_FROM_REF)
+                                              ? (!s->parent->d_pac || t.t_off + (uint64_t)t.tlen > s->parent->ref_bases)
+                                              : (t.t_off < lo || t.t_off + (uint64_t)t.tlen > hi));
         if (bad_len || bad_q || bad_t)
             return set_error(bad_len ? SWB_ERR_TOO_LARGE : SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": bad span or length");
     }
     auto *r = new Req();
     r->bases = bases;
     r->n_bases = n_bases;
+    r->origin = span_origin;
     r->tasks = tasks;
     r->n = n_tasks;
     r->out = out;
+    r->max_q = max_q;
+    r->tasks_pinned = is_pinned(tasks);
+    r->out_pinned = is_pinned(out);
     r->t_submit = now_ns();
     {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -427,11 +511,15 @@ int swb_server_stop(swb_server *s) {
         if (L.ctx) {
             cudaStreamSynchronize(L.ctx->stream);
             cudaStreamSynchronize(L.ctx->d2h);
+            cudaStreamSynchronize(L.ctx->h2d);
         }
         if (L.ev_done) cudaEventDestroy(L.ev_done);
         if (L.ev_t0) cudaEventDestroy(L.ev_t0);
         if (L.ev_t1) cudaEventDestroy(L.ev_t1);
         if (L.h_stage) cudaFreeHost(L.h_stage);
+        if (L.h_out) cudaFreeHost(L.h_out);
+        if (L.h_pieces) cudaFreeHost(L.h_pieces);
+        if (L.d_pieces) cudaFree(L.d_pieces);
         if (L.h_cells) cudaFreeHost(L.h_cells);
         if (L.ctx) swb_destroy(L.ctx);
     }

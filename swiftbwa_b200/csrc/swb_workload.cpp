@@ -363,4 +363,72 @@ void swbw_rescue_tasks(uint64_t seed, const uint8_t *ref, int64_t ref_len, int64
     });
 }
 
+// Seed chains for ExtensionAligner.extend: n reads of read_len bases, each
+// from a random position of either strand of the genome (BWT coordinates,
+// [0, 2*gl): positions >= gl read the reverse complement), with errors.  A
+// chain's seeds are the clean runs of at least min_seed bases at the read's
+// true location (up to max_seeds, in read order, score = len * a), plus with
+// probability spurious_frac one extra seed of the read placed at a random
+// offset of up to +-200 bases.  Reads go to bases_out (n * read_len); seeds
+// are compacted in chain order.  Returns the number of seeds.
+int64_t swbw_chains(uint64_t seed, const uint8_t *ref, int64_t gl, int64_t n, int read_len, double sub, double indel,
+                    double n_rate, int min_seed, int max_seeds, int a, double spurious_frac, uint8_t *bases_out,
+                    swb_seed *seeds_out, swb_chain *chains_out) {
+    std::vector<uint32_t> cnt((size_t)n, 0);
+    chunked((size_t)n, 4096, [&](size_t ci, size_t lo, size_t hi) {
+        Rng r(chunk_seed(seed, ci));
+        ReadSim rs;
+        std::vector<uint8_t> win;
+        const int span = read_len + 64;
+        for (size_t i = lo; i < hi; ++i) {
+            const bool rev = r.uniform() < 0.5;
+            const int64_t fpos = (int64_t)r.below((uint64_t)std::max<int64_t>(1, gl - span));
+            int64_t p0;                                         // BWT coordinate of win[0]
+            win.resize((size_t)span);
+            if (!rev) {
+                p0 = fpos;
+                std::memcpy(win.data(), ref + fpos, (size_t)span);
+            } else {                                            // reverse complement of ref[fpos, fpos+span)
+                p0 = 2 * gl - (fpos + span);
+                for (int k = 0; k < span; ++k) win[(size_t)k] = (uint8_t)(3 - ref[fpos + span - 1 - k]);
+            }
+            simulate_read(r, win.data(), span, 0, read_len, sub, indel, n_rate, rs);
+            std::memcpy(bases_out + i * (size_t)read_len, rs.bases.data(), (size_t)read_len);
+            swb_seed *sd = seeds_out + i * (size_t)(max_seeds + 1);
+            uint32_t m = 0;
+            int run = 0;
+            for (int k = 0; k <= read_len; ++k) {
+                const bool ok = k < read_len && rs.clean[(size_t)k] && rs.rpos[(size_t)k] < span &&
+                                (run == 0 || rs.rpos[(size_t)k] == rs.rpos[(size_t)k - 1] + 1);
+                if (ok) {
+                    ++run;
+                    continue;
+                }
+                if (run >= min_seed && (int)m < max_seeds) {
+                    const int qb = k - run;
+                    sd[m++] = swb_seed{p0 + rs.rpos[(size_t)qb], qb, run, run * a, 0};
+                }
+                run = (k < read_len && rs.clean[(size_t)k] && rs.rpos[(size_t)k] < span) ? 1 : 0;
+            }
+            if (m > 0 && r.uniform() < spurious_frac) {
+                const swb_seed &b = sd[r.below(m)];
+                int64_t rb = b.rbeg + r.range(-200, 200);
+                const int64_t lo_b = rev ? gl : 0, hi_b = rev ? 2 * gl - b.len : gl - b.len;
+                rb = std::min(std::max(rb, lo_b), hi_b);
+                sd[m++] = swb_seed{rb, b.qbeg, b.len, b.len * a, 0};
+            }
+            cnt[i] = m;
+            chains_out[i] = swb_chain{i * (uint64_t)read_len, read_len, (int32_t)(i & 0x7fffffff), 0, m};
+        }
+    });
+    uint64_t off = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        const swb_seed *src = seeds_out + (size_t)i * (size_t)(max_seeds + 1);
+        if (src != seeds_out + off) std::memmove(seeds_out + off, src, cnt[(size_t)i] * sizeof(swb_seed));
+        chains_out[i].seed_off = (uint32_t)off;
+        off += cnt[(size_t)i];
+    }
+    return (int64_t)off;
+}
+
 }  // extern "C"

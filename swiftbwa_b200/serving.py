@@ -21,7 +21,7 @@ class Server:
     arrays alive until its ticket has been waited for."""
 
     def __init__(self, engine: Engine, scoring: Scoring, arena_bytes: int = 0, max_wave_tasks: int = 0,
-                 plain: bool = False, start_paused: bool = False):
+                 plain: int = 0, start_paused: bool = False):
         self.lib = engine.lib
         self.engine = engine
         opts = abi.ServerOpts(arena_bytes, max_wave_tasks, int(plain), int(start_paused))
@@ -31,14 +31,16 @@ class Server:
         self._keep = {}
         self._lock = threading.Lock()
 
-    def submit(self, bases: np.ndarray, tasks: np.ndarray, out: Optional[np.ndarray] = None) -> int:
-        assert tasks.dtype == EXT_TASK_DTYPE
+    def submit(self, bases: np.ndarray, tasks: np.ndarray, out: Optional[np.ndarray] = None,
+               span_origin: int = 0) -> int:
+        """Queue one request; task offsets address bases[x - span_origin]."""
+        assert tasks.dtype == EXT_TASK_DTYPE and tasks.flags["C_CONTIGUOUS"]
         bases = np.ascontiguousarray(bases, dtype=np.uint8)
         if out is None:
             out = np.zeros(len(tasks), EXT_RESULT_DTYPE)
         t = C.c_uint64()
-        _check(self.lib.swb_server_submit(self.h, ptr(bases), bases.size, tasks.ctypes.data, len(tasks),
-                                          out.ctypes.data, C.byref(t)), "swb_server_submit")
+        _check(self.lib.swb_server_submit(self.h, ptr(bases), bases.size, span_origin, tasks.ctypes.data,
+                                          len(tasks), out.ctypes.data, C.byref(t)), "swb_server_submit")
         with self._lock:
             self._keep[t.value] = (bases, tasks, out)
         return t.value
@@ -119,11 +121,20 @@ def slice_request(bases: np.ndarray, tasks: np.ndarray, lo: int, hi: int):
     return bases[b0:max(b1, b0 + 1)], t
 
 
-def run_stream(server: Server, bases: np.ndarray, tasks: np.ndarray, reqs: List[Request], open_loop: bool = True):
-    """Submits the requests (at their arrival times when open_loop, else all at
-    once) and waits for them; returns per-request (n_tasks, latency_s) and the
-    makespan in seconds."""
-    prepared = [slice_request(bases, tasks, r.lo, r.hi) for r in reqs]
+def pool_request(bases: np.ndarray, tasks: np.ndarray, out: np.ndarray, lo: int, hi: int):
+    """Zero-copy request over a pool whose queries are laid out in task order
+    and whose targets are reference spans: (bases slice, span_origin, tasks
+    slice, out slice), all views of the pool arrays."""
+    q0 = int(tasks["q_off"][lo])
+    q1 = int(tasks["q_off"][hi - 1]) + int(tasks["qlen"][hi - 1])
+    return bases[q0:max(q1, q0 + 1)], q0, tasks[lo:hi], out[lo:hi]
+
+
+def run_pool_stream(server: Server, bases: np.ndarray, tasks: np.ndarray, out: np.ndarray, reqs: List[Request],
+                    open_loop: bool = True):
+    """Like run_stream for a pool of reference-target tasks with queries in
+    task order; requests are views of the (ideally pinned) pool arrays, so the
+    submitter does no host work besides the call."""
     tickets = [None] * len(reqs)
     lat = [None] * len(reqs)
     t0 = time.perf_counter()
@@ -134,7 +145,43 @@ def run_stream(server: Server, bases: np.ndarray, tasks: np.ndarray, reqs: List[
                 delay = r.at - (time.perf_counter() - t0)
                 if delay > 0:
                     time.sleep(delay)
-            b, t = prepared[k]
+            b, origin, t, o = pool_request(bases, tasks, out, r.lo, r.hi)
+            tickets[k] = server.submit(b, t, o, span_origin=origin)
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    for k in range(len(reqs)):
+        while tickets[k] is None:
+            time.sleep(0.0002)
+        _, s_ns, d_ns = server.wait(tickets[k], timeout_ms=600_000)
+        lat[k] = (d_ns - s_ns) * 1e-9
+    th.join()
+    makespan = time.perf_counter() - t0
+    return [(r.hi - r.lo, lat[k]) for k, r in enumerate(reqs)], makespan
+
+
+def run_stream(server: Server, bases: np.ndarray, tasks: np.ndarray, reqs: List[Request], open_loop: bool = True):
+    """Submits the requests (at their arrival times when open_loop, else all at
+    once) and waits for them; returns per-request (n_tasks, latency_s) and the
+    makespan in seconds."""
+    # Closed loop: every request prepared up front, then submitted at once.
+    # Open loop: each request is prepared just before its arrival time, so
+    # host memory holds only the requests in flight.
+    prepared = [slice_request(bases, tasks, r.lo, r.hi) for r in reqs] if not open_loop else None
+    tickets = [None] * len(reqs)
+    lat = [None] * len(reqs)
+    t0 = time.perf_counter()
+
+    def submitter():
+        for k, r in enumerate(reqs):
+            if open_loop:
+                b, t = slice_request(bases, tasks, r.lo, r.hi)
+                delay = r.at - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+            else:
+                b, t = prepared[k]
+                prepared[k] = None
             tickets[k] = server.submit(b, t)
 
     th = threading.Thread(target=submitter)

@@ -14,7 +14,7 @@ from typing import Optional
 
 import numpy as np
 
-from .abi import EXT_TASK_DTYPE, GLOBAL_TASK_DTYPE, LOCAL_TASK_DTYPE, SWB_GLB_RETRY
+from .abi import CHAIN_DTYPE, EXT_TASK_DTYPE, GLOBAL_TASK_DTYPE, LOCAL_TASK_DTYPE, SEED_DTYPE, SWB_GLB_RETRY
 from .build import WORKLOAD_OUT, build_workload
 
 SEED_BASE = 0x5EED0000
@@ -39,6 +39,8 @@ def lib() -> C.CDLL:
         L.swbw_uneven_tasks.restype = i64
         L.swbw_rescue_tasks.argtypes = [u64, vp, i64, i64, i32, i32, dbl, dbl, dbl, dbl, i32, vp, vp]
         L.swbw_rescue_tasks.restype = None
+        L.swbw_chains.argtypes = [u64, vp, i64, i64, i32, dbl, dbl, dbl, i32, i32, i32, dbl, vp, vp, vp]
+        L.swbw_chains.restype = i64
         _lib = L
     return _lib
 
@@ -172,3 +174,36 @@ def config3(rank: int = 0, n: int = 2_000_000, ref_len: int = 100_000_000) -> Re
     lib().swbw_rescue_tasks(SEED_BASE + 3 + 1000 * rank + 1, ref.codes.ctypes.data, ref.n, n, 150, 700, 400.0,
                             50.0, 0.02, 0.10, 19, bases.ctypes.data, tasks.ctypes.data)
     return RescueWorkload(ref, bases, tasks, f"config3: {n} mate-rescue local SW, 150 bp vs 700 bp")
+
+
+@dataclass
+class ChainWorkload:
+    ref: Reference
+    bases: np.ndarray          # reads, read_len bytes each
+    seeds: np.ndarray          # SEED_DTYPE, BWT coordinates [0, 2 * ref.n)
+    chains: np.ndarray         # CHAIN_DTYPE, one chain per read
+    read_len: int
+    name: str = ""
+
+
+def chains(ref: Reference, seed: int, n_reads: int, read_len: int = 150, *, sub=0.01, indel=0.001, n_rate=0.005,
+           min_seed=19, max_seeds=6, a=1, spurious_frac=0.1) -> ChainWorkload:
+    """One seed chain per read for ExtensionAligner.extend: reads from either
+    strand with errors; seeds = the clean runs of >= min_seed bases at the
+    true location (score len * a), plus an offset copy of one of them in a
+    fraction spurious_frac of chains."""
+    bases = np.empty(n_reads * read_len, np.uint8)
+    seeds = np.empty(n_reads * (max_seeds + 1), SEED_DTYPE)
+    ch = np.empty(n_reads, CHAIN_DTYPE)
+    ns = lib().swbw_chains(seed, ref.codes.ctypes.data, ref.n, n_reads, read_len, sub, indel, n_rate, min_seed,
+                           max_seeds, a, spurious_frac, bases.ctypes.data, seeds.ctypes.data, ch.ctypes.data)
+    return ChainWorkload(ref, bases, seeds[:ns].copy(), ch, read_len)
+
+
+def config5(rank: int = 0, n_reads: int = 1_000_000, ref_len: int = 100_000_000) -> ChainWorkload:
+    """ExtensionAligner.extend over 1M seed chains of 150 bp reads (both
+    strands, config-1 error rates) off a 100 Mbp reference."""
+    ref = reference(SEED_BASE + 5 + 1000 * rank, ref_len)
+    wl = chains(ref, SEED_BASE + 5 + 1000 * rank + 1, n_reads, 150)
+    wl.name = f"config5: {n_reads} seed chains of 150 bp reads ({len(wl.seeds)} seeds), {ref_len // 10**6} Mbp reference"
+    return wl

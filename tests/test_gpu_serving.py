@@ -101,3 +101,35 @@ def test_admission_waits_for_arena_space(engine):
         assert ei.value.status == abi.SWB_ERR_TOO_LARGE
     finally:
         srv.stop()
+
+
+@pytest.mark.parametrize("plain", [0, 2])
+def test_pinned_zero_copy_pool(engine, plain):
+    """Requests as views of a pinned pool (span_origin, device-side rebase),
+    served and through the plain single-launch kernel: same as alone."""
+    torch = pytest.importorskip("torch")
+    from swiftbwa_b200 import workloads as W
+    from swiftbwa_b200.abi import EXT_RESULT_DTYPE
+    from swiftbwa_b200.serving import Server, pool_request
+    sc = Scoring.default()
+    ref = W.reference(W.SEED_BASE + 9, 2_000_000)
+    engine.upload_reference(ref.pac, ref.n)
+    pool = W.uneven(ref, 99, 40_000)
+    pb = torch.from_numpy(pool.bases).pin_memory().numpy()
+    pt = torch.from_numpy(pool.tasks.view(np.uint8)).pin_memory().numpy().view(pool.tasks.dtype)
+    po = torch.zeros(len(pool.tasks) * EXT_RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy().view(EXT_RESULT_DTYPE)
+    expected = engine.ext_batch(sc, pool.bases, pool.tasks)
+    rng = np.random.default_rng(3)
+    cuts = np.sort(rng.choice(np.arange(1, len(pool.tasks)), 30, replace=False))
+    bounds = list(zip([0, *cuts], [*cuts, len(pool.tasks)]))     # disjoint requests covering the pool
+    srv = Server(engine, sc, arena_bytes=1 << 26, max_wave_tasks=5000, plain=plain)
+    try:
+        tickets = []
+        for lo, hi in bounds:
+            b, origin, t, o = pool_request(pb, pt, po, int(lo), int(hi))
+            tickets.append(srv.submit(b, t, o, span_origin=origin))
+        for tk in tickets:
+            srv.wait(tk)
+    finally:
+        srv.stop()
+    assert np.array_equal(po, expected)
