@@ -277,24 +277,33 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True):
     ct["initial_w"] = 100
     ct["ref_pos"] = info[:, 0]
     ct["flags"] = 0x8
-    eng.cigar_batch(sc, wl1.bases, ct[:1000])
+    eng.cigar_batch_raw(sc, wl1.bases, ct[:1000])
+    eng.profile(True)
+    eng.profile_reset()
     t0 = time.perf_counter()
-    cg = eng.cigar_batch(sc, wl1.bases, ct)
+    cres, ccig, cmd = eng.cigar_batch_raw(sc, wl1.bases, ct)
     e2e1 = time.perf_counter() - t0
     ms1, cells1 = eng.last_batch_stats()
-    n_dp = int(sum(1 for x in cg if x["used_dp"]))
-    c1 = {"reads": len(ct), "dp_alignments": n_dp, "cigars_per_s": len(ct) / e2e1, "nw_kernel_ms": ms1,
-          "nw_gcups": cells1 / ms1 / 1e6 if ms1 else None, "nw_alignments_per_s": n_dp / ms1 * 1e3 if ms1 else None}
+    prof1 = eng.profile_read()
+    eng.profile(False)
+    n_dp = int(cres["used_dp"].sum())
+    c1 = {"reads": len(ct), "dp_alignments": n_dp, "cigars_per_s": len(ct) / e2e1, "wall_ms": e2e1 * 1e3,
+          "nw_kernel_ms": ms1, "nw_gcups": cells1 / ms1 / 1e6 if ms1 else None,
+          "nw_alignments_per_s": n_dp / ms1 * 1e3 if ms1 else None,
+          "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof1.items()}}
     if cpu_on:
         s1 = 3000
         t0 = time.perf_counter()
         ok = 0
+        mdb = cmd.tobytes()
         for k in range(s1):
             q = wl1.bases[k * L:(k + 1) * L]
             r = wl1.ref.codes[int(ct["t_off"][k]): int(ct["t_off"][k]) + int(ct["rlen"][k])]
             e = oracle.cigar_generate(q, r, 0, L, L, False, int(ct["true_score"][k]), 100, sc, int(ct["ref_pos"][k]))
-            g = cg[k]
-            ok += (e["cigar"], e["nm"], e["md"], e["score"], e["pos"]) == (g["cigar"], g["nm"], g["md"], g["score"], g["pos"])
+            g = cres[k]
+            o, n, mo, ml = int(g["cigar_off"]), int(g["n_cigar"]), int(g["md_off"]), int(g["md_len"])
+            ok += (e["cigar"], e["nm"], e["md"], e["score"], e["pos"]) == (
+                [int(x) for x in ccig[o:o + n]], int(g["nm"]), mdb[mo:mo + ml].decode(), int(g["score"]), int(g["pos"]))
         c1["cpu_baseline"] = {"value": s1 / (time.perf_counter() - t0), "unit": "cigars/s", "cores": 1, "kind": "port",
                               "sample": f"first {s1} reads, one thread (per-call Python loop)"}
         c1["bitexact_sample"] = f"{ok}/{s1}"

@@ -147,24 +147,31 @@ class Engine:
                "swb_local_batch")
         return out
 
-    def cigar_batch(self, sc: Scoring, bases: np.ndarray, tasks: np.ndarray):
-        """CIGARGenerator.generate over CIGAR_TASK_DTYPE tasks -> list of dicts
-        (cigar, nm, md, score, pos, used_dp)."""
+    def cigar_batch_raw(self, sc: Scoring, bases: np.ndarray, tasks: np.ndarray):
+        """CIGARGenerator.generate over CIGAR_TASK_DTYPE tasks -> (CIGAR_RESULT_DTYPE
+        array, packed CIGAR words, MD bytes); task k's CIGAR is
+        cigar[cigar_off : cigar_off + n_cigar], its MD md[md_off : md_off + md_len]."""
         assert tasks.dtype == abi.CIGAR_TASK_DTYPE
         ql = tasks["qlen"].astype(np.int64)
         rl = tasks["rlen"].astype(np.int64)
         ccap = int((ql + rl + 2).sum()) + 1
         mcap = int((6 * (ql + rl) + 8).sum()) + 1
         res = np.zeros(len(tasks), abi.CIGAR_RESULT_DTYPE)
-        cig = np.zeros(ccap, np.uint32)
-        md = C.create_string_buffer(mcap)
+        cig = np.empty(ccap, np.uint32)
+        md = np.empty(mcap, np.uint8)
         bases = np.ascontiguousarray(bases, dtype=np.uint8)
         if bases.size == 0:
             bases = np.zeros(1, np.uint8)
         _check(self.lib.swb_cigar_batch(self.h, C.byref(sc), ptr(bases), bases.size, tasks.ctypes.data,
-                                        len(tasks), res.ctypes.data, ptr(cig, C.c_uint32), ccap, md, mcap),
-               "swb_cigar_batch")
-        raw = md.raw
+                                        len(tasks), res.ctypes.data, ptr(cig, C.c_uint32), ccap,
+                                        md.ctypes.data_as(C.c_char_p), mcap), "swb_cigar_batch")
+        return res, cig, md
+
+    def cigar_batch(self, sc: Scoring, bases: np.ndarray, tasks: np.ndarray):
+        """CIGARGenerator.generate over CIGAR_TASK_DTYPE tasks -> list of dicts
+        (cigar, nm, md, score, pos, used_dp)."""
+        res, cig, md = self.cigar_batch_raw(sc, bases, tasks)
+        raw = md.tobytes()
         out = []
         for r in res:
             o, n = int(r["cigar_off"]), int(r["n_cigar"])

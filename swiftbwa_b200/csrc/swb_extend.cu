@@ -2,331 +2,480 @@
 // (Sources/Alignment/ExtensionAligner.swift:114-346).
 //
 // Within one chain the reference is sequential: seeds run in descending
-// score order, a seed inside an earlier region of the chain is only
+// score order (stable), a seed inside an earlier region of the chain is only
 // counted (sub/subN), the left extension may be retried once with a doubled
-// band, the right extension starts from the left score (h0), and may be
-// retried too.  Across chains everything is independent.  So each chain is
-// a small host state machine, and the GPU work is gathered in rounds: every
-// round collects the one pending extension of every active chain into a
-// single batch (one sort + binned pass over the device-resident reads),
-// then feeds each result back to its chain, which either emits its next
-// extension (retry, right side, next seed) or finishes.
+// band, the right extension starts from the left score (h0) and may be
+// retried too.  Across chains everything is independent.  So every chain is
+// a small state machine held in device memory (one thread per chain), and
+// the extensions are gathered in rounds:
+//
+//   seed order     one segmented stable sort of all seeds by score
+//   init           rmax0/rmax1 per chain, then advance to the first task
+//   per round      compact the live chains, gather their pending task into a
+//                  dense batch, run the binned extension pass (launch_ext),
+//                  then feed each result back: the chain either emits its
+//                  next task (retry, right side, next seed) or finishes.
+//
+// The host only reads one count per round.  Regions are written in place
+// (chain c's at out[seed_off ...]) and copied back once at the end.
 #include <algorithm>
 #include <cstring>
 #include <string>
-#include <thread>
 #include <vector>
 
+#include <cub/device/device_segmented_sort.cuh>
+#include <cub/device/device_select.cuh>
+
+#include "swb_device.cuh"
 #include "swb_internal.h"
 
 namespace swb {
-int ext_big_max_q(const swb_ext_task *tasks, size_t n, int max_mat);
-}
-
-using namespace swb;
-
 namespace {
 
+enum : int32_t { kSeed = 0, kLeft = 1, kRight = 2, kDone = 3 };
+
+struct ChainState {
+    int64_t rmax0, rmax1, rbeg, rend;
+    swb_region reg;                       // region of the current seed
+    int32_t k, phase, qbeg, len, score, qend, accH0, w, prev, try_idx;
+    int32_t l_score, l_q, l_t, r_score, r_q, r_t, nreg, tmp;
+};
+
+struct ChainArgs {
+    DevScoring sc;
+    int64_t gl;
+    const swb_chain *chains;
+    const swb_seed *seeds;
+    const uint32_t *order;   // per chain, its seeds' global indices in descending score order
+    ChainState *state;
+    swb_ext_task *task;      // pending task per chain
+    swb_region *regions;     // chain c's at seed_off
+    uint32_t n_chains;
+};
+
 // calMaxGap (ExtensionAligner.swift:352-363)
-long cal_max_gap(long qlen, const swb_scoring &sc) {
+__device__ long cal_max_gap(long qlen, const DevScoring &sc) {
     const long a = sc.a, oDel = sc.o_del, eDel = sc.e_del, oIns = sc.o_ins, eIns = sc.e_ins;
     const long lDel = eDel > 0 ? (qlen * a - oDel) / eDel + 1 : 1;
     const long lIns = eIns > 0 ? (qlen * a - oIns) / eIns + 1 : 1;
-    long l = std::max(std::max(lDel, lIns), 1L);
-    return std::min(l, (long)sc.band_width << 1);
+    long l = lDel > lIns ? lDel : lIns;
+    l = l > 1 ? l : 1;
+    const long cap = (long)sc.band_width << 1;
+    return l < cap ? l : cap;
 }
 
 // FMIndex.getReference(at:length:) as a span of the resident forward strand
-// (FMIndex.swift:147-170): forward positions read directly, reverse-strand
+// (FMIndex.swift:147-170): forward positions directly, reverse-strand
 // positions as the reverse complement of the mirrored forward window.
 struct RefSpan {
-    uint64_t off = 0;
-    int32_t len = 0;
-    bool rc = false;   // reverse-complemented
+    uint64_t off;
+    int32_t len;
+    bool rc;
 };
 
-RefSpan get_reference(int64_t pos, long length, int64_t gl) {
-    RefSpan r;
+__device__ RefSpan get_reference(int64_t pos, int64_t length, int64_t gl) {
+    RefSpan r{0, 0, false};
     if (pos >= gl) {
         const int64_t fwdEnd = 2 * gl - pos, fwdStart = fwdEnd - length;
-        const int64_t s = std::max<int64_t>(0, fwdStart), e = std::min(fwdEnd, gl);
-        if (e - s > 0) {
-            r.off = (uint64_t)s;
-            r.len = (int32_t)(e - s);
-            r.rc = true;
-        }
+        const int64_t s = fwdStart > 0 ? fwdStart : 0, e = fwdEnd < gl ? fwdEnd : gl;
+        if (e - s > 0) r = RefSpan{(uint64_t)s, (int32_t)(e - s), true};
     } else {
-        const int64_t n = std::min<int64_t>(length, gl - pos);
-        if (n > 0 && pos >= 0) {
-            r.off = (uint64_t)pos;
-            r.len = (int32_t)n;
-        }
+        const int64_t n = length < gl - pos ? length : gl - pos;
+        if (n > 0 && pos >= 0) r = RefSpan{(uint64_t)pos, (int32_t)n, false};
     }
     return r;
 }
 
-enum Phase { kSeed, kLeft, kRight, kDone };
-
 struct Chain {
-    const swb_chain *ch = nullptr;
-    const swb_seed *seeds = nullptr;   // this chain's seeds
-    std::vector<uint32_t> order;
-    int64_t rmax0 = 0, rmax1 = 0;
-    int32_t tmp = 0;
-    size_t k = 0;
-    Phase phase = kSeed;
-    // current seed
-    int32_t qbeg = 0, len = 0, score = 0, qend = 0;
-    int64_t rbeg = 0, rend = 0;
-    swb_region reg{};
-    int32_t accH0 = 0, w = 0, prev = 0, tryIdx = 0;
-    int32_t lScore = 0, lQ = 0, lT = 0, rScore = 0, rQ = 0, rT = 0;
-    swb_ext_task task{};
-    std::vector<swb_region> regions;
-};
+    const ChainArgs &a;
+    const swb_chain ch;
+    ChainState &c;
+    swb_ext_task &task;
+    swb_region *regs;
 
-struct Driver {
-    const swb_scoring &sc;
-    int64_t gl;
-    std::vector<Chain> &chains;
-
-    // Left extension task of the current seed, or none (:206-216).
-    bool left_task(Chain &c) {
+    // Left extension of the current seed, if any (:202-216).  The fetched
+    // window is used reversed (:219-224): a forward window reads backwards,
+    // a reverse-complement window becomes the plain complement.
+    __device__ bool left_task() {
         if (c.qbeg <= 0) return false;
-        const long tl = std::min<int64_t>(c.rbeg - c.rmax0, 10000);
+        const int64_t d = c.rbeg - c.rmax0;
+        const int64_t tl = d < 10000 ? d : 10000;
         if (tl <= 0) return false;
-        const RefSpan t = get_reference(c.rbeg - tl, tl, gl);
-        // The fetched window is reversed (:219-224): a forward window reads
-        // backwards, a reverse-complement window becomes the plain complement.
-        const uint32_t tf = SWB_T_FROM_REF | (t.rc ? SWB_T_COMPLEMENT : SWB_T_REVERSE);
-        c.w = sc.band_width;
+        const RefSpan t = get_reference(c.rbeg - tl, tl, a.gl);
+        c.w = a.sc.band_width;
         c.prev = c.score;
-        c.tryIdx = 0;
-        c.task = swb_ext_task{c.ch->read_off, t.off, c.qbeg, t.len, c.w, c.score, sc.pen_clip5, SWB_Q_REVERSE | tf};
+        c.try_idx = 0;
+        task = swb_ext_task{ch.read_off, t.off, c.qbeg, t.len, c.w, c.score, a.sc.pen_clip5,
+                            SWB_Q_REVERSE | SWB_T_FROM_REF | (t.rc ? SWB_T_COMPLEMENT : SWB_T_REVERSE)};
         c.phase = kLeft;
         return true;
     }
 
-    // Right extension task (:269-279).
-    bool right_task(Chain &c) {
-        if (c.qend >= c.ch->read_len) return false;
-        const long tl = std::min<int64_t>(c.rmax1 - c.rend, 10000);
+    // Right extension (:265-279).
+    __device__ bool right_task() {
+        if (c.qend >= ch.read_len) return false;
+        const int64_t d = c.rmax1 - c.rend;
+        const int64_t tl = d < 10000 ? d : 10000;
         if (tl <= 0) return false;
-        const RefSpan t = get_reference(c.rend, tl, gl);
-        const uint32_t tf = SWB_T_FROM_REF | (t.rc ? (SWB_T_REVERSE | SWB_T_COMPLEMENT) : 0u);
-        c.w = sc.band_width;
+        const RefSpan t = get_reference(c.rend, tl, a.gl);
+        c.w = a.sc.band_width;
         c.prev = c.accH0;
-        c.tryIdx = 0;
-        c.task = swb_ext_task{c.ch->read_off + (uint64_t)c.qend, t.off, c.ch->read_len - c.qend, t.len, c.w, c.accH0,
-                              sc.pen_clip3, tf};
+        c.try_idx = 0;
+        task = swb_ext_task{ch.read_off + (uint64_t)c.qend, t.off, ch.read_len - c.qend, t.len, c.w, c.accH0,
+                            a.sc.pen_clip3, SWB_T_FROM_REF | (t.rc ? (SWB_T_REVERSE | SWB_T_COMPLEMENT) : 0u)};
         c.phase = kRight;
         return true;
     }
 
-    // Region assembly (:318-335).
-    void finish_seed(Chain &c) {
-        c.reg.qb = c.qbeg - c.lQ;
-        c.reg.qe = c.qend + c.rQ;
-        c.reg.rb = c.rbeg - c.lT;
-        c.reg.re = c.rend + c.rT;
-        int32_t trueScore = c.len * sc.a;
-        if (c.lScore > 0) trueScore = c.lScore;
-        if (c.rScore > 0) trueScore += c.rScore - c.accH0;
-        c.reg.score = trueScore;
-        c.reg.true_score = trueScore;
-        int32_t cov = 0;                                            // computeSeedCov (:36-70)
-        for (uint32_t i = 0; i < c.ch->n_seeds; ++i) {
-            const swb_seed &s = c.seeds[i];
-            if (s.qbeg >= c.reg.qb && s.qbeg + s.len <= c.reg.qe && s.rbeg >= c.reg.rb && s.rbeg + s.len <= c.reg.re)
-                cov += s.len;
+    // Region assembly and seed coverage (:318-335, computeSeedCov :36-70).
+    __device__ void finish_seed() {
+        swb_region &r = c.reg;
+        r.qb = c.qbeg - c.l_q;
+        r.qe = c.qend + c.r_q;
+        r.rb = c.rbeg - c.l_t;
+        r.re = c.rend + c.r_t;
+        int32_t trueScore = c.len * a.sc.a;
+        if (c.l_score > 0) trueScore = c.l_score;
+        if (c.r_score > 0) trueScore += c.r_score - c.accH0;
+        r.score = trueScore;
+        r.true_score = trueScore;
+        int32_t cov = 0;
+        const swb_seed *sd = a.seeds + ch.seed_off;
+        for (uint32_t i = 0; i < ch.n_seeds; ++i) {
+            const swb_seed s = sd[i];
+            if (s.qbeg >= r.qb && s.qbeg + s.len <= r.qe && s.rbeg >= r.rb && s.rbeg + s.len <= r.re) cov += s.len;
         }
-        c.reg.seed_cov = cov;
-        c.regions.push_back(c.reg);
+        r.seed_cov = cov;
+        regs[c.nreg++] = r;
         ++c.k;
         c.phase = kSeed;
     }
 
-    // Advances a chain on the host until it needs a GPU extension or is done.
-    void advance(Chain &c) {
+    // Runs the chain on until it needs an extension or is done.
+    __device__ void advance() {
         while (c.phase == kSeed) {
-            if (c.k == c.order.size()) {                            // :338-343
-                const int32_t thr = sc.min_seed_len * sc.a;
-                for (auto &r : c.regions)
-                    if (r.sub > 0 && r.sub < thr) r.sub = 0;
+            if ((uint32_t)c.k == ch.n_seeds) {                          // :338-343
+                const int32_t thr = a.sc.min_seed_len * a.sc.a;
+                for (int i = 0; i < c.nreg; ++i)
+                    if (regs[i].sub > 0 && regs[i].sub < thr) regs[i].sub = 0;
                 c.phase = kDone;
                 return;
             }
-            const swb_seed &s = c.seeds[c.order[c.k]];
+            const swb_seed s = a.seeds[a.order[ch.seed_off + (uint32_t)c.k]];
             c.qbeg = s.qbeg;
             c.len = s.len;
             c.score = s.score;
             c.rbeg = s.rbeg;
             c.qend = s.qbeg + s.len;
             c.rend = s.rbeg + s.len;
-            int cover = -1;                                          // :172-189
-            for (size_t i = 0; i < c.regions.size(); ++i)
-                if (c.qbeg >= c.regions[i].qb && c.qend <= c.regions[i].qe) {
-                    cover = (int)i;
+            int cover = -1;                                             // :172-189
+            for (int i = 0; i < c.nreg; ++i)
+                if (c.qbeg >= regs[i].qb && c.qend <= regs[i].qe) {
+                    cover = i;
                     break;
                 }
             if (cover >= 0) {
-                swb_region &r = c.regions[(size_t)cover];
-                const int32_t aln = c.len * sc.a;
+                swb_region &r = regs[cover];
+                const int32_t aln = c.len * a.sc.a;
                 if (aln > r.sub) r.sub = aln;
                 if (aln >= r.score - c.tmp) r.sub_n += 1;
                 ++c.k;
                 continue;
             }
-            c.reg = swb_region{};                                    // :191-199
-            c.reg.w = sc.band_width;
-            c.reg.rid = c.ch->rid;
+            c.reg = swb_region{};                                       // :191-199
+            c.reg.w = a.sc.band_width;
+            c.reg.rid = ch.rid;
             c.reg.seed_cov = c.len;
             c.reg.seed_len0 = c.len;
             c.accH0 = c.score;
-            c.lScore = c.lQ = c.lT = c.rScore = c.rQ = c.rT = 0;
-            if (left_task(c)) return;
-            if (right_task(c)) return;
-            finish_seed(c);
+            c.l_score = c.l_q = c.l_t = c.r_score = c.r_q = c.r_t = 0;
+            if (left_task()) return;
+            if (right_task()) return;
+            finish_seed();
         }
     }
 
-    // Feeds one extension result back (:233-260 and :288-314).
-    void feed(Chain &c, const swb_ext_result &r) {
-        const bool stop = r.score == c.prev || r.max_off < (c.w >> 1) + (c.w >> 2) || c.tryIdx == 1;
-        if (!stop) {
-            c.prev = r.score;
+    // One extension result (:233-260 left, :288-314 right).
+    __device__ void feed(const swb_ext_result &r) {
+        if (!(r.score == c.prev || r.max_off < (c.w >> 1) + (c.w >> 2) || c.try_idx == 1)) {
+            c.prev = r.score;                                           // retry with a doubled band
             c.w <<= 1;
-            c.tryIdx = 1;
-            c.task.w = c.w;
-            return;                                                  // same task, doubled band
+            c.try_idx = 1;
+            task.w = c.w;
+            return;
         }
+        c.reg.w = c.reg.w > c.w ? c.reg.w : c.w;
         if (c.phase == kLeft) {
             c.accH0 = r.score;
-            c.reg.w = std::max(c.reg.w, c.w);
-            if (r.gscore <= 0 || r.gscore <= r.score - sc.pen_clip5) {
-                c.lQ = r.qle;
-                c.lT = r.tle;
-                c.lScore = r.score;
+            if (r.gscore <= 0 || r.gscore <= r.score - a.sc.pen_clip5) {
+                c.l_q = r.qle;
+                c.l_t = r.tle;
+                c.l_score = r.score;
             } else {
-                c.lQ = c.qbeg;
-                c.lT = r.gtle;
-                c.lScore = r.gscore;
+                c.l_q = c.qbeg;
+                c.l_t = r.gtle;
+                c.l_score = r.gscore;
             }
             c.phase = kSeed;
-            if (right_task(c)) return;
-            finish_seed(c);
+            if (right_task()) return;
+            finish_seed();
         } else {
-            c.reg.w = std::max(c.reg.w, c.w);
-            if (r.gscore <= 0 || r.gscore <= r.score - sc.pen_clip3) {
-                c.rQ = r.qle;
-                c.rT = r.tle;
-                c.rScore = r.score;
+            if (r.gscore <= 0 || r.gscore <= r.score - a.sc.pen_clip3) {
+                c.r_q = r.qle;
+                c.r_t = r.tle;
+                c.r_score = r.score;
             } else {
-                c.rQ = c.ch->read_len - c.qend;
-                c.rT = r.gtle;
-                c.rScore = r.gscore;
+                c.r_q = ch.read_len - c.qend;
+                c.r_t = r.gtle;
+                c.r_score = r.gscore;
             }
-            finish_seed(c);
+            finish_seed();
         }
-        advance(c);
+        advance();
     }
 };
 
+__global__ void seed_keys_kernel(const swb_seed *__restrict__ seeds, size_t n_seeds, const swb_chain *__restrict__ chains,
+                                 uint32_t n_chains, int32_t *__restrict__ keys, uint32_t *__restrict__ vals,
+                                 uint32_t *__restrict__ beg, uint32_t *__restrict__ end) {
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i < n_seeds) {
+        keys[i] = seeds[i].score;
+        vals[i] = (uint32_t)i;
+    }
+    if (i < n_chains) {
+        beg[i] = chains[i].seed_off;
+        end[i] = chains[i].seed_off + chains[i].n_seeds;
+    }
+}
+
+// Chain set-up (:126-158) and the first advance; live[c] = chain c has a task.
+__global__ void chain_init_kernel(ChainArgs a, uint32_t *__restrict__ ids, uint8_t *__restrict__ live) {
+    const uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ci >= a.n_chains) return;
+    const swb_chain ch = a.chains[ci];
+    ChainState c{};
+    const long lq = ch.read_len;
+    c.rmax0 = INT64_MAX;
+    c.rmax1 = 0;
+    const swb_seed *sd = a.seeds + ch.seed_off;
+    for (uint32_t k = 0; k < ch.n_seeds; ++k) {
+        const swb_seed t = sd[k];
+        const int64_t b = t.rbeg - (int64_t)((long)t.qbeg + cal_max_gap(t.qbeg, a.sc));
+        const long remaining = lq - t.qbeg - t.len;
+        const int64_t e = t.rbeg + t.len + (int64_t)(remaining + cal_max_gap(remaining, a.sc));
+        c.rmax0 = b < c.rmax0 ? b : c.rmax0;
+        c.rmax1 = e > c.rmax1 ? e : c.rmax1;
+    }
+    if (c.rmax0 < 0) c.rmax0 = 0;
+    c.tmp = imax(a.sc.a + a.sc.b, imax(a.sc.o_ins + a.sc.e_ins, a.sc.o_del + a.sc.e_del));
+    c.phase = kSeed;
+    swb_ext_task task{};
+    Chain{a, ch, c, task, a.regions + ch.seed_off}.advance();
+    a.state[ci] = c;
+    a.task[ci] = task;
+    ids[ci] = ci;
+    live[ci] = c.phase != kDone;
+}
+
+// Feeds round results back; live[k] = active chain k still has a task.
+__global__ void chain_feed_kernel(ChainArgs a, const uint32_t *__restrict__ active, uint32_t n,
+                                  const swb_ext_result *__restrict__ res, uint8_t *__restrict__ live) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t ci = active[k];
+    const swb_chain ch = a.chains[ci];
+    ChainState c = a.state[ci];
+    swb_ext_task task = a.task[ci];
+    Chain{a, ch, c, task, a.regions + ch.seed_off}.feed(res[k]);
+    a.state[ci] = c;
+    a.task[ci] = task;
+    live[k] = c.phase != kDone;
+}
+
+// Dense batch of the live chains' tasks (count read on the device).
+__global__ void gather_tasks_kernel(const uint32_t *__restrict__ active, const uint32_t *__restrict__ n_active,
+                                    const swb_ext_task *__restrict__ task, swb_ext_task *__restrict__ out, uint32_t cap) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < cap && k < *n_active) out[k] = task[active[k]];
+}
+
+__global__ void region_counts_kernel(const ChainState *__restrict__ st, uint32_t n, uint32_t *__restrict__ counts) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) counts[k] = (uint32_t)st[k].nreg;
+}
+
+inline size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
 }  // namespace
+}  // namespace swb
+
+using namespace swb;
 
 extern "C" int swb_extend_chains(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, size_t n_bases,
                                  const swb_seed *seeds, size_t n_seeds, const swb_chain *chains, size_t n_chains,
                                  uint64_t genome_len, swb_region *out, uint32_t *n_regions, uint32_t *rounds) {
-    if (!ctx || !sc || (!bases && n_bases) || (!seeds && n_seeds) || (!chains && n_chains) ||
-        (!out && n_seeds) || (!n_regions && n_chains))
+    if (!ctx || (!bases && n_bases) || (!seeds && n_seeds) || (!chains && n_chains) || (!out && n_seeds) ||
+        (!n_regions && n_chains))
         return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
-    if (sc->e_ins <= 0 || sc->e_del <= 0 || sc->a < 0 || sc->b < 0 || sc->a > 127 || sc->b > 128)
-        return set_error(SWB_ERR_INVALID_ARG, "scoring out of range");
+    int rc;
+    if ((rc = validate_scoring(sc))) return rc;
     if (rounds) *rounds = 0;
     if (n_chains == 0) return SWB_OK;
+    if (n_chains > 0x7FFFFFF0ull || n_seeds > 0x7FFFFFF0ull)
+        return set_error(SWB_ERR_TOO_LARGE, "more than 2^31-16 chains or seeds");
     if (!ctx->d_pac || genome_len > ctx->ref_bases)
         return set_error(SWB_ERR_NO_REFERENCE, "the forward strand (genome_len bases) must be uploaded first");
-    // Chain set-up (:126-158).
-    std::vector<Chain> cs(n_chains);
+    // Validation: spans inside the inputs, seed ranges of different chains
+    // disjoint (regions are written at each chain's seed_off).
+    int max_read = 0;
+    bool sorted = true;
+    uint64_t prev_end = 0;
     for (size_t i = 0; i < n_chains; ++i) {
         const swb_chain &ch = chains[i];
         if ((uint64_t)ch.seed_off + ch.n_seeds > n_seeds || ch.read_len < 0 || ch.read_len > kMaxLen ||
             ch.read_off + (uint64_t)ch.read_len > n_bases)
             return set_error(SWB_ERR_INVALID_ARG, "chain " + std::to_string(i) + ": seeds or read outside the inputs");
-        Chain &c = cs[i];
-        c.ch = &ch;
-        c.seeds = seeds + ch.seed_off;
+        max_read = std::max(max_read, ch.read_len);
         for (uint32_t k = 0; k < ch.n_seeds; ++k) {
-            const swb_seed &s = c.seeds[k];
-            if (s.qbeg < 0 || s.len < 0 || s.qbeg + s.len > ch.read_len || s.rbeg < 0 || s.rbeg + s.len > 2 * (int64_t)genome_len)
-                return set_error(SWB_ERR_INVALID_ARG, "chain " + std::to_string(i) + ": seed " + std::to_string(k) + " out of range");
+            const swb_seed &s = seeds[ch.seed_off + k];
+            if (s.qbeg < 0 || s.len < 0 || s.qbeg + s.len > ch.read_len || s.rbeg < 0 ||
+                s.rbeg + s.len > 2 * (int64_t)genome_len)
+                return set_error(SWB_ERR_INVALID_ARG,
+                                 "chain " + std::to_string(i) + ": seed " + std::to_string(k) + " out of range");
         }
-        c.rmax0 = INT64_MAX;
-        c.rmax1 = 0;
-        const long lq = ch.read_len;
-        for (uint32_t k = 0; k < ch.n_seeds; ++k) {
-            const swb_seed &t = c.seeds[k];
-            const int64_t b = t.rbeg - (int64_t)((long)t.qbeg + cal_max_gap(t.qbeg, *sc));
-            const long remaining = lq - t.qbeg - t.len;
-            const int64_t e = t.rbeg + t.len + (int64_t)(remaining + cal_max_gap(remaining, *sc));
-            c.rmax0 = std::min(c.rmax0, b);
-            c.rmax1 = std::max(c.rmax1, e);
+        if (ch.n_seeds) {
+            if (ch.seed_off < prev_end) sorted = false;
+            prev_end = std::max<uint64_t>(prev_end, (uint64_t)ch.seed_off + ch.n_seeds);
         }
-        if (c.rmax0 < 0) c.rmax0 = 0;
-        c.tmp = std::max(sc->a + sc->b, std::max(sc->o_ins + sc->e_ins, sc->o_del + sc->e_del));
-        c.order.resize(ch.n_seeds);
-        for (uint32_t k = 0; k < ch.n_seeds; ++k) c.order[k] = k;
-        std::stable_sort(c.order.begin(), c.order.end(),
-                         [&](uint32_t x, uint32_t y) { return c.seeds[x].score > c.seeds[y].score; });
     }
-    Driver drv{*sc, (int64_t)genome_len, cs};
-    for (Chain &c : cs) drv.advance(c);
+    if (!sorted) {
+        std::vector<std::pair<uint32_t, uint32_t>> r;
+        for (size_t i = 0; i < n_chains; ++i)
+            if (chains[i].n_seeds) r.emplace_back(chains[i].seed_off, chains[i].n_seeds);
+        std::sort(r.begin(), r.end());
+        for (size_t i = 1; i < r.size(); ++i)
+            if ((uint64_t)r[i - 1].first + r[i - 1].second > r[i].first)
+                return set_error(SWB_ERR_INVALID_ARG, "chains' seed ranges overlap");
+    }
 
     std::lock_guard<std::mutex> lk(ctx->mu);
     SWB_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
     const DevScoring dsc = make_dev_scoring(*sc);
-    const size_t bases_bytes = (std::max<size_t>(n_bases, 1) + 255) & ~(size_t)255;
-    int rc;
-    if ((rc = ensure_dev(ctx, ctx->d_bases, bases_bytes))) return rc;
-    SWB_CUDA(cudaMemcpyAsync(ctx->d_bases.p, bases, std::max<size_t>(n_bases, 1), cudaMemcpyHostToDevice, ctx->stream));
-    SWB_CUDA(cudaMemsetAsync(ctx->d_counters, 0, sizeof(unsigned long long) * kNumCounters, ctx->stream));
-    std::vector<swb_ext_task> batch;
-    std::vector<size_t> owner;
-    std::vector<swb_ext_result> res;
-    uint32_t nround = 0;
-    for (;;) {
-        batch.clear();
-        owner.clear();
-        for (size_t i = 0; i < cs.size(); ++i)
-            if (cs[i].phase == kLeft || cs[i].phase == kRight) {
-                batch.push_back(cs[i].task);
-                owner.push_back(i);
-            }
-        if (batch.empty()) break;
-        const size_t n = batch.size();
-        res.resize(n);
-        if ((rc = ensure_dev(ctx, ctx->d_tasks, n * sizeof(swb_ext_task))) ||
-            (rc = ensure_dev(ctx, ctx->d_out, n * sizeof(swb_ext_result))))
-            return rc;
-        SWB_CUDA(cudaMemcpyAsync(ctx->d_tasks.p, batch.data(), n * sizeof(swb_ext_task), cudaMemcpyHostToDevice, ctx->stream));
-        if ((rc = launch_ext(ctx, dsc, (const uint8_t *)ctx->d_bases.p, (const swb_ext_task *)ctx->d_tasks.p, n,
-                             (swb_ext_result *)ctx->d_out.p, ctx->d_counters, ctx->stream,
-                             ext_big_max_q(batch.data(), n, dsc.max_mat))))
-            return rc;
-        SWB_CUDA(cudaMemcpyAsync(res.data(), ctx->d_out.p, n * sizeof(swb_ext_result), cudaMemcpyDeviceToHost, ctx->stream));
-        SWB_CUDA(cudaStreamSynchronize(ctx->stream));
-        ++nround;
-        for (size_t k = 0; k < n; ++k) drv.feed(cs[owner[k]], res[k]);
+    const size_t nc = n_chains, ns = std::max<size_t>(n_seeds, 1);
+    // Device layout of the chain buffer.
+    size_t off = 0;
+    auto carve = [&](size_t bytes) {
+        const size_t o = off;
+        off += al256(bytes);
+        return o;
+    };
+    const size_t o_seeds = carve(ns * sizeof(swb_seed)), o_chains = carve(nc * sizeof(swb_chain));
+    const size_t o_state = carve(nc * sizeof(ChainState)), o_task = carve(nc * sizeof(swb_ext_task));
+    const size_t o_reg = carve(ns * sizeof(swb_region)), o_act0 = carve(nc * 4), o_act1 = carve(nc * 4);
+    const size_t o_live = carve(nc), o_num = carve(8), o_counts = carve(nc * 4);
+    const size_t o_keys = carve(ns * 4), o_keys2 = carve(ns * 4), o_vals = carve(ns * 4), o_order = carve(ns * 4);
+    const size_t o_beg = carve(nc * 4), o_end = carve(nc * 4);
+    if ((rc = ensure_dev(ctx, ctx->d_chain, off))) return rc;
+    char *base = (char *)ctx->d_chain.p;
+    swb_seed *d_seeds = (swb_seed *)(base + o_seeds);
+    swb_chain *d_chains = (swb_chain *)(base + o_chains);
+    uint32_t *act[2] = {(uint32_t *)(base + o_act0), (uint32_t *)(base + o_act1)};
+    uint8_t *d_live = (uint8_t *)(base + o_live);
+    uint32_t *d_num = (uint32_t *)(base + o_num);
+    swb_region *d_reg = (swb_region *)(base + o_reg);
+    ChainState *d_state = (ChainState *)(base + o_state);
+    const size_t bases_bytes = std::max<size_t>(n_bases, 1);
+    if ((rc = ensure_dev(ctx, ctx->d_bases, al256(bases_bytes))) ||
+        (rc = ensure_dev(ctx, ctx->d_tasks, nc * sizeof(swb_ext_task))) ||
+        (rc = ensure_dev(ctx, ctx->d_out, nc * sizeof(swb_ext_result))))
+        return rc;
+
+    SWB_CUDA(cudaMemsetAsync(ctx->d_counters, 0, sizeof(unsigned long long) * kNumCounters, st));
+    SWB_CUDA(cudaEventRecord(ctx->ev_start, st));
+    if (n_bases) SWB_CUDA(cudaMemcpyAsync(ctx->d_bases.p, bases, n_bases, cudaMemcpyHostToDevice, st));
+    if (n_seeds) SWB_CUDA(cudaMemcpyAsync(d_seeds, seeds, n_seeds * sizeof(swb_seed), cudaMemcpyHostToDevice, st));
+    SWB_CUDA(cudaMemcpyAsync(d_chains, chains, nc * sizeof(swb_chain), cudaMemcpyHostToDevice, st));
+    SWB_CUDA(cudaMemsetAsync(d_reg, 0, ns * sizeof(swb_region), st));
+
+    // Seed order: stable descending sort of each chain's seeds by score (:155-158).
+    uint32_t *order = (uint32_t *)(base + o_order);
+    const unsigned tb = 256;
+    {
+        const size_t m = std::max(ns, nc);
+        ProfScope ps(ctx, st, "chain_seed_order", -1);
+        seed_keys_kernel<<<(unsigned)((m + tb - 1) / tb), tb, 0, st>>>(
+            d_seeds, n_seeds, d_chains, (uint32_t)nc, (int32_t *)(base + o_keys), (uint32_t *)(base + o_vals),
+            (uint32_t *)(base + o_beg), (uint32_t *)(base + o_end));
+        ctx->launches++;
+        SWB_CUDA(cudaGetLastError());
+        if (n_seeds) {
+            size_t tmp = 0;
+            SWB_CUDA(cub::DeviceSegmentedSort::StableSortPairsDescending(
+                nullptr, tmp, (const int32_t *)(base + o_keys), (int32_t *)(base + o_keys2),
+                (const uint32_t *)(base + o_vals), order, (int)n_seeds, (int)nc, (const uint32_t *)(base + o_beg),
+                (const uint32_t *)(base + o_end), st));
+            if ((rc = ensure_dev(ctx, ctx->d_sort_tmp, tmp))) return rc;
+            SWB_CUDA(cub::DeviceSegmentedSort::StableSortPairsDescending(
+                ctx->d_sort_tmp.p, tmp, (const int32_t *)(base + o_keys), (int32_t *)(base + o_keys2),
+                (const uint32_t *)(base + o_vals), order, (int)n_seeds, (int)nc, (const uint32_t *)(base + o_beg),
+                (const uint32_t *)(base + o_end), st));
+        }
     }
+    ChainArgs ca{dsc, (int64_t)genome_len, d_chains, d_seeds, order, d_state,
+                 (swb_ext_task *)(base + o_task), d_reg, (uint32_t)nc};
+    {
+        ProfScope ps(ctx, st, "chain_step", -1);
+        chain_init_kernel<<<(unsigned)((nc + tb - 1) / tb), tb, 0, st>>>(ca, act[1], d_live);
+        ctx->launches++;
+        SWB_CUDA(cudaGetLastError());
+    }
+    // act[1] lists the chains of the last step with their live flags; each
+    // round compacts it into act[0], then the two swap.
+    uint32_t n_prev = (uint32_t)nc, nround = 0;
+    swb_ext_task *d_batch = (swb_ext_task *)ctx->d_tasks.p;
+    swb_ext_result *d_res = (swb_ext_result *)ctx->d_out.p;
+    for (;;) {
+        size_t tmp = 0;
+        SWB_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp, act[1], d_live, act[0], d_num, (int)n_prev, st));
+        if ((rc = ensure_dev(ctx, ctx->d_sort_tmp, tmp))) return rc;
+        SWB_CUDA(cub::DeviceSelect::Flagged(ctx->d_sort_tmp.p, tmp, act[1], d_live, act[0], d_num, (int)n_prev, st));
+        gather_tasks_kernel<<<(n_prev + tb - 1) / tb, tb, 0, st>>>(act[0], d_num, ca.task, d_batch, n_prev);
+        ctx->launches++;
+        SWB_CUDA(cudaGetLastError());
+        uint32_t n = 0;
+        SWB_CUDA(cudaMemcpyAsync(&n, d_num, sizeof(n), cudaMemcpyDeviceToHost, st));
+        SWB_CUDA(cudaStreamSynchronize(st));
+        if (n == 0) break;
+        if ((rc = launch_ext(ctx, dsc, (const uint8_t *)ctx->d_bases.p, d_batch, n, d_res, ctx->d_counters, st,
+                             max_read)))
+            return rc;
+        ++nround;
+        {
+            ProfScope ps(ctx, st, "chain_step", -1);
+            chain_feed_kernel<<<(n + tb - 1) / tb, tb, 0, st>>>(ca, act[0], n, d_res, d_live);
+            ctx->launches++;
+            SWB_CUDA(cudaGetLastError());
+        }
+        std::swap(act[0], act[1]);
+        n_prev = n;
+    }
+    uint32_t *d_counts = (uint32_t *)(base + o_counts);
+    region_counts_kernel<<<(unsigned)((nc + tb - 1) / tb), tb, 0, st>>>(d_state, (uint32_t)nc, d_counts);
+    ctx->launches++;
+    SWB_CUDA(cudaGetLastError());
+    if (n_seeds) SWB_CUDA(cudaMemcpyAsync(out, d_reg, n_seeds * sizeof(swb_region), cudaMemcpyDeviceToHost, st));
+    SWB_CUDA(cudaMemcpyAsync(n_regions, d_counts, nc * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    SWB_CUDA(cudaEventRecord(ctx->ev_stop, st));
+    SWB_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) ctx->last_ms = ms;
     unsigned long long c[kNumCounters] = {0};
     if (cudaMemcpy(c, ctx->d_counters, sizeof(c), cudaMemcpyDeviceToHost) == cudaSuccess) {
         unsigned long long sum = 0;
         for (int k = 0; k < kNumCounters; ++k) sum += c[k];
         ctx->last_cells = sum;
-    }
-    for (size_t i = 0; i < cs.size(); ++i) {
-        n_regions[i] = (uint32_t)cs[i].regions.size();
-        std::copy(cs[i].regions.begin(), cs[i].regions.end(), out + chains[i].seed_off);
     }
     if (rounds) *rounds = nround;
     return SWB_OK;

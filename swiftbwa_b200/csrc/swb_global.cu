@@ -28,6 +28,7 @@ struct GlobalArgs {
     const unsigned long long *cigar_off;   // per task
     unsigned long long *cells;
     size_t n;
+    int qsplit;   // tasks with qlen <= qsplit belong to the shared-memory kernel
 };
 
 struct Scratch {
@@ -116,8 +117,10 @@ struct CigarOut {
     }
 };
 
-// Traceback (GlobalAligner.swift:160-232).
-__device__ int global_traceback(const Scratch &s, int qlen, int tlen, int w, int nCol, uint32_t *out) {
+// Traceback (GlobalAligner.swift:160-232); zat(i, col) is the 4-bit
+// direction code of row i, band column col.
+template <class ZAt>
+__device__ int global_traceback(ZAt zat, int qlen, int tlen, int w, int nCol, uint32_t *out) {
     CigarOut c{out};
     int i = tlen - 1, j = qlen - 1, state = 0;
     while (i >= 0 || j >= 0) {
@@ -126,7 +129,7 @@ __device__ int global_traceback(const Scratch &s, int qlen, int tlen, int w, int
         const int beg = imax(0, i - w);
         const int col = j - beg;
         if (!(col >= 0 && col < nCol)) break;
-        const uint32_t d = s.Z(i, col);
+        const uint32_t d = zat(i, col);
         if (state == 0) {
             const uint32_t hDir = (d >> 2) & 3u;
             if (hDir == 0) { c.append(0u); --i; --j; }
@@ -155,6 +158,7 @@ __global__ void __launch_bounds__(kGT) global_kernel(GlobalArgs a, Scratch base)
         const size_t k = it * s.nslots + s.slot;
         if (k >= a.n) continue;
         const swb_global_task tk = a.tasks[k];
+        if (tk.qlen <= a.qsplit) continue;
         swb_global_result r{0, 0, tk.w, 1, a.cigar_off[k]};
         const int qlen = tk.qlen, tlen = tk.tlen;
         if (qlen > 0 && tlen > 0) {                                          // :29-31
@@ -179,7 +183,120 @@ __global__ void __launch_bounds__(kGT) global_kernel(GlobalArgs a, Scratch base)
             }
             r.score = score;
             r.w_used = w0;
-            r.n_cigar = global_traceback(s, qlen, tlen, w, nCol, a.cigar + r.cigar_off);
+            r.n_cigar = global_traceback([&](int i, int col) -> uint32_t { return s.Z(i, col); }, qlen, tlen, w, nCol,
+                                             a.cigar + r.cigar_off);
+        }
+        a.res[k] = r;
+    }
+    for (int o = 16; o > 0; o >>= 1) cells += __shfl_down_sync(0xFFFFFFFFu, cells, o);
+    if ((threadIdx.x & 31) == 0 && cells) atomicAdd(a.cells, cells);
+}
+
+// ------------------------------------------------------------------------
+// Shared-memory variant for queries of up to kGlbSmemMaxQ bases: the H/E
+// row of each thread's alignment lives in shared memory ([column][thread],
+// 8 bytes per column), the query codes beside it, and the 4-bit direction
+// codes go to global memory packed 8 per word, laid out
+// [row][word][slot] so a warp's stores of one word index are contiguous.
+// Same recurrences, sentinels and traceback as above.
+constexpr int kGlbSmemMaxQ = kGlobalSmemMaxQ;
+
+struct ZPacked {
+    uint32_t *z;      // this slot's first word
+    size_t nslots;
+    int ncw;          // words per row for this attempt
+    __device__ __forceinline__ uint32_t operator()(int i, int col) const {
+        return (z[((size_t)i * ncw + (col >> 3)) * nslots] >> ((col & 7) << 2)) & 0xFu;
+    }
+};
+
+__device__ int global_dp_smem(const DevScoring &sc, int2 *he, const uint8_t *qs, int T, const GlobalArgs &a,
+                              const swb_global_task &tk, int w, const ZPacked &zp, unsigned long long &cells) {
+    const int qlen = tk.qlen, tlen = tk.tlen;
+    const int oDel = sc.o_del, eDel = sc.e_del, oIns = sc.o_ins, eIns = sc.e_ins;
+    const int oeDel = oDel + eDel, oeIns = oIns + eIns;
+    for (int j = 0; j <= qlen; ++j) he[j * T] = make_int2(kNegInf, kNegInf);    // :75-76
+    he[0].x = 0;                                                                 // :80-84
+    const int initEnd = imin(w, qlen);
+    for (int j = 1; j <= initEnd; ++j) he[j * T].x = 0 - (oIns + eIns * j);
+    const size_t rstride = (size_t)zp.ncw * zp.nslots;
+    for (int i = 0; i < tlen; ++i) {                                             // :89-142
+        const int beg = imax(0, i - w);
+        const int end = (int)min((long long)qlen, (long long)i + w + 1);
+        const RowTable rt = row_table(sc, span_base(a.bases, a.pac, tk.t_off, i, tlen, tk.flags, true));
+        int f = kNegInf;
+        int hDiag = he[beg * T].x;
+        const int hBeg = beg == 0 ? 0 - (oeDel + eDel * i) : kNegInf;
+        he[beg * T].x = hBeg;
+        if (end > beg) cells += (unsigned long long)(end - beg);
+        int hLeft = hBeg;
+        uint32_t *zrow = zp.z + (size_t)i * rstride;
+        uint32_t word = 0;
+        int col = 0;
+        for (int j = beg; j < end; ++j, ++col) {
+            const int2 v = he[(j + 1) * T];
+            int hCur = hDiag + row_score(rt, qs[j * T]);
+            hDiag = v.x;
+            const int eOpen = v.x - oeDel;
+            const int eExtend = v.y - eDel;
+            const uint32_t eFlag = eOpen > eExtend ? 0u : 1u;
+            const int eVal = eOpen > eExtend ? eOpen : eExtend;
+            const int fOpen = hLeft - oeIns;
+            const int fExtend = f - eIns;
+            const uint32_t fFlag = fOpen > fExtend ? 0u : 2u;
+            const int fVal = fOpen > fExtend ? fOpen : fExtend;
+            f = fVal;
+            const uint32_t fromE = eVal > hCur ? 4u : 0u;
+            hCur = eVal > hCur ? eVal : hCur;
+            const uint32_t fromF = fVal > hCur ? 8u : 0u;
+            hCur = fVal > hCur ? fVal : hCur;
+            he[(j + 1) * T] = make_int2(hCur, eVal);
+            hLeft = hCur;
+            word |= (eFlag | fFlag | fromE | fromF) << ((col & 7) << 2);
+            if ((col & 7) == 7) {
+                zrow[(size_t)(col >> 3) * zp.nslots] = word;
+                word = 0;
+            }
+        }
+        if (col & 7) zrow[(size_t)(col >> 3) * zp.nslots] = word;
+    }
+    return he[qlen * T].x;                                                       // :144
+}
+
+__global__ void __launch_bounds__(256) global_smem_kernel(GlobalArgs a, uint32_t *z, size_t nslots, int qcap) {
+    extern __shared__ int2 smem[];
+    const int T = blockDim.x;
+    int2 *he = smem + threadIdx.x;
+    uint8_t *qs = reinterpret_cast<uint8_t *>(smem + (size_t)(qcap + 1) * T) + threadIdx.x;
+    const size_t slot = blockIdx.x * (size_t)T + threadIdx.x;
+    unsigned long long cells = 0;
+    for (size_t k = slot; k < a.n; k += nslots) {
+        const swb_global_task tk = a.tasks[k];
+        if (tk.qlen > qcap) continue;                                    // the global-scratch kernel's
+        swb_global_result r{0, 0, tk.w, 1, a.cigar_off[k]};
+        const int qlen = tk.qlen, tlen = tk.tlen;
+        if (qlen > 0 && tlen > 0) {                                      // :29-31
+            for (int j = 0; j < qlen; ++j) qs[j * T] = (uint8_t)span_base(a.bases, a.pac, tk.q_off, j, qlen, tk.flags, false);
+            int w0 = tk.w;
+            int w = imax(w0, abs(qlen - tlen));                          // :47
+            int nCol = (int)min((long long)qlen, 2ll * w + 1);           // :48
+            ZPacked zp{z + slot, nslots, (nCol + 7) >> 3};
+            int score = global_dp_smem(a.sc, he, qs, T, a, tk, w, zp, cells);
+            if (tk.flags & SWB_GLB_RETRY) {                              // CIGARGenerator.swift:88-96
+                int retries = 0;
+                while (score < tk.true_score && retries < 3) {
+                    w0 *= 2;
+                    ++retries;
+                    r.attempts++;
+                    w = imax(w0, abs(qlen - tlen));
+                    nCol = (int)min((long long)qlen, 2ll * w + 1);
+                    zp.ncw = (nCol + 7) >> 3;
+                    score = global_dp_smem(a.sc, he, qs, T, a, tk, w, zp, cells);
+                }
+            }
+            r.score = score;
+            r.w_used = w0;
+            r.n_cigar = global_traceback(zp, qlen, tlen, w, nCol, a.cigar + r.cigar_off);
         }
         a.res[k] = r;
     }
@@ -202,7 +319,7 @@ namespace swb {
 
 int launch_global(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
                   const swb_global_task *d_tasks, size_t n, swb_global_result *d_res,
-                  uint32_t *d_cigar, unsigned long long *d_cells, cudaStream_t st, int max_q, int max_t) {
+                  uint32_t *d_cigar, unsigned long long *d_cells, cudaStream_t st, const GlobalShape &shape) {
     if (n == 0) return SWB_OK;
     int rc;
     // Per-task CIGAR windows: exclusive prefix sum of (qlen + tlen).
@@ -215,52 +332,84 @@ int launch_global(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     SWB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, lens, offs, (int)n, st));
     if ((rc = ensure_dev(ctx, ctx->d_sort_tmp, tmp))) return rc;
     SWB_CUDA(cub::DeviceScan::ExclusiveSum(ctx->d_sort_tmp.p, tmp, lens, offs, (int)n, st));
+    GlobalArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_res, d_cigar, offs, d_cells + kCntGlobal, n, kGlbSmemMaxQ};
+    const size_t avail0 = ctx->budget > ctx->allocated ? (ctx->budget - ctx->allocated) / 2 : 0;
 
-    const int qmax = imax(max_q, 1), tmax = imax(max_t, 1);
-    // Slots: as many as fit a quarter of the remaining budget, capped at
-    // 8 resident blocks per SM.
-    const size_t per_slot = (size_t)(qmax + 1) * 8 + (size_t)qmax + (size_t)tmax + (size_t)tmax * qmax;
-    size_t nslots = (size_t)ctx->sm_count * 8 * kGT;
-    const size_t avail = ctx->budget > ctx->allocated ? (ctx->budget - ctx->allocated) / 2 : 0;
-    while (nslots > kGT && nslots * per_slot > avail) nslots /= 2;
-    nslots = (nslots / kGT) * kGT;
-    if (nslots == 0 || nslots * per_slot > avail)
-        return set_error(SWB_ERR_OOM, "global alignment scratch does not fit the memory budget");
-    const size_t bytes = nslots * per_slot + 1024;
-    if ((rc = ensure_dev(ctx, ctx->d_scratch, bytes))) return rc;
-    char *p = (char *)ctx->d_scratch.p;
-    Scratch s;
-    s.nslots = nslots;
-    s.slot = 0;
-    s.qmax = qmax;
-    s.tmax = tmax;
-    s.h = (int *)p;
-    p += (size_t)(qmax + 1) * nslots * 4;
-    s.e = (int *)p;
-    p += (size_t)(qmax + 1) * nslots * 4;
-    s.q = (uint8_t *)p;
-    p += (size_t)qmax * nslots;
-    s.t = (uint8_t *)p;
-    p += (size_t)tmax * nslots;
-    s.z = (uint8_t *)p;
-    GlobalArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_res, d_cigar, offs, d_cells + kCntGlobal, n};
-    const size_t grid = std::min(nslots / kGT, (n + kGT - 1) / kGT);
-    s.nslots = grid * kGT;   // fewer tasks than slots: pack the layout tighter
-    // Re-derive pointers for the tighter layout so strides match nslots.
-    p = (char *)ctx->d_scratch.p;
-    s.h = (int *)p;
-    p += (size_t)(qmax + 1) * s.nslots * 4;
-    s.e = (int *)p;
-    p += (size_t)(qmax + 1) * s.nslots * 4;
-    s.q = (uint8_t *)p;
-    p += (size_t)qmax * s.nslots;
-    s.t = (uint8_t *)p;
-    p += (size_t)tmax * s.nslots;
-    s.z = (uint8_t *)p;
+    // Shared-memory kernel: block size and blocks per SM that keep the most
+    // threads resident for this query cap.
+    size_t z_bytes = 0, z_nslots = 0;
+    int qcap = 0, T = 0, grid_s = 0;
+    size_t smem = 0;
+    if (shape.n_small > 0) {
+        qcap = imax(shape.small_q, 1);
+        const size_t per_thread = (size_t)(qcap + 1) * 8 + (size_t)((qcap + 7) & ~7);
+        int sm_bytes = 0, blk_bytes = 0;
+        SWB_CUDA(cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
+        SWB_CUDA(cudaDeviceGetAttribute(&blk_bytes, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+        int best = 0;
+        for (int t = 32; t <= 256; t += 32) {
+            const size_t b = (size_t)t * per_thread;
+            if (b > (size_t)blk_bytes) break;
+            const int blocks = imin((int)((size_t)sm_bytes / (b + 1024)), 2048 / t);
+            if (blocks * t > best) {
+                best = blocks * t;
+                T = t;
+            }
+        }
+        if (T == 0) return set_error(SWB_ERR_TOO_LARGE, "global alignment rows do not fit shared memory");
+        smem = (size_t)T * per_thread;
+        const int bps = best / T;
+        grid_s = (int)std::min<size_t>((size_t)ctx->sm_count * bps, (shape.n_small + T - 1) / T);
+        const size_t per_slot = (size_t)imax(shape.small_t, 1) * (size_t)((qcap + 7) >> 3) * 4;
+        while (grid_s > 1 && (size_t)grid_s * T * per_slot > avail0) grid_s /= 2;
+        z_nslots = (size_t)grid_s * T;
+        z_bytes = (z_nslots * per_slot + 1023) & ~(size_t)1023;
+        if (z_bytes > avail0) return set_error(SWB_ERR_OOM, "global alignment scratch does not fit the memory budget");
+        SWB_CUDA(cudaFuncSetAttribute(global_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    // Global-scratch kernel for longer queries.
+    Scratch s{};
+    size_t big_bytes = 0, grid_b = 0;
+    if (shape.n_big > 0) {
+        const int qmax = imax(shape.big_q, 1), tmax = imax(shape.big_t, 1);
+        const size_t per_slot = (size_t)(qmax + 1) * 8 + (size_t)qmax + (size_t)tmax + (size_t)tmax * qmax;
+        size_t nslots = std::min((size_t)ctx->sm_count * 8 * kGT, ((shape.n_big + kGT - 1) / kGT) * kGT);
+        const size_t avail = avail0 > z_bytes ? avail0 - z_bytes : 0;
+        while (nslots > kGT && nslots * per_slot > avail) nslots /= 2;
+        nslots = (nslots / kGT) * kGT;
+        if (nslots == 0 || nslots * per_slot > avail)
+            return set_error(SWB_ERR_OOM, "global alignment scratch does not fit the memory budget");
+        grid_b = nslots / kGT;
+        big_bytes = nslots * per_slot + 1024;
+        s.nslots = nslots;
+        s.qmax = qmax;
+        s.tmax = tmax;
+    }
+    if ((rc = ensure_dev(ctx, ctx->d_scratch, z_bytes + big_bytes + 256))) return rc;
     ProfScope ps(ctx, st, "global_nw_traceback", kCntGlobal);
-    global_kernel<<<(unsigned)grid, kGT, 0, st>>>(a, s);
-    ctx->launches++;
-    SWB_CUDA(cudaGetLastError());
+    if (shape.n_small > 0) {
+        global_smem_kernel<<<(unsigned)grid_s, T, smem, st>>>(a, (uint32_t *)ctx->d_scratch.p, z_nslots, qcap);
+        ctx->launches++;
+        SWB_CUDA(cudaGetLastError());
+    }
+    if (shape.n_big > 0) {
+        // The big kernel visits every task and skips those of the shared-memory kernel.
+        char *p = (char *)ctx->d_scratch.p + z_bytes;
+        s.slot = 0;
+        s.h = (int *)p;
+        p += (size_t)(s.qmax + 1) * s.nslots * 4;
+        s.e = (int *)p;
+        p += (size_t)(s.qmax + 1) * s.nslots * 4;
+        s.q = (uint8_t *)p;
+        p += (size_t)s.qmax * s.nslots;
+        s.t = (uint8_t *)p;
+        p += (size_t)s.tmax * s.nslots;
+        s.z = (uint8_t *)p;
+        a.qsplit = shape.n_small > 0 ? qcap : 0;
+        global_kernel<<<(unsigned)grid_b, kGT, 0, st>>>(a, s);
+        ctx->launches++;
+        SWB_CUDA(cudaGetLastError());
+    }
     return SWB_OK;
 }
 

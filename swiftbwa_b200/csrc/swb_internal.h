@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -89,7 +90,7 @@ struct swb_ctx {
     size_t pac_bytes = 0;
     // named scratch buffers (grow-only)
     swb::DevBuf d_bases, d_tasks, d_out, d_keys, d_keys2, d_idx, d_idx2, d_sort_tmp, d_misc,
-        d_scratch, d_cigar, d_aux;
+        d_scratch, d_cigar, d_aux, d_chain;
     swb::HostBuf h_in, h_out;
     unsigned long long launches = 0;
     double last_ms = 0.0;
@@ -111,6 +112,8 @@ namespace swb {
 
 // Error plumbing (thread-local message, set by every failing call).
 int set_error(int code, const std::string &msg);
+// Scoring ranges every entry point accepts (SWB_ERR_INVALID_ARG otherwise).
+int validate_scoring(const swb_scoring *sc);
 int check_cuda(cudaError_t e, const char *what);
 #define SWB_CUDA(call)                                               \
     do {                                                             \
@@ -140,11 +143,29 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
                const swb_ext_task *d_tasks, size_t n, swb_ext_result *d_out,
                unsigned long long *d_cells, cudaStream_t stream, int max_q_hint);
 
-// Banded global + traceback (kernel 2).
+// Banded global + traceback (kernel 2).  Tasks with qlen <= kGlobalSmemMaxQ
+// run in the shared-memory kernel, longer ones in the global-scratch kernel;
+// the shape gives each group's count and largest query / target.
+constexpr int kGlobalSmemMaxQ = 256;
+struct GlobalShape {
+    size_t n_small = 0, n_big = 0;
+    int small_q = 0, small_t = 0, big_q = 0, big_t = 0;
+    void add(int qlen, int tlen) {
+        if (qlen <= kGlobalSmemMaxQ) {
+            ++n_small;
+            small_q = std::max(small_q, qlen);
+            small_t = std::max(small_t, tlen);
+        } else {
+            ++n_big;
+            big_q = std::max(big_q, qlen);
+            big_t = std::max(big_t, tlen);
+        }
+    }
+};
 int launch_global(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
                   const swb_global_task *d_tasks, size_t n, swb_global_result *d_res,
                   uint32_t *d_cigar, unsigned long long *d_cells, cudaStream_t stream,
-                  int max_q, int max_t);
+                  const GlobalShape &shape);
 
 // Local SW for mate rescue (kernel 3).
 int launch_local(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,

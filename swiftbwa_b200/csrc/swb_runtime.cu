@@ -93,7 +93,7 @@ static void free_buf(swb_ctx *ctx, DevBuf &b) {
     b.cap = 0;
 }
 
-static int validate_scoring(const swb_scoring *sc) {
+int validate_scoring(const swb_scoring *sc) {
     if (!sc) return set_error(SWB_ERR_INVALID_ARG, "scoring is NULL");
     if (sc->e_ins <= 0 || sc->e_del <= 0 || sc->o_ins < 0 || sc->o_del < 0 || sc->a < 0 || sc->b < 0 ||
         sc->a > 127 || sc->b > 128)
@@ -319,7 +319,7 @@ void swb_destroy(swb_ctx *ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     DevBuf *bufs[] = {&ctx->d_bases, &ctx->d_tasks, &ctx->d_out, &ctx->d_keys, &ctx->d_keys2, &ctx->d_idx,
-                      &ctx->d_idx2, &ctx->d_sort_tmp, &ctx->d_misc, &ctx->d_scratch, &ctx->d_cigar, &ctx->d_aux};
+                      &ctx->d_idx2, &ctx->d_sort_tmp, &ctx->d_misc, &ctx->d_scratch, &ctx->d_cigar, &ctx->d_aux, &ctx->d_chain};
     for (DevBuf *b : bufs) free_buf(ctx, *b);
     if (ctx->d_pac && ctx->pac_owned) cudaFree(ctx->d_pac);
     if (ctx->d_counters) cudaFree(ctx->d_counters);
@@ -471,9 +471,11 @@ int swb_global_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, 
     int max_q = 0, max_t = 0;
     if ((rc = validate_spans(ctx, tasks, n_tasks, n_bases, &max_q, &max_t))) return rc;
     size_t need = 0;
+    GlobalShape shape;
     for (size_t i = 0; i < n_tasks; ++i) {
         need += (size_t)tasks[i].qlen + (size_t)tasks[i].tlen;
         const swb_global_task &t = tasks[i];
+        shape.add(t.qlen, t.tlen);
         if (t.qlen > 0 && t.tlen > 0 && std::max(t.w, std::abs(t.qlen - t.tlen)) < 1)
             return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": band width below 1 with equal lengths");
     }
@@ -488,7 +490,7 @@ int swb_global_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, 
     if ((rc = tm.begin())) return rc;
     if ((rc = launch_global(ctx, dsc, (const uint8_t *)d_b, (const swb_global_task *)d_t, n_tasks,
                             (swb_global_result *)ctx->d_out.p, (uint32_t *)ctx->d_cigar.p, tm.d_cells,
-                            ctx->stream, max_q, max_t)))
+                            ctx->stream, shape)))
         return rc;
     if ((rc = tm.end())) return rc;
     SWB_CUDA(cudaMemcpyAsync(results, ctx->d_out.p, n_tasks * sizeof(swb_global_result), cudaMemcpyDeviceToHost, ctx->stream));

@@ -104,15 +104,18 @@ def test_ext_fuzz_int32_path(engine, oracle_mod):
     assert bad.size == 0, f"{bad.size} mismatches: {got[bad[:3]]} vs {exp[bad[:3]]}"
 
 
-@pytest.mark.parametrize("si", [0, 3, 4])
-def test_global_fuzz(engine, oracle_mod, si):
+@pytest.mark.parametrize("si,qmax", [(0, 200), (3, 200), (4, 200), (0, 420), (5, 420)])
+def test_global_fuzz(engine, oracle_mod, si, qmax):
+    """qmax 420 mixes both kernels in one batch: queries up to 256 bases in
+    the shared-memory kernel, longer ones in the global-scratch kernel."""
     sc = Scoring.default(**SCORINGS[si])
-    d = gen.global_tasks(2000 + si, 1500)
+    d = gen.global_tasks(2000 + si + qmax, 1500, qmax=qmax)
     res, cig = engine.global_batch(sc, d["bases"], d["tasks"])
     eres, ecig, _ = oracle_mod.global_batch(sc, d["bases"], d["tasks"], n_threads=8)
     for k in range(len(res)):
         assert res["score"][k] == eres["score"][k], k
         assert res["n_cigar"][k] == eres["n_cigar"][k], k
+        assert res["w_used"][k] == eres["w_used"][k] and res["attempts"][k] == eres["attempts"][k], k
         o, n = int(res["cigar_off"][k]), int(res["n_cigar"][k])
         eo = int(eres["cigar_off"][k])
         assert np.array_equal(cig[o:o + n], ecig[eo:eo + n]), k
