@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--c4-pool", type=int, default=3_000_000)
     ap.add_argument("--sat-requests", type=int, default=120)
     ap.add_argument("--c5-chains", type=int, default=1_000_000)
+    ap.add_argument("--suite-only", default="",
+                    help="comma list of secondary configs to run alone (config0, config2, config3, config1_nw_cigar, "
+                         "config5_extend_chains, config4); prints their JSON and skips the headline")
     return ap.parse_args()
 
 
@@ -174,7 +177,7 @@ def _pct(xs, q):
     return float(np.percentile(np.asarray(xs), q)) if len(xs) else None
 
 
-def secondary_suite(eng, sc, args, dev, torch, cpu_on=True):
+def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
     """Configs 0, 2, 3, 4, 5 and the config-1 NW+CIGAR stage, each bounded to a
     few seconds of GPU time; CPU-oracle samples beside them."""
     from swiftbwa_b200 import workloads as W
@@ -182,196 +185,207 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True):
     from oracle import oracle
     threads = os.cpu_count() or 1
     out = {}
+
+    def want(name):
+        return only is None or name in only
+
     stream = torch.cuda.Stream(dev)
 
     # ---- config 0: 10k right extensions (host entry point; launch-latency bound)
-    wl0 = W.config0()
-    eng.upload_reference(wl0.ref.pac, wl0.ref.n)
-    eng.ext_batch(sc, wl0.bases, wl0.tasks)
-    t0 = time.perf_counter()
-    for _ in range(5):
-        r0 = eng.ext_batch(sc, wl0.bases, wl0.tasks)
-    e2e0 = (time.perf_counter() - t0) / 5
-    ms0, cells0 = eng.last_batch_stats()
-    exp0, _ = oracle.ext_batch(sc, wl0.bases, wl0.tasks, pac=wl0.ref.pac, ref_bases=wl0.ref.n, n_threads=threads)
-    out["config0"] = {"tasks": len(wl0.tasks), "e2e_ext_per_s": len(wl0.tasks) / e2e0, "kernel_ms": ms0,
-                      "gcups_kernel": cells0 / ms0 / 1e6, "bitexact": bool(np.array_equal(r0, exp0))}
+    if want("config0"):
+        wl0 = W.config0()
+        eng.upload_reference(wl0.ref.pac, wl0.ref.n)
+        eng.ext_batch(sc, wl0.bases, wl0.tasks)
+        t0 = time.perf_counter()
+        for _ in range(5):
+            r0 = eng.ext_batch(sc, wl0.bases, wl0.tasks)
+        e2e0 = (time.perf_counter() - t0) / 5
+        ms0, cells0 = eng.last_batch_stats()
+        exp0, _ = oracle.ext_batch(sc, wl0.bases, wl0.tasks, pac=wl0.ref.pac, ref_bases=wl0.ref.n, n_threads=threads)
+        out["config0"] = {"tasks": len(wl0.tasks), "e2e_ext_per_s": len(wl0.tasks) / e2e0, "kernel_ms": ms0,
+                          "gcups_kernel": cells0 / ms0 / 1e6, "bitexact": bool(np.array_equal(r0, exp0))}
 
     # ---- config 2: 20M uneven extensions, binned (ours) vs the plain single-launch kernel
-    wl2 = W.config2(n=args.c2_tasks)
-    eng.upload_reference(wl2.ref.pac, wl2.ref.n)
-    db = torch.from_numpy(wl2.bases).to(dev)
-    dt = torch.from_numpy(wl2.tasks.view(np.uint8)).to(dev)
-    dpac = torch.from_numpy(wl2.ref.pac).to(dev)
-    n2 = len(wl2.tasks)
-    do = torch.empty(n2 * EXT_RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
-    do2 = torch.empty_like(do)
-    torch.cuda.synchronize()
-    eng.profile(True)
-    eng.profile_reset()
-    ms_b = _cuda_time(torch, stream, lambda: eng.ext_batch_device(sc, db.data_ptr(), dt.data_ptr(), n2, do.data_ptr(),
-                                                                   stream.cuda_stream), 2)
-    prof2 = eng.profile_read()
-    eng.profile(False)
-    cells2 = sum(v[2] for k, v in prof2.items() if k.startswith("ext_")) / 3
-    lib = eng.lib
-    import ctypes as C
+    if want("config2"):
+        wl2 = W.config2(n=args.c2_tasks)
+        eng.upload_reference(wl2.ref.pac, wl2.ref.n)
+        db = torch.from_numpy(wl2.bases).to(dev)
+        dt = torch.from_numpy(wl2.tasks.view(np.uint8)).to(dev)
+        dpac = torch.from_numpy(wl2.ref.pac).to(dev)
+        n2 = len(wl2.tasks)
+        do = torch.empty(n2 * EXT_RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+        do2 = torch.empty_like(do)
+        torch.cuda.synchronize()
+        eng.profile(True)
+        eng.profile_reset()
+        ms_b = _cuda_time(torch, stream, lambda: eng.ext_batch_device(sc, db.data_ptr(), dt.data_ptr(), n2, do.data_ptr(),
+                                                                       stream.cuda_stream), 2)
+        prof2 = eng.profile_read()
+        eng.profile(False)
+        cells2 = sum(v[2] for k, v in prof2.items() if k.startswith("ext_")) / 3
+        lib = eng.lib
+        import ctypes as C
 
-    def plain():
-        rc = lib.swb_ext_batch_static(C.byref(sc), C.c_void_p(db.data_ptr()), C.c_void_p(dpac.data_ptr()),
-                                      C.c_void_p(dt.data_ptr()), n2, C.c_void_p(do2.data_ptr()),
-                                      C.c_void_p(stream.cuda_stream))
-        assert rc == 0, lib.swb_last_error_message()
-    ms_p = _cuda_time(torch, stream, plain, 1)
-    same2 = bool(torch.equal(do, do2))
-    c2 = {"tasks": n2, "binned_ms": ms_b, "binned_ext_per_s": n2 / ms_b * 1e3, "gcups": cells2 / ms_b / 1e6,
-          "plain_kernel_ms": ms_p, "plain_kernel_ext_per_s": n2 / ms_p * 1e3, "speedup_vs_plain": ms_p / ms_b,
-          "plain_kernel": "one launch, input order, one 256-column int16 row layout for every task (swb_ext_batch_static)",
-          "binned_equals_plain": same2}
-    if cpu_on:
-        s2 = 60_000
-        t0 = time.perf_counter()
-        e2, _ = oracle.ext_batch(sc, wl2.bases, wl2.tasks[:s2], pac=wl2.ref.pac, ref_bases=wl2.ref.n, n_threads=threads)
-        c2["cpu_baseline"] = {"value": s2 / (time.perf_counter() - t0), "unit": "ext/s", "cores": threads, "kind": "port",
-                              "sample": f"first {s2} tasks"}
-        g2 = do.cpu().numpy().view(EXT_RESULT_DTYPE)[:s2]
-        c2["bitexact_sample"] = f"{int(np.sum(g2 == e2))}/{s2}"
-    out["config2"] = c2
-    del db, dt, do, do2, dpac
-    torch.cuda.empty_cache()
+        def plain():
+            rc = lib.swb_ext_batch_static(C.byref(sc), C.c_void_p(db.data_ptr()), C.c_void_p(dpac.data_ptr()),
+                                          C.c_void_p(dt.data_ptr()), n2, C.c_void_p(do2.data_ptr()),
+                                          C.c_void_p(stream.cuda_stream))
+            assert rc == 0, lib.swb_last_error_message()
+        ms_p = _cuda_time(torch, stream, plain, 1)
+        same2 = bool(torch.equal(do, do2))
+        c2 = {"tasks": n2, "binned_ms": ms_b, "binned_ext_per_s": n2 / ms_b * 1e3, "gcups": cells2 / ms_b / 1e6,
+              "plain_kernel_ms": ms_p, "plain_kernel_ext_per_s": n2 / ms_p * 1e3, "speedup_vs_plain": ms_p / ms_b,
+              "plain_kernel": "one launch, input order, one 256-column int16 row layout for every task (swb_ext_batch_static)",
+              "binned_equals_plain": same2}
+        if cpu_on:
+            s2 = 60_000
+            t0 = time.perf_counter()
+            e2, _ = oracle.ext_batch(sc, wl2.bases, wl2.tasks[:s2], pac=wl2.ref.pac, ref_bases=wl2.ref.n, n_threads=threads)
+            c2["cpu_baseline"] = {"value": s2 / (time.perf_counter() - t0), "unit": "ext/s", "cores": threads, "kind": "port",
+                                  "sample": f"first {s2} tasks"}
+            g2 = do.cpu().numpy().view(EXT_RESULT_DTYPE)[:s2]
+            c2["bitexact_sample"] = f"{int(np.sum(g2 == e2))}/{s2}"
+        out["config2"] = c2
+        del db, dt, do, do2, dpac
+        torch.cuda.empty_cache()
 
     # ---- config 3: 2M mate-rescue local SW (host entry point)
-    wl3 = W.config3(n=args.c3_pairs)
-    eng.upload_reference(wl3.ref.pac, wl3.ref.n)
-    eng.local_batch(sc, wl3.bases, wl3.tasks[:1000])
-    t0 = time.perf_counter()
-    r3 = eng.local_batch(sc, wl3.bases, wl3.tasks)
-    e2e3 = time.perf_counter() - t0
-    ms3, cells3 = eng.last_batch_stats()
-    c3 = {"pairs": len(wl3.tasks), "kernel_ms": ms3, "rescues_per_s": len(wl3.tasks) / ms3 * 1e3,
-          "e2e_rescues_per_s": len(wl3.tasks) / e2e3, "gcups": cells3 / ms3 / 1e6,
-          "hits": int(np.sum(r3["score"] >= 19))}
-    if cpu_on:
-        s3 = 20_000
+    if want("config3"):
+        wl3 = W.config3(n=args.c3_pairs)
+        eng.upload_reference(wl3.ref.pac, wl3.ref.n)
+        eng.local_batch(sc, wl3.bases, wl3.tasks[:1000])
         t0 = time.perf_counter()
-        e3, _ = oracle.local_batch(sc, wl3.bases, wl3.tasks[:s3], pac=wl3.ref.pac, ref_bases=wl3.ref.n, n_threads=threads)
-        c3["cpu_baseline"] = {"value": s3 / (time.perf_counter() - t0), "unit": "rescues/s", "cores": threads,
-                              "kind": "port", "sample": f"first {s3} pairs"}
-        c3["bitexact_sample"] = f"{int(np.sum(r3[:s3] == e3))}/{s3}"
-    out["config3"] = c3
+        r3 = eng.local_batch(sc, wl3.bases, wl3.tasks)
+        e2e3 = time.perf_counter() - t0
+        ms3, cells3 = eng.last_batch_stats()
+        c3 = {"pairs": len(wl3.tasks), "kernel_ms": ms3, "rescues_per_s": len(wl3.tasks) / ms3 * 1e3,
+              "e2e_rescues_per_s": len(wl3.tasks) / e2e3, "gcups": cells3 / ms3 / 1e6,
+              "hits": int(np.sum(r3["score"] >= 19))}
+        if cpu_on:
+            s3 = 20_000
+            t0 = time.perf_counter()
+            e3, _ = oracle.local_batch(sc, wl3.bases, wl3.tasks[:s3], pac=wl3.ref.pac, ref_bases=wl3.ref.n, n_threads=threads)
+            c3["cpu_baseline"] = {"value": s3 / (time.perf_counter() - t0), "unit": "rescues/s", "cores": threads,
+                                  "kind": "port", "sample": f"first {s3} pairs"}
+            c3["bitexact_sample"] = f"{int(np.sum(r3[:s3] == e3))}/{s3}"
+        out["config3"] = c3
 
     # ---- config 1 NW + CIGAR stage (CIGARGenerator.generate through swb_cigar_batch)
-    wl1 = W.config1(n_reads=args.nw_reads, ref_len=args.ref_len)
-    eng.upload_reference(wl1.ref.pac, wl1.ref.n)
-    info = wl1.read_info
-    ct = np.zeros(len(info), CIGAR_TASK_DTYPE)
-    L = wl1.read_len
-    ct["q_off"] = np.arange(len(info), dtype=np.uint64) * L
-    ct["t_off"] = info[:, 0].astype(np.uint64)
-    ct["qlen"] = L
-    ct["rlen"] = np.minimum(info[:, 1] - info[:, 0], 10_000)
-    ct["qb"] = 0
-    ct["qe"] = L
-    ct["read_len"] = L
-    ct["true_score"] = L - info[:, 2] * 5 - info[:, 3] * 2
-    ct["initial_w"] = 100
-    ct["ref_pos"] = info[:, 0]
-    ct["flags"] = 0x8
-    eng.cigar_batch_raw(sc, wl1.bases, ct[:1000])
-    eng.profile(True)
-    eng.profile_reset()
-    t0 = time.perf_counter()
-    cres, ccig, cmd = eng.cigar_batch_raw(sc, wl1.bases, ct)
-    e2e1 = time.perf_counter() - t0
-    ms1, cells1 = eng.last_batch_stats()
-    prof1 = eng.profile_read()
-    eng.profile(False)
-    n_dp = int(cres["used_dp"].sum())
-    c1 = {"reads": len(ct), "dp_alignments": n_dp, "cigars_per_s": len(ct) / e2e1, "wall_ms": e2e1 * 1e3,
-          "nw_kernel_ms": ms1, "nw_gcups": cells1 / ms1 / 1e6 if ms1 else None,
-          "nw_alignments_per_s": n_dp / ms1 * 1e3 if ms1 else None,
-          "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof1.items()}}
-    if cpu_on:
-        s1 = 3000
+    if want("config1_nw_cigar"):
+        wl1 = W.config1(n_reads=args.nw_reads, ref_len=args.ref_len)
+        eng.upload_reference(wl1.ref.pac, wl1.ref.n)
+        info = wl1.read_info
+        ct = np.zeros(len(info), CIGAR_TASK_DTYPE)
+        L = wl1.read_len
+        ct["q_off"] = np.arange(len(info), dtype=np.uint64) * L
+        ct["t_off"] = info[:, 0].astype(np.uint64)
+        ct["qlen"] = L
+        ct["rlen"] = np.minimum(info[:, 1] - info[:, 0], 10_000)
+        ct["qb"] = 0
+        ct["qe"] = L
+        ct["read_len"] = L
+        ct["true_score"] = L - info[:, 2] * 5 - info[:, 3] * 2
+        ct["initial_w"] = 100
+        ct["ref_pos"] = info[:, 0]
+        ct["flags"] = 0x8
+        eng.cigar_batch_raw(sc, wl1.bases, ct[:1000])
+        eng.profile(True)
+        eng.profile_reset()
         t0 = time.perf_counter()
-        ok = 0
-        mdb = cmd.tobytes()
-        for k in range(s1):
-            q = wl1.bases[k * L:(k + 1) * L]
-            r = wl1.ref.codes[int(ct["t_off"][k]): int(ct["t_off"][k]) + int(ct["rlen"][k])]
-            e = oracle.cigar_generate(q, r, 0, L, L, False, int(ct["true_score"][k]), 100, sc, int(ct["ref_pos"][k]))
-            g = cres[k]
-            o, n, mo, ml = int(g["cigar_off"]), int(g["n_cigar"]), int(g["md_off"]), int(g["md_len"])
-            ok += (e["cigar"], e["nm"], e["md"], e["score"], e["pos"]) == (
-                [int(x) for x in ccig[o:o + n]], int(g["nm"]), mdb[mo:mo + ml].decode(), int(g["score"]), int(g["pos"]))
-        c1["cpu_baseline"] = {"value": s1 / (time.perf_counter() - t0), "unit": "cigars/s", "cores": 1, "kind": "port",
-                              "sample": f"first {s1} reads, one thread (per-call Python loop)"}
-        c1["bitexact_sample"] = f"{ok}/{s1}"
-    out["config1_nw_cigar"] = c1
+        cres, ccig, cmd = eng.cigar_batch_raw(sc, wl1.bases, ct)
+        e2e1 = time.perf_counter() - t0
+        ms1, cells1 = eng.last_batch_stats()
+        prof1 = eng.profile_read()
+        eng.profile(False)
+        n_dp = int(cres["used_dp"].sum())
+        nw_ms = prof1.get("global_nw_traceback", (0, 0.0))[1]
+        c1 = {"reads": len(ct), "dp_alignments": n_dp, "cigars_per_s": len(ct) / e2e1, "wall_ms": e2e1 * 1e3,
+              "device_ms": ms1, "nw_kernel_ms": nw_ms, "nw_gcups": cells1 / nw_ms / 1e6 if nw_ms else None,
+              "nw_alignments_per_s": n_dp / nw_ms * 1e3 if nw_ms else None,
+              "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof1.items()}}
+        if cpu_on:
+            s1 = 3000
+            t0 = time.perf_counter()
+            ok = 0
+            mdb = cmd.tobytes()
+            for k in range(s1):
+                q = wl1.bases[k * L:(k + 1) * L]
+                r = wl1.ref.codes[int(ct["t_off"][k]): int(ct["t_off"][k]) + int(ct["rlen"][k])]
+                e = oracle.cigar_generate(q, r, 0, L, L, False, int(ct["true_score"][k]), 100, sc, int(ct["ref_pos"][k]))
+                g = cres[k]
+                o, n, mo, ml = int(g["cigar_off"]), int(g["n_cigar"]), int(g["md_off"]), int(g["md_len"])
+                ok += (e["cigar"], e["nm"], e["md"], e["score"], e["pos"]) == (
+                    [int(x) for x in ccig[o:o + n]], int(g["nm"]), mdb[mo:mo + ml].decode(), int(g["score"]), int(g["pos"]))
+            c1["cpu_baseline"] = {"value": s1 / (time.perf_counter() - t0), "unit": "cigars/s", "cores": 1, "kind": "port",
+                                  "sample": f"first {s1} reads, one thread (per-call Python loop)"}
+            c1["bitexact_sample"] = f"{ok}/{s1}"
+        out["config1_nw_cigar"] = c1
 
     # ---- config 5: ExtensionAligner.extend over 1M seed chains (swb_extend_chains)
-    wl5 = W.config5(n_reads=args.c5_chains, ref_len=args.ref_len)
-    eng.upload_reference(wl5.ref.pac, wl5.ref.n)
-    eng.extend_chains(sc, wl5.bases, wl5.seeds, wl5.chains[:1000], wl5.ref.n)
-    t0 = time.perf_counter()
-    g5, n5, rounds5 = eng.extend_chains(sc, wl5.bases, wl5.seeds, wl5.chains, wl5.ref.n)
-    e2e5 = time.perf_counter() - t0
-    _, cells5 = eng.last_batch_stats()
-    c5 = {"chains": len(wl5.chains), "seeds": len(wl5.seeds), "regions": int(n5.sum()), "rounds": rounds5,
-          "chains_per_s": len(wl5.chains) / e2e5, "gcups_wall": cells5 / e2e5 / 1e9}
-    if cpu_on:
-        s5 = 100_000
+    if want("config5_extend_chains"):
+        wl5 = W.config5(n_reads=args.c5_chains, ref_len=args.ref_len)
+        eng.upload_reference(wl5.ref.pac, wl5.ref.n)
+        eng.extend_chains(sc, wl5.bases, wl5.seeds, wl5.chains[:1000], wl5.ref.n)
         t0 = time.perf_counter()
-        e5, en5, _ = oracle.extend_batch(sc, wl5.bases, wl5.ref.pac, wl5.ref.n, wl5.seeds, wl5.chains[:s5],
-                                         n_threads=threads)
-        c5["cpu_baseline"] = {"value": s5 / (time.perf_counter() - t0), "unit": "chains/s", "cores": threads,
-                              "kind": "port", "sample": f"first {s5} chains"}
-        ok = int(np.array_equal(n5[:s5], en5))
-        last = int(wl5.chains["seed_off"][s5 - 1] + en5[-1])
-        mask = np.zeros(last, bool)
-        for so, n in zip(wl5.chains["seed_off"][:s5], en5):
-            mask[so:so + n] = True
-        same = int(np.sum(g5[:last][mask] == e5[:last][mask]))
-        c5["bitexact_sample"] = f"{same}/{int(mask.sum())} regions, counts equal: {bool(ok)}"
-    out["config5_extend_chains"] = c5
-    del wl5, g5
+        g5, n5, rounds5 = eng.extend_chains(sc, wl5.bases, wl5.seeds, wl5.chains, wl5.ref.n)
+        e2e5 = time.perf_counter() - t0
+        _, cells5 = eng.last_batch_stats()
+        c5 = {"chains": len(wl5.chains), "seeds": len(wl5.seeds), "regions": int(n5.sum()), "rounds": rounds5,
+              "chains_per_s": len(wl5.chains) / e2e5, "gcups_wall": cells5 / e2e5 / 1e9}
+        if cpu_on:
+            s5 = 100_000
+            t0 = time.perf_counter()
+            e5, en5, _ = oracle.extend_batch(sc, wl5.bases, wl5.ref.pac, wl5.ref.n, wl5.seeds, wl5.chains[:s5],
+                                             n_threads=threads)
+            c5["cpu_baseline"] = {"value": s5 / (time.perf_counter() - t0), "unit": "chains/s", "cores": threads,
+                                  "kind": "port", "sample": f"first {s5} chains"}
+            ok = int(np.array_equal(n5[:s5], en5))
+            last = int(wl5.chains["seed_off"][s5 - 1] + en5[-1])
+            mask = np.zeros(last, bool)
+            for so, n in zip(wl5.chains["seed_off"][:s5], en5):
+                mask[so:so + n] = True
+            same = int(np.sum(g5[:last][mask] == e5[:last][mask]))
+            c5["bitexact_sample"] = f"{same}/{int(mask.sum())} regions, counts equal: {bool(ok)}"
+        out["config5_extend_chains"] = c5
+        del wl5, g5
 
     # ---- config 4: serving, Poisson 200 req/s, 1 Gbp resident reference
-    from swiftbwa_b200 import serving as S
-    ref4 = W.reference(W.SEED_BASE + 4, args.c4_ref_len)
-    eng.upload_reference(ref4.pac, ref4.n)
-    pool = W.uneven(ref4, W.SEED_BASE + 4 + 1, args.c4_pool, name="config4 pool")
-    # The serving process keeps its read chunks in pinned memory, so requests
-    # are zero-copy views of the pool.
-    pb = torch.from_numpy(pool.bases).pin_memory().numpy()
-    pt = torch.from_numpy(pool.tasks.view(np.uint8)).pin_memory().numpy().view(pool.tasks.dtype)
-    po = torch.empty(len(pool.tasks) * EXT_RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy().view(EXT_RESULT_DTYPE)
-    reqs = S.request_stream(W.SEED_BASE + 4 + 2, len(pool.tasks), rate=200.0, duration=args.serve_seconds)
-    srv = S.Server(eng, sc, arena_bytes=1 << 30, max_wave_tasks=1 << 19)
-    res, span = S.run_pool_stream(srv, pb, pt, po, reqs, open_loop=True)
-    st = srv.stats()
-    srv.stop()
-    lat = [l for _, l in res]
-    mid = [l for n, l in res if 50_000 <= n <= 200_000]
-    c4 = {"requests": len(reqs), "tasks": int(sum(n for n, _ in res)), "offered_req_per_s": 200.0,
-          "ext_per_s": sum(n for n, _ in res) / span, "p50_ms": _pct(lat, 50) * 1e3, "p99_ms": _pct(lat, 99) * 1e3,
-          "p50_ms_50k_200k": _pct(mid, 50) * 1e3 if mid else None,
-          "p99_ms_50k_200k": _pct(mid, 99) * 1e3 if mid else None, "n_50k_200k": len(mid),
-          "waves": st["waves"], "wave_device_ms_sum": st["busy_ms"], "span_s": span,
-          "stream": "Poisson 200 req/s, sizes log-uniform 1k-1M tasks, qlen log-uniform 30-250, w 10-100, h0 19-60, "
-                    "1 Gbp resident 2-bit reference"}
-    # saturation: the same size distribution submitted at once, served vs plain
-    sat = S.request_stream(W.SEED_BASE + 4 + 3, len(pool.tasks), rate=1e6, duration=args.sat_requests / 1e6)
-    for mode, plain in (("served", 0), ("plain_batching", 1), ("plain_kernel", 2)):
-        srv = S.Server(eng, sc, arena_bytes=1 << 30, max_wave_tasks=1 << 19 if plain == 0 else 1 << 20, plain=plain)
-        r_, span_ = S.run_pool_stream(srv, pb, pt, po, sat, open_loop=False)
+    if want("config4"):
+        from swiftbwa_b200 import serving as S
+        ref4 = W.reference(W.SEED_BASE + 4, args.c4_ref_len)
+        eng.upload_reference(ref4.pac, ref4.n)
+        pool = W.uneven(ref4, W.SEED_BASE + 4 + 1, args.c4_pool, name="config4 pool")
+        # The serving process keeps its read chunks in pinned memory, so requests
+        # are zero-copy views of the pool.
+        pb = torch.from_numpy(pool.bases).pin_memory().numpy()
+        pt = torch.from_numpy(pool.tasks.view(np.uint8)).pin_memory().numpy().view(pool.tasks.dtype)
+        po = torch.empty(len(pool.tasks) * EXT_RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy().view(EXT_RESULT_DTYPE)
+        reqs = S.request_stream(W.SEED_BASE + 4 + 2, len(pool.tasks), rate=200.0, duration=args.serve_seconds)
+        srv = S.Server(eng, sc, arena_bytes=1 << 30, max_wave_tasks=1 << 19)
+        res, span = S.run_pool_stream(srv, pb, pt, po, reqs, open_loop=True)
+        st = srv.stats()
         srv.stop()
-        c4[f"saturation_{mode}_ext_per_s"] = sum(n for n, _ in r_) / span_
-        c4[f"saturation_{mode}_p99_ms"] = _pct([l for _, l in r_], 99) * 1e3
-    c4["saturation_requests"] = len(sat)
-    c4["served_over_plain_batching"] = c4["saturation_served_ext_per_s"] / c4["saturation_plain_batching_ext_per_s"]
-    c4["served_over_plain_kernel"] = c4["saturation_served_ext_per_s"] / c4["saturation_plain_kernel_ext_per_s"]
-    out["config4"] = c4
+        lat = [l for _, l in res]
+        mid = [l for n, l in res if 50_000 <= n <= 200_000]
+        c4 = {"requests": len(reqs), "tasks": int(sum(n for n, _ in res)), "offered_req_per_s": 200.0,
+              "ext_per_s": sum(n for n, _ in res) / span, "p50_ms": _pct(lat, 50) * 1e3, "p99_ms": _pct(lat, 99) * 1e3,
+              "p50_ms_50k_200k": _pct(mid, 50) * 1e3 if mid else None,
+              "p99_ms_50k_200k": _pct(mid, 99) * 1e3 if mid else None, "n_50k_200k": len(mid),
+              "waves": st["waves"], "wave_device_ms_sum": st["busy_ms"], "span_s": span,
+              "stream": "Poisson 200 req/s, sizes log-uniform 1k-1M tasks, qlen log-uniform 30-250, w 10-100, h0 19-60, "
+                        "1 Gbp resident 2-bit reference"}
+        # saturation: the same size distribution submitted at once, served vs plain
+        sat = S.request_stream(W.SEED_BASE + 4 + 3, len(pool.tasks), rate=1e6, duration=args.sat_requests / 1e6)
+        for mode, plain in (("served", 0), ("plain_batching", 1), ("plain_kernel", 2)):
+            srv = S.Server(eng, sc, arena_bytes=1 << 30, max_wave_tasks=1 << 19 if plain == 0 else 1 << 20, plain=plain)
+            r_, span_ = S.run_pool_stream(srv, pb, pt, po, sat, open_loop=False)
+            srv.stop()
+            c4[f"saturation_{mode}_ext_per_s"] = sum(n for n, _ in r_) / span_
+            c4[f"saturation_{mode}_p99_ms"] = _pct([l for _, l in r_], 99) * 1e3
+        c4["saturation_requests"] = len(sat)
+        c4["served_over_plain_batching"] = c4["saturation_served_ext_per_s"] / c4["saturation_plain_batching_ext_per_s"]
+        c4["served_over_plain_kernel"] = c4["saturation_served_ext_per_s"] / c4["saturation_plain_kernel_ext_per_s"]
+        out["config4"] = c4
     return out
 
 
@@ -435,6 +449,14 @@ def run_ours(args):
     build()
 
     sc = Scoring.default()
+    if args.suite_only:
+        if rank == 0:
+            eng = Engine(local)
+            only = {x.strip() for x in args.suite_only.split(",") if x.strip()}
+            suite = secondary_suite(eng, sc, args, torch.device("cuda", local), torch, cpu_on=not args.no_cpu,
+                                    only=only)
+            print(json.dumps({"suite_only": sorted(only), "configs": suite}), flush=True)
+        return
     t_gen = time.perf_counter()
     wl = W.config1(rank=rank, n_reads=args.n_reads, ref_len=args.ref_len)
     t_gen = time.perf_counter() - t_gen

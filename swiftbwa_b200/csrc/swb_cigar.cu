@@ -1,39 +1,31 @@
 // swb_cigar.cu -- CIGARGenerator.generate for a batch
-// (Sources/Alignment/CIGARGenerator.swift:30-111): the band inference and the
-// pure-M fast path on the host, the banded global alignments with their
-// band-doubling retries on the device (kernel 2), then the reference's
-// post-processing -- deletion squeeze, NM, MD and soft clips -- on host
-// threads, exactly as the reference's own GPU path post-processes on the CPU
-// (CIGARGenerator.postProcess, :118-142).
+// (Sources/Alignment/CIGARGenerator.swift:30-111), device-resident:
+//
+//   host     band inference (inferBandWidth) and the pure-M fast-path test
+//            per task; the tasks needing DP become banded global tasks
+//   kernel 2 the banded global alignments with the band-doubling retries
+//            (launch_global), raw CIGARs in device scratch
+//   measure  per task: deletion squeeze, NM, MD and soft clips walked once to
+//            size the final CIGAR and MD (CIGARGenerator.postProcess :118-142)
+//   scan     exclusive sums of the sizes give compact output offsets
+//   emit     the same walk again, writing the CIGAR words and MD bytes
+//
+// Only the results and the compact CIGAR / MD bytes come back to the host.
 #include <algorithm>
 #include <cstring>
 #include <string>
 #include <thread>
 #include <vector>
 
+#include <cub/device/device_scan.cuh>
+
+#include "swb_device.cuh"
 #include "swb_internal.h"
 
 namespace swb {
 namespace {
 
 enum : uint32_t { kOpM = 0, kOpI = 1, kOpD = 2, kOpS = 4 };
-
-inline uint8_t pac_base(const uint8_t *pac, uint64_t p) { return (uint8_t)((pac[p >> 2] >> ((3u - (p & 3)) << 1)) & 3u); }
-
-// A task span materialised on the host (same flags semantics as the kernels).
-void load_span(const uint8_t *bases, const uint8_t *pac, uint64_t off, int len, uint32_t flags, bool target,
-               std::vector<uint8_t> &dst) {
-    dst.resize((size_t)std::max(len, 0));
-    const bool rev = target ? (flags & SWB_T_REVERSE) : (flags & SWB_Q_REVERSE);
-    const bool comp = target && (flags & SWB_T_COMPLEMENT);
-    const bool ref = target && (flags & SWB_T_FROM_REF);
-    for (int k = 0; k < len; ++k) {
-        const uint64_t i = off + (uint64_t)(rev ? len - 1 - k : k);
-        uint8_t b = ref ? pac_base(pac, i) : bases[i];
-        if (comp && b < 4) b = (uint8_t)(3 - b);
-        dst[(size_t)k] = b;
-    }
-}
 
 // inferBandWidth (:147-170)
 int32_t infer_band_width(int32_t qlen, int32_t rlen, int32_t score, const swb_scoring &sc) {
@@ -46,42 +38,100 @@ int32_t infer_band_width(int32_t qlen, int32_t rlen, int32_t score, const swb_sc
     return std::max(diff + 3, est);
 }
 
-const char kBaseChar[5] = {'A', 'C', 'G', 'T', 'N'};
+struct PostArgs {
+    const uint8_t *bases;
+    const uint8_t *pac;
+    const swb_cigar_task *tasks;
+    const int32_t *dp_index;              // -1: fast path
+    const swb_global_result *gres;
+    const uint32_t *raw;                  // raw CIGARs of the DP tasks
+    swb_cigar_result *res;
+    unsigned long long *cig_len, *md_len; // measure: sizes; emit: compact offsets (after the scans)
+    uint32_t *cig_out;
+    char *md_out;
+    size_t n;
+};
 
-// Squeeze, NM, MD and soft clips of one alignment (:98-108, :118-142).
-void post_process(std::vector<uint32_t> cigar, const std::vector<uint8_t> &q, const std::vector<uint8_t> &r,
-                  const swb_cigar_task &t, int32_t score, bool squeeze, swb_cigar_result &res, uint32_t *cig_out,
-                  char *md_out) {
+__device__ const char kBaseChar[5] = {'A', 'C', 'G', 'T', 'N'};
+
+// Decimal digits of v (v >= 0), written at p when EMIT.
+template <bool EMIT>
+__device__ __forceinline__ int put_uint(char *p, unsigned long long v) {
+    char tmp[20];
+    int n = 0;
+    do {
+        tmp[n++] = (char)('0' + (int)(v % 10));
+        v /= 10;
+    } while (v);
+    if (EMIT)
+        for (int i = 0; i < n; ++i) p[i] = tmp[n - 1 - i];
+    return n;
+}
+
+// Squeeze (squeezeDeletions :272-295), NM (:173-210), MD (:219-268) and
+// soft clips (addSoftClips :298-320) of one task.
+template <bool EMIT>
+__global__ void cigar_post_kernel(PostArgs a) {
+    const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (k >= a.n) return;
+    const swb_cigar_task t = a.tasks[k];
+    const int32_t di = a.dp_index[k];
+    uint32_t one = ((uint32_t)t.qlen << 4) | kOpM;   // fast path: a single M run (:69-80)
+    const uint32_t *ops = &one;
+    int n_ops = 1, score = t.true_score;
+    long lead = 0, trail = 0;
     int64_t pos_adj = 0;
-    size_t ref_off = 0;
-    if (squeeze) {                                               // squeezeDeletions (:272-295)
-        size_t lead = 0;
-        while (lead < cigar.size() && (cigar[lead] & 0xF) == kOpD) {
-            pos_adj += cigar[lead] >> 4;
-            ref_off += cigar[lead] >> 4;
-            ++lead;
-        }
-        cigar.erase(cigar.begin(), cigar.begin() + (long)lead);
-        while (!cigar.empty() && (cigar.back() & 0xF) == kOpD) cigar.pop_back();
+    if (di >= 0) {
+        const swb_global_result g = a.gres[di];
+        ops = a.raw + g.cigar_off;
+        n_ops = g.n_cigar;
+        score = g.score;
+        while (lead < n_ops && (ops[lead] & 0xF) == kOpD) pos_adj += ops[lead++] >> 4;
+        while (n_ops - trail > lead && (ops[n_ops - 1 - trail] & 0xF) == kOpD) ++trail;
     }
-    // NM (:173-210) and MD (:219-268) in one walk.
-    const size_t qn = q.size(), rn = r.size();
+    const size_t ref_off = (size_t)pos_adj;
+    const int qn = t.qlen, rn = t.rlen;
+    uint32_t *cig = nullptr;
+    char *md = nullptr;
+    if (EMIT) {
+        cig = a.cig_out + a.cig_len[k];
+        md = a.md_out + a.md_len[k];
+    }
+    long front, back;
+    if (t.is_reverse) {
+        front = (long)t.read_len - t.qe;
+        back = t.qb;
+    } else {
+        front = t.qb;
+        back = (long)t.read_len - t.qe;
+    }
+    int nc = 0;
+    if (front > 0) {
+        if (EMIT) cig[nc] = ((uint32_t)front << 4) | kOpS;
+        ++nc;
+    }
     size_t qi = 0, ti = ref_off;
     int32_t nm = 0;
-    long match = 0;
-    std::string md;
-    for (uint32_t c : cigar) {
+    unsigned long long match = 0;
+    long mdn = 0;
+    for (long o = lead; o < n_ops - trail; ++o) {
+        const uint32_t c = ops[o];
+        if (EMIT) cig[nc] = c;
+        ++nc;
         const uint32_t op = c & 0xF;
         const size_t len = c >> 4;
         if (op == kOpM) {
             for (size_t x = 0; x < len; ++x)
-                if (qi < qn && ti < rn) {
-                    if (q[qi] == r[ti]) {
+                if (qi < (size_t)qn && ti < (size_t)rn) {
+                    const uint32_t qb = span_base(a.bases, a.pac, t.q_off, (int)qi, qn, t.flags, false);
+                    const uint32_t rb = span_base(a.bases, a.pac, t.t_off, (int)ti, rn, t.flags, true);
+                    if (qb == rb) {
                         ++match;
                     } else {
                         ++nm;
-                        md += std::to_string(match);
-                        md += kBaseChar[std::min<int>(r[ti], 4)];
+                        mdn += put_uint<EMIT>(md + (EMIT ? mdn : 0), match);
+                        if (EMIT) md[mdn] = kBaseChar[rb < 4 ? rb : 4];
+                        ++mdn;
                         match = 0;
                     }
                     ++qi;
@@ -92,49 +142,45 @@ void post_process(std::vector<uint32_t> cigar, const std::vector<uint8_t> &q, co
             qi += len;
         } else if (op == kOpD) {
             nm += (int32_t)len;
-            md += std::to_string(match);
-            md += '^';
+            mdn += put_uint<EMIT>(md + (EMIT ? mdn : 0), match);
+            if (EMIT) md[mdn] = '^';
+            ++mdn;
             for (size_t x = 0; x < len; ++x)
-                if (ti < rn) md += kBaseChar[std::min<int>(r[ti++], 4)];
+                if (ti < (size_t)rn) {
+                    if (EMIT) {
+                        const uint32_t rb = span_base(a.bases, a.pac, t.t_off, (int)ti, rn, t.flags, true);
+                        md[mdn] = kBaseChar[rb < 4 ? rb : 4];
+                    }
+                    ++mdn;
+                    ++ti;
+                }
             match = 0;
         }
     }
-    md += std::to_string(match);
-    // addSoftClips (:298-320)
-    std::vector<uint32_t> out;
-    out.reserve(cigar.size() + 2);
-    long front = 0, back = 0;
-    if (t.is_reverse) {
-        front = (long)t.read_len - t.qe;
-        back = t.qb;
-    } else {
-        front = t.qb;
-        back = (long)t.read_len - t.qe;
+    mdn += put_uint<EMIT>(md + (EMIT ? mdn : 0), match);
+    if (back > 0) {
+        if (EMIT) cig[nc] = ((uint32_t)back << 4) | kOpS;
+        ++nc;
     }
-    if (front > 0) out.push_back(((uint32_t)front << 4) | kOpS);
-    out.insert(out.end(), cigar.begin(), cigar.end());
-    if (back > 0) out.push_back(((uint32_t)back << 4) | kOpS);
-    std::copy(out.begin(), out.end(), cig_out);
-    std::memcpy(md_out, md.c_str(), md.size() + 1);
-    res.score = score;
-    res.nm = nm;
-    res.n_cigar = (int32_t)out.size();
-    res.md_len = (int32_t)md.size();
-    res.pos = t.ref_pos + pos_adj;
+    if (EMIT) {
+        md[mdn] = '\0';
+        swb_cigar_result r{};
+        r.score = score;
+        r.nm = nm;
+        r.n_cigar = nc;
+        r.md_len = (int32_t)mdn;
+        r.pos = t.ref_pos + pos_adj;
+        r.cigar_off = a.cig_len[k];
+        r.md_off = a.md_len[k];
+        r.used_dp = di >= 0;
+        a.res[k] = r;
+    } else {
+        a.cig_len[k] = (unsigned long long)nc;
+        a.md_len[k] = (unsigned long long)mdn + 1;
+    }
 }
 
-template <class F>
-void parallel(size_t n, F fn) {
-    const size_t nth = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), (n + 4095) / 4096);
-    if (nth <= 1) {
-        fn(0, n);
-        return;
-    }
-    std::vector<std::thread> th;
-    const size_t per = (n + nth - 1) / nth;
-    for (size_t k = 0; k < nth; ++k) th.emplace_back([&, k] { fn(k * per, std::min(n, (k + 1) * per)); });
-    for (auto &x : th) x.join();
-}
+inline size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 }  // namespace
 }  // namespace swb
@@ -147,82 +193,167 @@ extern "C" int swb_cigar_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_
     if (!ctx || !sc || (!tasks && n_tasks) || (!results && n_tasks) || (!bases && n_bases) ||
         (!cigar_out && n_tasks) || (!md_out && n_tasks))
         return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
+    int rc;
+    if ((rc = validate_scoring(sc))) return rc;
     if (n_tasks == 0) return SWB_OK;
-    // Offsets, validation and the fast-path decision (:44-80).
-    std::vector<uint64_t> coff(n_tasks + 1, 0), moff(n_tasks + 1, 0);
-    for (size_t i = 0; i < n_tasks; ++i) {
-        const swb_cigar_task &t = tasks[i];
-        if (t.qlen < 0 || t.rlen < 0) return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": negative length");
-        if (t.qlen > kMaxLen || t.rlen > kMaxLen) return set_error(SWB_ERR_TOO_LARGE, "task " + std::to_string(i) + ": length above 65535");
-        if (t.qlen > 0 && t.q_off + (uint64_t)t.qlen > n_bases)
-            return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": query span outside bases");
-        if (t.rlen > 0) {
-            if (t.flags & SWB_T_FROM_REF) {
-                if (ctx->h_pac.empty()) return set_error(SWB_ERR_NO_REFERENCE, "task reads the reference but none is uploaded");
-                if (t.t_off + (uint64_t)t.rlen > ctx->ref_bases)
-                    return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": reference span outside reference");
-            } else if (t.t_off + (uint64_t)t.rlen > n_bases) {
-                return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": reference span outside bases");
-            }
-        }
-        coff[i + 1] = coff[i] + (uint64_t)t.qlen + (uint64_t)t.rlen + 2;
-        moff[i + 1] = moff[i] + 6ull * ((uint64_t)t.qlen + (uint64_t)t.rlen) + 8;
-    }
-    if (coff[n_tasks] > cigar_cap) return set_error(SWB_ERR_INVALID_ARG, "cigar_cap below sum of (qlen + rlen + 2)");
-    if (moff[n_tasks] > md_cap) return set_error(SWB_ERR_INVALID_ARG, "md_cap below sum of (6*(qlen+rlen)+8)");
-    const int32_t min_indel = sc->o_ins + sc->e_ins + sc->o_del + sc->e_del;
+    if (n_tasks > 0x7FFFFFF0ull) return set_error(SWB_ERR_TOO_LARGE, "more than 2^31-16 tasks in one batch");
+    // Validation, the capacity rule and the fast-path decision (:44-80), in parallel.
     std::vector<uint8_t> fast(n_tasks, 0);
+    std::vector<int> bad_code(std::max(1u, std::thread::hardware_concurrency()), 0);
+    std::vector<std::string> bad_msg(bad_code.size());
+    std::vector<unsigned long long> cap_c(bad_code.size(), 0), cap_m(bad_code.size(), 0);
+    const int32_t min_indel = sc->o_ins + sc->e_ins + sc->o_del + sc->e_del;
+    const bool have_ref = ctx->d_pac != nullptr;
+    {
+        const size_t nth = bad_code.size();
+        const size_t per = (n_tasks + nth - 1) / nth;
+        std::vector<std::thread> th;
+        for (size_t w = 0; w < nth; ++w)
+            th.emplace_back([&, w] {
+                const size_t lo = std::min(n_tasks, w * per), hi = std::min(n_tasks, lo + per);
+                unsigned long long cc = 0, cm = 0;
+                for (size_t i = lo; i < hi; ++i) {
+                    const swb_cigar_task &t = tasks[i];
+                    const char *why = nullptr;
+                    int code = SWB_ERR_INVALID_ARG;
+                    if (t.qlen < 0 || t.rlen < 0) why = "negative length";
+                    else if (t.qlen > kMaxLen || t.rlen > kMaxLen) why = "length above 65535", code = SWB_ERR_TOO_LARGE;
+                    else if (t.qlen > 0 && t.q_off + (uint64_t)t.qlen > n_bases) why = "query span outside bases";
+                    else if (t.rlen > 0 && (t.flags & SWB_T_FROM_REF) && !have_ref)
+                        why = "task reads the reference but none is uploaded", code = SWB_ERR_NO_REFERENCE;
+                    else if (t.rlen > 0 && (t.flags & SWB_T_FROM_REF) && t.t_off + (uint64_t)t.rlen > ctx->ref_bases)
+                        why = "reference span outside reference";
+                    else if (t.rlen > 0 && !(t.flags & SWB_T_FROM_REF) && t.t_off + (uint64_t)t.rlen > n_bases)
+                        why = "reference span outside bases";
+                    if (why) {
+                        bad_code[w] = code;
+                        bad_msg[w] = "task " + std::to_string(i) + ": " + why;
+                        return;
+                    }
+                    cc += (unsigned long long)t.qlen + (unsigned long long)t.rlen + 2;
+                    cm += 6ull * ((unsigned long long)t.qlen + (unsigned long long)t.rlen) + 8;
+                    const int32_t deficit = t.qlen * sc->a - t.true_score;
+                    fast[i] = t.qlen == t.rlen && t.qlen > 0 && deficit < min_indel;
+                }
+                cap_c[w] = cc;
+                cap_m[w] = cm;
+            });
+        for (auto &x : th) x.join();
+    }
+    unsigned long long need_c = 0, need_m = 0;
+    for (size_t w = 0; w < bad_code.size(); ++w) {
+        if (bad_code[w]) return set_error(bad_code[w], bad_msg[w]);
+        need_c += cap_c[w];
+        need_m += cap_m[w];
+    }
+    if (need_c > cigar_cap) return set_error(SWB_ERR_INVALID_ARG, "cigar_cap below sum of (qlen + rlen + 2)");
+    if (need_m > md_cap) return set_error(SWB_ERR_INVALID_ARG, "md_cap below sum of (6*(qlen+rlen)+8)");
+    // Global tasks for the rest, with the inferred band (:82-96).
     std::vector<swb_global_task> dp;
-    std::vector<size_t> dp_of;
+    std::vector<int32_t> dp_index(n_tasks, -1);
+    GlobalShape shape;
+    size_t raw_words = 0;
     for (size_t i = 0; i < n_tasks; ++i) {
+        if (fast[i]) continue;
         const swb_cigar_task &t = tasks[i];
-        int32_t w = infer_band_width(t.qe - t.qb, t.rlen, t.true_score, *sc);
-        w = std::max(w, t.initial_w);
-        const int32_t deficit = t.qlen * sc->a - t.true_score;
-        if (t.qlen == t.rlen && t.qlen > 0 && deficit < min_indel) {
-            fast[i] = 1;
-        } else {
-            dp.push_back(swb_global_task{t.q_off, t.t_off, t.qlen, t.rlen, w, t.true_score,
-                                         (t.flags & (SWB_Q_REVERSE | SWB_T_REVERSE | SWB_T_COMPLEMENT | SWB_T_FROM_REF)) |
-                                             SWB_GLB_RETRY,
-                                         0});
-            dp_of.push_back(i);
-        }
+        const int32_t w = std::max(infer_band_width(t.qe - t.qb, t.rlen, t.true_score, *sc), t.initial_w);
+        if (t.qlen > 0 && t.rlen > 0 && std::max(w, std::abs(t.qlen - t.rlen)) < 1)
+            return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": band width below 1 with equal lengths");
+        dp_index[i] = (int32_t)dp.size();
+        dp.push_back(swb_global_task{t.q_off, t.t_off, t.qlen, t.rlen, w, t.true_score,
+                                     (t.flags & (SWB_Q_REVERSE | SWB_T_REVERSE | SWB_T_COMPLEMENT | SWB_T_FROM_REF)) |
+                                         SWB_GLB_RETRY,
+                                     0});
+        shape.add(t.qlen, t.rlen);
+        raw_words += (size_t)t.qlen + (size_t)t.rlen;
     }
-    // Device DP for the rest (the ABI's global batch: DP, retries, traceback).
-    std::vector<swb_global_result> dres(dp.size());
-    std::vector<uint32_t> dcig;
-    if (!dp.empty()) {
-        size_t need = 0;
-        for (const auto &g : dp) need += (size_t)g.qlen + (size_t)g.tlen;
-        dcig.resize(std::max<size_t>(need, 1));
-        const int rc = swb_global_batch(ctx, sc, bases, n_bases, dp.data(), dp.size(), dres.data(), dcig.data(), dcig.size());
-        if (rc) return rc;
+
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->last_ms = 0;
+    ctx->last_cells = 0;
+    SWB_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const size_t n = n_tasks, nd = dp.size();
+    size_t off = 0;
+    auto carve = [&](size_t bytes) {
+        const size_t o = off;
+        off += al256(bytes);
+        return o;
+    };
+    const size_t o_bases = carve(std::max<size_t>(n_bases, 1)), o_tasks = carve(n * sizeof(swb_cigar_task));
+    const size_t o_dpi = carve(n * 4), o_dp = carve(std::max<size_t>(nd, 1) * sizeof(swb_global_task));
+    const size_t o_gres = carve(std::max<size_t>(nd, 1) * sizeof(swb_global_result));
+    const size_t o_res = carve(n * sizeof(swb_cigar_result));
+    const size_t o_cl = carve(n * 8), o_ml = carve(n * 8), o_co = carve(n * 8), o_mo = carve(n * 8);
+    if ((rc = ensure_dev(ctx, ctx->d_chain, off)) ||
+        (rc = ensure_dev(ctx, ctx->d_cigar, std::max<size_t>(raw_words, 1) * sizeof(uint32_t))))
+        return rc;
+    char *base = (char *)ctx->d_chain.p;
+    unsigned long long *d_cl = (unsigned long long *)(base + o_cl), *d_ml = (unsigned long long *)(base + o_ml);
+    unsigned long long *d_co = (unsigned long long *)(base + o_co), *d_mo = (unsigned long long *)(base + o_mo);
+    SWB_CUDA(cudaMemsetAsync(ctx->d_counters, 0, sizeof(unsigned long long) * kNumCounters, st));
+    SWB_CUDA(cudaEventRecord(ctx->ev_start, st));
+    if (n_bases) SWB_CUDA(cudaMemcpyAsync(base + o_bases, bases, n_bases, cudaMemcpyHostToDevice, st));
+    SWB_CUDA(cudaMemcpyAsync(base + o_tasks, tasks, n * sizeof(swb_cigar_task), cudaMemcpyHostToDevice, st));
+    SWB_CUDA(cudaMemcpyAsync(base + o_dpi, dp_index.data(), n * 4, cudaMemcpyHostToDevice, st));
+    if (nd) {
+        SWB_CUDA(cudaMemcpyAsync(base + o_dp, dp.data(), nd * sizeof(swb_global_task), cudaMemcpyHostToDevice, st));
+        if ((rc = launch_global(ctx, make_dev_scoring(*sc), (const uint8_t *)(base + o_bases),
+                                (const swb_global_task *)(base + o_dp), nd, (swb_global_result *)(base + o_gres),
+                                (uint32_t *)ctx->d_cigar.p, ctx->d_counters, st, shape)))
+            return rc;
     }
-    std::vector<int64_t> dp_index(n_tasks, -1);
-    for (size_t k = 0; k < dp_of.size(); ++k) dp_index[dp_of[k]] = (int64_t)k;
-    const uint8_t *hpac = ctx->h_pac.empty() ? nullptr : ctx->h_pac.data();
-    parallel(n_tasks, [&](size_t lo, size_t hi) {
-        std::vector<uint8_t> q, r;
-        for (size_t i = lo; i < hi; ++i) {
-            const swb_cigar_task &t = tasks[i];
-            load_span(bases, hpac, t.q_off, t.qlen, t.flags, false, q);
-            load_span(bases, hpac, t.t_off, t.rlen, t.flags, true, r);
-            swb_cigar_result &res = results[i];
-            res = swb_cigar_result{};
-            res.cigar_off = coff[i];
-            res.md_off = moff[i];
-            if (fast[i]) {                                             // :69-80
-                post_process({((uint32_t)t.qlen << 4) | kOpM}, q, r, t, t.true_score, false, res, cigar_out + coff[i],
-                             md_out + moff[i]);
-                res.used_dp = 0;
-            } else {                                                   // :82-110
-                const swb_global_result &g = dres[(size_t)dp_index[i]];
-                std::vector<uint32_t> raw(dcig.begin() + (long)g.cigar_off, dcig.begin() + (long)(g.cigar_off + (uint64_t)g.n_cigar));
-                post_process(std::move(raw), q, r, t, g.score, true, res, cigar_out + coff[i], md_out + moff[i]);
-                res.used_dp = 1;
-            }
-        }
-    });
+    PostArgs pa{(const uint8_t *)(base + o_bases), ctx->d_pac, (const swb_cigar_task *)(base + o_tasks),
+                (const int32_t *)(base + o_dpi), (const swb_global_result *)(base + o_gres),
+                (const uint32_t *)ctx->d_cigar.p, (swb_cigar_result *)(base + o_res), d_cl, d_ml, nullptr, nullptr, n};
+    const unsigned tb = 128;
+    const unsigned grid = (unsigned)((n + tb - 1) / tb);
+    {
+        ProfScope ps(ctx, st, "cigar_post_measure", -1);
+        cigar_post_kernel<false><<<grid, tb, 0, st>>>(pa);
+        ctx->launches++;
+        SWB_CUDA(cudaGetLastError());
+    }
+    // Compact offsets: exclusive sums of the sizes; each total is the last
+    // offset plus the last size.
+    size_t tmp = 0, tmp2 = 0;
+    SWB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, d_cl, d_co, (int)n, st));
+    SWB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp2, d_ml, d_mo, (int)n, st));
+    if ((rc = ensure_dev(ctx, ctx->d_sort_tmp, std::max(tmp, tmp2)))) return rc;
+    SWB_CUDA(cub::DeviceScan::ExclusiveSum(ctx->d_sort_tmp.p, tmp, d_cl, d_co, (int)n, st));
+    SWB_CUDA(cub::DeviceScan::ExclusiveSum(ctx->d_sort_tmp.p, tmp2, d_ml, d_mo, (int)n, st));
+    unsigned long long last[4];
+    SWB_CUDA(cudaMemcpyAsync(&last[0], d_co + (n - 1), 8, cudaMemcpyDeviceToHost, st));
+    SWB_CUDA(cudaMemcpyAsync(&last[1], d_cl + (n - 1), 8, cudaMemcpyDeviceToHost, st));
+    SWB_CUDA(cudaMemcpyAsync(&last[2], d_mo + (n - 1), 8, cudaMemcpyDeviceToHost, st));
+    SWB_CUDA(cudaMemcpyAsync(&last[3], d_ml + (n - 1), 8, cudaMemcpyDeviceToHost, st));
+    SWB_CUDA(cudaStreamSynchronize(st));
+    const size_t tot_c = (size_t)(last[0] + last[1]), tot_m = (size_t)(last[2] + last[3]);
+    if ((rc = ensure_dev(ctx, ctx->d_aux, al256(tot_c * 4) + al256(tot_m)))) return rc;
+    uint32_t *d_cig = (uint32_t *)ctx->d_aux.p;
+    char *d_md = (char *)ctx->d_aux.p + al256(tot_c * 4);
+    pa.cig_len = d_co;
+    pa.md_len = d_mo;
+    pa.cig_out = d_cig;
+    pa.md_out = d_md;
+    {
+        ProfScope ps(ctx, st, "cigar_post_emit", -1);
+        cigar_post_kernel<true><<<grid, tb, 0, st>>>(pa);
+        ctx->launches++;
+        SWB_CUDA(cudaGetLastError());
+    }
+    SWB_CUDA(cudaMemcpyAsync(results, base + o_res, n * sizeof(swb_cigar_result), cudaMemcpyDeviceToHost, st));
+    if (tot_c) SWB_CUDA(cudaMemcpyAsync(cigar_out, d_cig, tot_c * 4, cudaMemcpyDeviceToHost, st));
+    if (tot_m) SWB_CUDA(cudaMemcpyAsync(md_out, d_md, tot_m, cudaMemcpyDeviceToHost, st));
+    SWB_CUDA(cudaEventRecord(ctx->ev_stop, st));
+    SWB_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) ctx->last_ms = ms;
+    unsigned long long c[kNumCounters] = {0};
+    if (cudaMemcpy(c, ctx->d_counters, sizeof(c), cudaMemcpyDeviceToHost) == cudaSuccess) {
+        unsigned long long sum = 0;
+        for (int k = 0; k < kNumCounters; ++k) sum += c[k];
+        ctx->last_cells = sum;
+    }
     return SWB_OK;
 }

@@ -85,7 +85,6 @@ struct swb_ctx {
     // resident 2-bit reference (.pac layout)
     uint8_t *d_pac = nullptr;
     bool pac_owned = true;        // false for a server lane sharing its parent's reference
-    std::vector<uint8_t> h_pac;   // host copy, for host-side post-processing of reference spans
     uint64_t ref_bases = 0;
     size_t pac_bytes = 0;
     // named scratch buffers (grow-only)

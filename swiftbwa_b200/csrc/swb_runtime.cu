@@ -361,7 +361,6 @@ int swb_upload_reference(swb_ctx *ctx, const uint8_t *pac, uint64_t n_bases) {
         ctx->d_pac = nullptr;
         ctx->pac_bytes = 0;
         ctx->ref_bases = 0;
-        ctx->h_pac.clear();
     }
     if (n_bases == 0) return SWB_OK;
     if (ctx->allocated + bytes + 16 > ctx->budget) return set_error(SWB_ERR_OOM, "reference exceeds the memory budget");
@@ -369,7 +368,6 @@ int swb_upload_reference(swb_ctx *ctx, const uint8_t *pac, uint64_t n_bases) {
     ctx->pac_bytes = bytes + 16;
     ctx->allocated += ctx->pac_bytes;
     SWB_CUDA(cudaMemcpy(ctx->d_pac, pac, bytes, cudaMemcpyHostToDevice));
-    ctx->h_pac.assign(pac, pac + bytes);
     ctx->ref_bases = n_bases;
     return SWB_OK;
 }
