@@ -57,9 +57,10 @@ def parse():
     ap.add_argument("--c4-pool", type=int, default=3_000_000)
     ap.add_argument("--sat-requests", type=int, default=120)
     ap.add_argument("--c5-chains", type=int, default=1_000_000)
+    ap.add_argument("--c3-jobs", type=int, default=1_000_000)
     ap.add_argument("--suite-only", default="",
-                    help="comma list of secondary configs to run alone (config0, config2, config3, config1_nw_cigar, "
-                         "config5_extend_chains, config4); prints their JSON and skips the headline")
+                    help="comma list of secondary configs to run alone (config0, config2, config3, config3_rescue_driver, "
+                         "config1_nw_cigar, config5_extend_chains, config4); prints their JSON and skips the headline")
     return ap.parse_args()
 
 
@@ -270,6 +271,41 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
             c3["bitexact_sample"] = f"{int(np.sum(r3[:s3] == e3))}/{s3}"
         out["config3"] = c3
 
+    # ---- config 3 rescue driver: MateRescue.rescue over 1M mates (swb_mate_rescue)
+    if want("config3_rescue_driver"):
+        wr = W.config3_jobs(n=args.c3_jobs, ref_len=args.ref_len)
+        eng.upload_reference(wr.ref.pac, wr.ref.n)
+        rargs = (wr.bases, wr.jobs, wr.templates, wr.mate_regions, wr.stats, wr.primary, wr.contig_offsets,
+                 wr.contig_lengths, wr.ref.n)
+        eng.mate_rescue(sc, *rargs)
+        times = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            gr, gn, gc = eng.mate_rescue(sc, *rargs)
+            times.append(time.perf_counter() - t0)
+        e2er = float(np.median(times))
+        msr, cellsr = eng.last_batch_stats()
+        cr = {"mates": len(wr.jobs), "templates": len(wr.templates), "local_alignments": int(gc.sum()),
+              "rescued": int(gn.sum()), "mates_per_s": len(wr.jobs) / e2er, "wall_ms": e2er * 1e3,
+              "device_ms": msr, "gcups_device": cellsr / msr / 1e6 if msr else None, "workload": wr.name}
+        if cpu_on:
+            sr = 20_000
+            t0 = time.perf_counter()
+            er, en, ec, _ = oracle.mate_rescue_batch(sc, wr.bases, wr.ref.pac, wr.ref.n, wr.jobs[:sr], wr.templates,
+                                                     wr.mate_regions, wr.stats, wr.primary, wr.contig_offsets,
+                                                     wr.contig_lengths, n_threads=threads)
+            cr["cpu_baseline"] = {"value": sr / (time.perf_counter() - t0), "unit": "mates/s", "cores": threads,
+                                  "kind": "port", "sample": f"first {sr} mates"}
+            same = bool(np.array_equal(gn[:sr], en) and np.array_equal(gc[:sr], ec))
+            for j in range(sr):
+                o = 4 * int(wr.jobs["tmpl_off"][j])
+                if not np.array_equal(gr[o:o + int(en[j])], er[o:o + int(en[j])]):
+                    same = False
+                    break
+            cr["bitexact_sample"] = f"{sr} mates: {'all equal' if same else 'DIFFERENT'}"
+        out["config3_rescue_driver"] = cr
+        del wr
+
     # ---- config 1 NW + CIGAR stage (CIGARGenerator.generate through swb_cigar_batch)
     if want("config1_nw_cigar"):
         wl1 = W.config1(n_reads=args.nw_reads, ref_len=args.ref_len)
@@ -325,10 +361,13 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
     if want("config5_extend_chains"):
         wl5 = W.config5(n_reads=args.c5_chains, ref_len=args.ref_len)
         eng.upload_reference(wl5.ref.pac, wl5.ref.n)
-        eng.extend_chains(sc, wl5.bases, wl5.seeds, wl5.chains[:1000], wl5.ref.n)
-        t0 = time.perf_counter()
-        g5, n5, rounds5 = eng.extend_chains(sc, wl5.bases, wl5.seeds, wl5.chains, wl5.ref.n)
-        e2e5 = time.perf_counter() - t0
+        eng.extend_chains(sc, wl5.bases, wl5.seeds, wl5.chains, wl5.ref.n)
+        times = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            g5, n5, rounds5 = eng.extend_chains(sc, wl5.bases, wl5.seeds, wl5.chains, wl5.ref.n)
+            times.append(time.perf_counter() - t0)
+        e2e5 = float(np.median(times))
         _, cells5 = eng.last_batch_stats()
         c5 = {"chains": len(wl5.chains), "seeds": len(wl5.seeds), "regions": int(n5.sum()), "rounds": rounds5,
               "chains_per_s": len(wl5.chains) / e2e5, "gcups_wall": cells5 / e2e5 / 1e9}

@@ -305,6 +305,63 @@ int swb_extend_chains(swb_ctx *ctx, const swb_scoring *sc,
                       const swb_chain *chains, size_t n_chains, uint64_t genome_len,
                       swb_region *out, uint32_t *n_regions, uint32_t *rounds);
 
+/* ------------------------------------------------ mate rescue (MateRescue.swift) */
+/* Insert-size statistics of one pair orientation, the fields mate rescue
+ * reads (OrientationStats, Sources/BWAMem/InsertSizeEstimator.swift:21-35).
+ * Orientations are indexed FF 0, FR 1, RF 2, RR 3. */
+typedef struct swb_orientation {
+    int32_t failed;           /* nonzero: orientation skipped */
+    int32_t reserved;
+    int64_t proper_low, proper_high;
+} swb_orientation;           /* 24 bytes */
+
+/* The two MemAlnReg fields rescue reads from template and mate regions. */
+typedef struct swb_anchor {
+    int64_t rb;               /* BWT coordinate, [0, 2*genome_len) */
+    int32_t rid;
+    int32_t reserved;
+} swb_anchor;                /* 16 bytes */
+
+/* One MateRescue.rescue call: the mate read bases[mate_off ..+mate_len),
+ * its template regions templates[tmpl_off ..+n_tmpl) and the mate's own
+ * regions mate_regions[mreg_off ..+n_mreg). */
+typedef struct swb_rescue_job {
+    uint64_t mate_off;
+    int32_t  mate_len;
+    int32_t  reserved;
+    uint32_t tmpl_off, n_tmpl;
+    uint32_t mreg_off, n_mreg;
+} swb_rescue_job;            /* 32 bytes */
+
+/* A rescued region: the MemAlnReg fields MateRescue sets (MateRescue.swift:
+ * 133-163); the others keep MemAlnReg() defaults (sub 0, subN 0, w 0,
+ * secondary -1, seedLen0 0). */
+typedef struct swb_rescued {
+    int64_t rb, re;
+    int32_t qb, qe;
+    int32_t rid, score, true_score, csub, seed_cov, reserved;
+} swb_rescued;               /* 48 bytes */
+
+/* MateRescue.rescue (Sources/BWAMem/MateRescue.swift:29-171) for many
+ * mates: for each template region and each non-failed orientation without a
+ * consistent mate hit, the rescue window is clamped, fetched from the
+ * resident reference strand-aware within the template's contig
+ * (PackedReference.fetchSequence, PackedReference.swift:73-121), aligned
+ * with LocalSWAligner.align (minSubScore = UInt8(clamping: min_seed_len*a))
+ * and kept when score >= min_seed_len*a.  Contigs are given by their
+ * offsets (ascending) and lengths in the forward strand (ReferenceMetadata
+ * annotations).  Job j's regions are out[4*tmpl_off ..+n_out[j]), in the
+ * reference's order; out must hold 4*n_templates entries.  n_cand (optional)
+ * receives the local alignments run per job. */
+int swb_mate_rescue(swb_ctx *ctx, const swb_scoring *sc,
+                    const uint8_t *bases, size_t n_bases,
+                    const swb_rescue_job *jobs, size_t n_jobs,
+                    const swb_anchor *templates, size_t n_templates,
+                    const swb_anchor *mate_regions, size_t n_mate_regions,
+                    const swb_orientation stats[4], int32_t primary_orientation,
+                    const int64_t *contig_offsets, const int32_t *contig_lengths, size_t n_contigs,
+                    uint64_t genome_len, swb_rescued *out, uint32_t *n_out, uint32_t *n_cand);
+
 /* ------------------------------------------------ serving (continuous batching) */
 /* A request loop over one context's GPU for extension batches of differing
  * sizes that arrive concurrently (the actor loop of BWAMemAligner's

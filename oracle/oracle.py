@@ -92,6 +92,10 @@ def lib() -> C.CDLL:
         L.orc_extend_batch.argtypes = [P(Scoring), u8p, u8p, C.c_int64, C.c_void_p, C.c_void_p, C.c_size_t,
                                        C.c_void_p, P(C.c_uint32), C.c_int, P(C.c_uint64)]
         L.orc_extend_batch.restype = C.c_int
+        L.orc_mate_rescue_batch.argtypes = [P(Scoring), u8p, u8p, C.c_int64, C.c_void_p, C.c_size_t, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_size_t,
+                                            C.c_void_p, P(C.c_uint32), P(C.c_uint32), C.c_int, P(C.c_uint64)]
+        L.orc_mate_rescue_batch.restype = C.c_int
         _lib = L
     return _lib
 
@@ -267,3 +271,29 @@ def extend_batch(sc: Scoring, bases: np.ndarray, pac: np.ndarray, genome_len: in
     if rc != 0:
         raise ValueError("extend_batch failed")
     return out, counts[:len(chains)], cells.value
+
+
+def mate_rescue_batch(sc: Scoring, bases: np.ndarray, pac: np.ndarray, genome_len: int, jobs: np.ndarray,
+                      templates: np.ndarray, mate_regions: np.ndarray, stats: np.ndarray, primary: int,
+                      contig_offsets: np.ndarray, contig_lengths: np.ndarray, n_threads: int = 1):
+    """MateRescue.rescue for every job (RESCUE_JOB_DTYPE) -> (RESCUED_DTYPE array
+    laid out like swb_mate_rescue's output, per-job counts, per-job local
+    alignments run, cells)."""
+    from swiftbwa_b200.abi import ANCHOR_DTYPE, RESCUED_DTYPE
+    out = np.zeros(max(4 * len(templates), 1), RESCUED_DTYPE)
+    n_out = np.zeros(max(len(jobs), 1), np.uint32)
+    n_cand = np.zeros(max(len(jobs), 1), np.uint32)
+    cells = C.c_uint64()
+    mr = mate_regions if len(mate_regions) else np.zeros(1, ANCHOR_DTYPE)
+    tp = templates if len(templates) else np.zeros(1, ANCHOR_DTYPE)
+    offs = np.ascontiguousarray(contig_offsets, np.int64)
+    lens = np.ascontiguousarray(contig_lengths, np.int32)
+    bases = np.ascontiguousarray(bases, np.uint8) if bases.size else np.zeros(1, np.uint8)
+    rc = lib().orc_mate_rescue_batch(C.byref(sc), ptr(bases), ptr(pac),
+                                     genome_len, jobs.ctypes.data, len(jobs), tp.ctypes.data, mr.ctypes.data,
+                                     stats.ctypes.data, primary, offs.ctypes.data, lens.ctypes.data, len(offs),
+                                     out.ctypes.data, ptr(n_out, C.c_uint32), ptr(n_cand, C.c_uint32), n_threads,
+                                     C.byref(cells))
+    if rc != 0:
+        raise ValueError("mate_rescue_batch failed")
+    return out, n_out[:len(jobs)], n_cand[:len(jobs)], cells.value

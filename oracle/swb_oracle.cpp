@@ -1339,3 +1339,157 @@ int orc_extend_batch(const swb_scoring *sc, const uint8_t *bases, const uint8_t 
     if (cells) { *cells = 0; for (auto v : per) *cells += v; }
     return bad ? -1 : 0;
 }
+
+// --------------------------------------------------------------------------
+// MateRescue.rescue -- Sources/BWAMem/MateRescue.swift:29-171, with
+// hasMateHit (:319-346), PackedReference.fetchSequence
+// (Sources/FMIndex/PackedReference.swift:73-121) and
+// ReferenceMetadata.sequenceID (Sources/BWACore/ReferenceMetadata.swift:77-89).
+// --------------------------------------------------------------------------
+namespace {
+
+int32_t sequence_id(const int64_t *off, size_t n, int64_t pos) {   // ReferenceMetadata.swift:77-89
+    long lo = 0, hi = (long)n - 1;
+    while (lo < hi) {
+        const long mid = (lo + hi + 1) / 2;
+        if (off[mid] <= pos) lo = mid; else hi = mid - 1;
+    }
+    return (int32_t)lo;
+}
+
+struct Fetched {
+    std::vector<uint8_t> bases;
+    int64_t clamped_begin = 0;
+    int32_t rid = 0;
+};
+
+bool fetch_sequence(const uint8_t *pac, int64_t bwtBegin, int64_t bwtEnd, int64_t gl, const int64_t *off,
+                    const int32_t *len, size_t n, Fetched &f) {         // PackedReference.swift:73-121
+    if (!(bwtBegin < bwtEnd)) return false;
+    const bool isReverse = bwtBegin >= gl;
+    if (!isReverse) {
+        const int32_t rid = sequence_id(off, n, bwtBegin);
+        const int64_t chromEnd = off[rid] + (int64_t)len[rid];
+        const int64_t cb = std::max(bwtBegin, off[rid]), ce = std::min(bwtEnd, chromEnd);
+        if (!(cb < ce)) return false;
+        f.bases.resize((size_t)(ce - cb));
+        for (int64_t i = 0; i < ce - cb; ++i) f.bases[(size_t)i] = pac_base(pac, cb + i);
+        f.clamped_begin = cb;
+        f.rid = rid;
+    } else {
+        const int64_t fwdBegin = 2 * gl - bwtEnd, fwdEnd = 2 * gl - bwtBegin;
+        const int32_t rid = sequence_id(off, n, fwdBegin);
+        const int64_t chromEnd = off[rid] + (int64_t)len[rid];
+        const int64_t cb = std::max(fwdBegin, off[rid]), ce = std::min(fwdEnd, chromEnd);
+        if (!(cb < ce)) return false;
+        f.bases.resize((size_t)(ce - cb));
+        for (int64_t i = 0; i < ce - cb; ++i) f.bases[(size_t)i] = pac_base(pac, cb + i);
+        std::reverse(f.bases.begin(), f.bases.end());
+        for (auto &b : f.bases) b = (uint8_t)(3 - b);
+        f.clamped_begin = 2 * gl - ce;
+        f.rid = rid;
+    }
+    return true;
+}
+
+bool has_mate_hit(const swb_anchor *mregs, uint32_t nm, const swb_anchor &t, int dir, const swb_orientation &st,
+                  int64_t gl) {                                         // MateRescue.swift:319-346
+    for (uint32_t k = 0; k < nm; ++k) {
+        const swb_anchor &m = mregs[k];
+        if (m.rid != t.rid) continue;
+        const bool sameStrand = (t.rb >= gl) == (m.rb >= gl);
+        const int64_t p2 = sameStrand ? m.rb : (2 * gl - 1 - m.rb);
+        const int bwaDir = (sameStrand ? 0 : 1) ^ (p2 > t.rb ? 0 : 3);
+        if (bwaDir != dir) continue;
+        const int64_t d = p2 > t.rb ? p2 - t.rb : t.rb - p2;
+        if (d >= st.proper_low && d <= st.proper_high) return true;
+    }
+    return false;
+}
+
+}  // namespace
+
+int orc_mate_rescue_batch(const swb_scoring *sc, const uint8_t *bases, const uint8_t *pac, int64_t gl,
+                          const swb_rescue_job *jobs, size_t n_jobs, const swb_anchor *templates,
+                          const swb_anchor *mate_regions, const swb_orientation *stats, int32_t primary,
+                          const int64_t *coff, const int32_t *clen, size_t n_contigs,
+                          swb_rescued *out, uint32_t *n_out, uint32_t *n_cand, int n_threads, uint64_t *cells) {
+    std::vector<uint64_t> per(std::max(n_threads, 1), 0);
+    parallel_for(n_jobs, n_threads, [&](size_t lo, size_t hi, int tid) {
+        std::vector<uint8_t> fwd, rev;
+        Fetched f;
+        for (size_t j = lo; j < hi; ++j) {
+            const swb_rescue_job &jb = jobs[j];
+            uint32_t nout = 0, ncand = 0;
+            swb_rescued *o = out + 4 * (size_t)jb.tmpl_off;
+            if (jb.n_tmpl > 0 && !stats[primary].failed) {                // :40-44
+                const int64_t mateLen = jb.mate_len;
+                const int32_t minScore = sc->min_seed_len * sc->a;
+                fwd.assign(bases + jb.mate_off, bases + jb.mate_off + jb.mate_len);
+                rev.resize(fwd.size());
+                for (size_t k = 0; k < fwd.size(); ++k) {                  // ReadSequence.reverseComplement
+                    const uint8_t b = fwd[fwd.size() - 1 - k];
+                    rev[k] = b < 4 ? (uint8_t)(3 - b) : 4;
+                }
+                for (uint32_t ti = 0; ti < jb.n_tmpl; ++ti) {
+                    const swb_anchor &a = templates[jb.tmpl_off + ti];
+                    bool allSatisfied = true;
+                    for (int r = 0; r < 4; ++r) {
+                        const swb_orientation &os = stats[r];
+                        if (os.failed) continue;
+                        if (has_mate_hit(mate_regions + jb.mreg_off, jb.n_mreg, a, r, os, gl)) continue;
+                        allSatisfied = false;
+                        const bool isRev = (r >> 1) != (r & 1), isLarger = (r >> 1) == 0;   // :70-73
+                        int64_t rb, re;
+                        if (!isRev) {
+                            if (isLarger) { rb = a.rb + os.proper_low; re = a.rb + os.proper_high + mateLen; }
+                            else { rb = a.rb - os.proper_high - mateLen; re = a.rb - os.proper_low; }
+                        } else {
+                            if (isLarger) { rb = a.rb + os.proper_low - mateLen; re = a.rb + os.proper_high; }
+                            else { rb = a.rb - os.proper_high; re = a.rb - os.proper_low + mateLen; }
+                        }
+                        rb = std::max<int64_t>(rb, 0);                     // :104-106
+                        re = std::min<int64_t>(re, 2 * gl);
+                        if (!(rb < re)) continue;
+                        if (!fetch_sequence(pac, rb, re, gl, coff, clen, n_contigs, f)) continue;
+                        if (f.rid != a.rid) continue;
+                        const std::vector<uint8_t> &q = isRev ? rev : fwd;
+                        swb_local_result sw;
+                        uint64_t c = 0;
+                        ++ncand;
+                        local_align(q.data(), (int)q.size(), f.bases.data(), (int)f.bases.size(), sc,
+                                    clamp_u8(minScore), &sw, &c, nullptr);
+                        per[tid] += c;
+                        if (sw.score == 0) continue;                         // nil
+                        if (!(sw.score >= minScore)) continue;
+                        swb_rescued g{};
+                        g.score = sw.score;
+                        g.true_score = sw.score;
+                        g.csub = sw.score2;
+                        g.rid = a.rid;
+                        const int64_t tb = sw.tb, te = sw.te;
+                        if (!isRev) {                                       // :146-158
+                            g.rb = f.clamped_begin + tb;
+                            g.re = f.clamped_begin + te + 1;
+                            g.qb = sw.qb;
+                            g.qe = sw.qe + 1;
+                        } else {
+                            g.rb = 2 * gl - (f.clamped_begin + te + 1);
+                            g.re = 2 * gl - (f.clamped_begin + tb);
+                            g.qb = (int32_t)mateLen - (sw.qe + 1);
+                            g.qe = (int32_t)mateLen - sw.qb;
+                        }
+                        const int64_t refSpan = te - tb + 1, querySpan = (int64_t)(sw.qe - sw.qb + 1);
+                        g.seed_cov = (int32_t)(std::min(refSpan, querySpan) / 2);
+                        o[nout++] = g;
+                    }
+                    if (allSatisfied) break;
+                }
+            }
+            n_out[j] = nout;
+            if (n_cand) n_cand[j] = ncand;
+        }
+    });
+    if (cells) { *cells = 0; for (auto v : per) *cells += v; }
+    return 0;
+}

@@ -121,6 +121,14 @@ int orc_extend_batch(const swb_scoring *sc, const uint8_t *bases, const uint8_t 
                      const swb_seed *seeds, const swb_chain *chains, size_t n_chains,
                      swb_region *out, uint32_t *n_regions, int n_threads, uint64_t *cells);
 
+/* MateRescue.rescue (Sources/BWAMem/MateRescue.swift:29-171) for every job,
+ * same layout as swb_mate_rescue; pac is the forward strand (.pac). */
+int orc_mate_rescue_batch(const swb_scoring *sc, const uint8_t *bases, const uint8_t *pac, int64_t genome_len,
+                          const swb_rescue_job *jobs, size_t n_jobs, const swb_anchor *templates,
+                          const swb_anchor *mate_regions, const swb_orientation *stats, int32_t primary,
+                          const int64_t *contig_offsets, const int32_t *contig_lengths, size_t n_contigs,
+                          swb_rescued *out, uint32_t *n_out, uint32_t *n_cand, int n_threads, uint64_t *cells);
+
 #ifdef __cplusplus
 }
 #endif

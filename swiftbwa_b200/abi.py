@@ -110,6 +110,14 @@ CHAIN_DTYPE = np.dtype([("read_off", "<u8"), ("read_len", "<i4"), ("rid", "<i4")
 REGION_DTYPE = np.dtype([("rb", "<i8"), ("re", "<i8"), ("qb", "<i4"), ("qe", "<i4"), ("rid", "<i4"),
                          ("score", "<i4"), ("true_score", "<i4"), ("sub", "<i4"), ("sub_n", "<i4"), ("w", "<i4"),
                          ("seed_cov", "<i4"), ("seed_len0", "<i4")])
+ORIENTATION_DTYPE = np.dtype([("failed", "<i4"), ("reserved", "<i4"), ("proper_low", "<i8"), ("proper_high", "<i8")])
+ANCHOR_DTYPE = np.dtype([("rb", "<i8"), ("rid", "<i4"), ("reserved", "<i4")])
+RESCUE_JOB_DTYPE = np.dtype([("mate_off", "<u8"), ("mate_len", "<i4"), ("reserved", "<i4"), ("tmpl_off", "<u4"),
+                             ("n_tmpl", "<u4"), ("mreg_off", "<u4"), ("n_mreg", "<u4")])
+RESCUED_DTYPE = np.dtype([("rb", "<i8"), ("re", "<i8"), ("qb", "<i4"), ("qe", "<i4"), ("rid", "<i4"), ("score", "<i4"),
+                          ("true_score", "<i4"), ("csub", "<i4"), ("seed_cov", "<i4"), ("reserved", "<i4")])
+assert ORIENTATION_DTYPE.itemsize == 24 and ANCHOR_DTYPE.itemsize == 16
+assert RESCUE_JOB_DTYPE.itemsize == 32 and RESCUED_DTYPE.itemsize == 48
 assert SEED_DTYPE.itemsize == 24 and CHAIN_DTYPE.itemsize == 24 and REGION_DTYPE.itemsize == 56
 assert EXT_TASK_DTYPE.itemsize == C.sizeof(ExtTask) == 40
 assert GLOBAL_TASK_DTYPE.itemsize == C.sizeof(GlobalTask) == 40
@@ -127,7 +135,7 @@ EXPORTED_SYMBOLS = (
     "swb_kernel_launches", "swb_last_batch_stats", "swb_profile", "swb_profile_reset",
     "swb_profile_read", "swb_int_alu_peak", "swb_ext_batch_static", "swb_cigar_batch",
     "swb_server_start", "swb_server_submit", "swb_server_poll", "swb_server_wait", "swb_server_resume",
-    "swb_server_stats_get", "swb_server_stop", "swb_extend_chains",
+    "swb_server_stats_get", "swb_server_stop", "swb_extend_chains", "swb_mate_rescue",
 )
 
 
@@ -227,6 +235,10 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.swb_extend_chains.argtypes = [vp, P(Scoring), u8p, C.c_size_t, vp, C.c_size_t, vp, C.c_size_t, C.c_uint64,
                                       vp, P(C.c_uint32), P(C.c_uint32)]
     lib.swb_extend_chains.restype = C.c_int
+    lib.swb_mate_rescue.argtypes = [vp, P(Scoring), u8p, C.c_size_t, vp, C.c_size_t, vp, C.c_size_t, vp, C.c_size_t,
+                                    vp, C.c_int32, vp, vp, C.c_size_t, C.c_uint64, vp, P(C.c_uint32),
+                                    P(C.c_uint32)]
+    lib.swb_mate_rescue.restype = C.c_int
     for f in ("swb_server_start", "swb_server_submit", "swb_server_poll", "swb_server_wait", "swb_server_resume",
               "swb_server_stats_get", "swb_server_stop"):
         getattr(lib, f).restype = C.c_int

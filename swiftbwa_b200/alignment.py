@@ -208,6 +208,30 @@ class Engine:
                                           ptr(counts, C.c_uint32), C.byref(rounds)), "swb_extend_chains")
         return out, counts[:len(chains)], rounds.value
 
+    def mate_rescue(self, sc: Scoring, bases: np.ndarray, jobs: np.ndarray, templates: np.ndarray,
+                    mate_regions: np.ndarray, stats: np.ndarray, primary: int, contig_offsets: np.ndarray,
+                    contig_lengths: np.ndarray, genome_len: int):
+        """MateRescue.rescue for every job (RESCUE_JOB_DTYPE) against the uploaded
+        forward strand -> (RESCUED_DTYPE array, per-job counts, per-job local
+        alignments run).  Job j's regions are out[4*tmpl_off : 4*tmpl_off + counts[j]]."""
+        assert jobs.dtype == abi.RESCUE_JOB_DTYPE and stats.dtype == abi.ORIENTATION_DTYPE and len(stats) == 4
+        bases = np.ascontiguousarray(bases, dtype=np.uint8)
+        if bases.size == 0:
+            bases = np.zeros(1, np.uint8)
+        tp = templates if len(templates) else np.zeros(1, abi.ANCHOR_DTYPE)
+        mr = mate_regions if len(mate_regions) else np.zeros(1, abi.ANCHOR_DTYPE)
+        offs = np.ascontiguousarray(contig_offsets, np.int64)
+        lens = np.ascontiguousarray(contig_lengths, np.int32)
+        out = np.zeros(max(4 * len(templates), 1), abi.RESCUED_DTYPE)
+        n_out = np.zeros(max(len(jobs), 1), np.uint32)
+        n_cand = np.zeros(max(len(jobs), 1), np.uint32)
+        _check(self.lib.swb_mate_rescue(self.h, C.byref(sc), ptr(bases), bases.size, jobs.ctypes.data, len(jobs),
+                                        tp.ctypes.data, len(templates), mr.ctypes.data, len(mate_regions),
+                                        stats.ctypes.data, primary, offs.ctypes.data, lens.ctypes.data, len(offs),
+                                        genome_len, out.ctypes.data, ptr(n_out, C.c_uint32),
+                                        ptr(n_cand, C.c_uint32)), "swb_mate_rescue")
+        return out, n_out[:len(jobs)], n_cand[:len(jobs)]
+
     def last_batch_stats(self):
         ms, cells = C.c_double(), C.c_uint64()
         _check(self.lib.swb_last_batch_stats(self.h, C.byref(ms), C.byref(cells)), "stats")

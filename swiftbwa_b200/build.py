@@ -16,7 +16,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libswb_cuda.so")
-SOURCES = ["swb_runtime.cu", "swb_ext.cu", "swb_global.cu", "swb_local.cu", "swb_probe.cu", "swb_noalloc.cu", "swb_cigar.cu", "swb_serve.cu", "swb_extend.cu"]
+SOURCES = ["swb_runtime.cu", "swb_ext.cu", "swb_global.cu", "swb_local.cu", "swb_probe.cu", "swb_noalloc.cu", "swb_cigar.cu", "swb_serve.cu", "swb_extend.cu", "swb_rescue.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

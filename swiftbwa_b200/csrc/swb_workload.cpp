@@ -431,4 +431,85 @@ int64_t swbw_chains(uint64_t seed, const uint8_t *ref, int64_t gl, int64_t n, in
     return (int64_t)off;
 }
 
+// Mate-rescue jobs: n mates of mate_len bases.  Each job has 1-3 template
+// regions on a random strand (BWT coordinates); the first one is the true
+// anchor: in the template's strand the mate's reverse complement lies at
+// [rb + ins - mate_len, rb + ins), ins ~ N(ins_mean, ins_sd) (an FR pair),
+// with `sub` substitutions.  A fraction no_hit_frac of mates are random.
+// With probability hit_frac the mate already has a region consistent with
+// FR (so that direction is skipped), plus 0-2 unrelated mate regions.  The
+// template's rid is the contig of its forward position.  Mates go to
+// bases_out (n * mate_len); templates / mate regions are compacted; returns
+// (n_templates << 32) | n_mate_regions.
+uint64_t swbw_rescue_jobs(uint64_t seed, const uint8_t *ref, int64_t gl, const int64_t *coff, int64_t n_contigs,
+                          int64_t n, int mate_len, double ins_mean, double ins_sd, double sub, double no_hit_frac,
+                          double hit_frac, uint8_t *bases_out, swb_rescue_job *jobs, swb_anchor *tmpl,
+                          swb_anchor *mreg) {
+    auto full = [&](int64_t p) -> uint8_t { return p < gl ? ref[p] : (uint8_t)(3 - ref[2 * gl - 1 - p]); };
+    auto rid_of = [&](int64_t bwt) -> int32_t {   // contig of the forward position
+        const int64_t f = bwt < gl ? bwt : 2 * gl - 1 - bwt;
+        int64_t lo = 0, hi = n_contigs - 1;
+        while (lo < hi) {
+            const int64_t mid = (lo + hi + 1) / 2;
+            if (coff[mid] <= f) lo = mid; else hi = mid - 1;
+        }
+        return (int32_t)lo;
+    };
+    std::vector<uint32_t> nt((size_t)n), nm((size_t)n);
+    chunked((size_t)n, 4096, [&](size_t ci, size_t lo, size_t hi) {
+        Rng r(chunk_seed(seed, ci));
+        for (size_t i = lo; i < hi; ++i) {
+            uint8_t *m = bases_out + i * (size_t)mate_len;
+            swb_anchor *t = tmpl + i * 3;
+            swb_anchor *mr = mreg + i * 3;
+            const int64_t rb = (int64_t)r.below((uint64_t)(2 * gl - mate_len));
+            const int64_t ins = (int64_t)std::llround(ins_mean + ins_sd * r.normal());
+            if (r.uniform() < no_hit_frac) {
+                for (int k = 0; k < mate_len; ++k) m[k] = r.base();
+            } else {
+                // mate = reverse complement of full[rb + ins - mate_len, rb + ins)
+                for (int k = 0; k < mate_len; ++k) {
+                    const int64_t p = rb + ins - 1 - k;
+                    uint8_t b = (p >= 0 && p < 2 * gl) ? (uint8_t)(3 - full(p)) : r.base();
+                    if (r.uniform() < sub) b = (uint8_t)((b + r.range(1, 3)) & 3);
+                    m[k] = b;
+                }
+            }
+            uint32_t a = 0;
+            t[a++] = swb_anchor{rb, rid_of(rb), 0};
+            const int extra = (int)r.below(3);
+            for (int k = 0; k < extra; ++k) {
+                const int64_t x = (int64_t)r.below((uint64_t)(2 * gl));
+                t[a++] = swb_anchor{x, rid_of(x), 0};
+            }
+            uint32_t b = 0;
+            if (r.uniform() < hit_frac) {
+                // opposite strand at FR distance ins: p2 = rb + ins, m.rb = 2gl - 1 - p2
+                const int64_t p2 = rb + ins;
+                const int64_t mrb = 2 * gl - 1 - p2;
+                if (mrb >= 0 && mrb < 2 * gl) mr[b++] = swb_anchor{mrb, rid_of(mrb), 0};
+            }
+            const int decoys = (int)r.below(3);
+            for (int k = 0; k < decoys; ++k) {
+                const int64_t x = (int64_t)r.below((uint64_t)(2 * gl));
+                if (b < 3) mr[b++] = swb_anchor{x, rid_of(x), 0};
+            }
+            nt[i] = a;
+            nm[i] = b;
+            jobs[i] = swb_rescue_job{i * (uint64_t)mate_len, mate_len, 0, 0, a, 0, b};
+        }
+    });
+    uint64_t to = 0, mo = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        const swb_anchor *ts = tmpl + (size_t)i * 3, *ms = mreg + (size_t)i * 3;
+        if (ts != tmpl + to) std::memmove(tmpl + to, ts, nt[(size_t)i] * sizeof(swb_anchor));
+        if (ms != mreg + mo) std::memmove(mreg + mo, ms, nm[(size_t)i] * sizeof(swb_anchor));
+        jobs[i].tmpl_off = (uint32_t)to;
+        jobs[i].mreg_off = (uint32_t)mo;
+        to += nt[(size_t)i];
+        mo += nm[(size_t)i];
+    }
+    return (to << 32) | mo;
+}
+
 }  // extern "C"

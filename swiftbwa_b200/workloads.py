@@ -14,7 +14,8 @@ from typing import Optional
 
 import numpy as np
 
-from .abi import CHAIN_DTYPE, EXT_TASK_DTYPE, GLOBAL_TASK_DTYPE, LOCAL_TASK_DTYPE, SEED_DTYPE, SWB_GLB_RETRY
+from .abi import (ANCHOR_DTYPE, CHAIN_DTYPE, EXT_TASK_DTYPE, GLOBAL_TASK_DTYPE, LOCAL_TASK_DTYPE, ORIENTATION_DTYPE,
+                  RESCUE_JOB_DTYPE, SEED_DTYPE, SWB_GLB_RETRY)
 from .build import WORKLOAD_OUT, build_workload
 
 SEED_BASE = 0x5EED0000
@@ -41,6 +42,8 @@ def lib() -> C.CDLL:
         L.swbw_rescue_tasks.restype = None
         L.swbw_chains.argtypes = [u64, vp, i64, i64, i32, dbl, dbl, dbl, i32, i32, i32, dbl, vp, vp, vp]
         L.swbw_chains.restype = i64
+        L.swbw_rescue_jobs.argtypes = [u64, vp, i64, vp, i64, i64, i32, dbl, dbl, dbl, dbl, dbl, vp, vp, vp, vp]
+        L.swbw_rescue_jobs.restype = u64
         _lib = L
     return _lib
 
@@ -206,4 +209,57 @@ def config5(rank: int = 0, n_reads: int = 1_000_000, ref_len: int = 100_000_000)
     ref = reference(SEED_BASE + 5 + 1000 * rank, ref_len)
     wl = chains(ref, SEED_BASE + 5 + 1000 * rank + 1, n_reads, 150)
     wl.name = f"config5: {n_reads} seed chains of 150 bp reads ({len(wl.seeds)} seeds), {ref_len // 10**6} Mbp reference"
+    return wl
+
+
+@dataclass
+class RescueJobs:
+    ref: Reference
+    bases: np.ndarray              # mates, mate_len bytes each
+    jobs: np.ndarray               # RESCUE_JOB_DTYPE
+    templates: np.ndarray          # ANCHOR_DTYPE
+    mate_regions: np.ndarray       # ANCHOR_DTYPE
+    stats: np.ndarray              # ORIENTATION_DTYPE[4] (FF, FR, RF, RR)
+    primary: int
+    contig_offsets: np.ndarray     # int64, ascending
+    contig_lengths: np.ndarray     # int32
+    name: str = ""
+
+
+def rescue_jobs(ref: Reference, seed: int, n: int, mate_len: int = 150, *, n_contigs: int = 1, ins_mean=400.0,
+                ins_sd=50.0, sub=0.02, no_hit_frac=0.1, hit_frac=0.2, more_orientations=False) -> RescueJobs:
+    """MateRescue.rescue jobs: FR pairs (insert N(ins_mean, ins_sd)), 1-3
+    template regions per mate (the first the true anchor), existing mate
+    regions that already satisfy FR in a fraction hit_frac, random mates in a
+    fraction no_hit_frac, the genome cut into n_contigs contigs.  Stats: FR
+    with proper range mean +- 4 sd (InsertSizeEstimator.swift:209-210); with
+    more_orientations also FF and RR, with the same range."""
+    rng = np.random.default_rng(seed)
+    cuts = np.sort(rng.choice(np.arange(1, ref.n), n_contigs - 1, replace=False)) if n_contigs > 1 else np.array([], np.int64)
+    offs = np.concatenate([[0], cuts]).astype(np.int64)
+    lens = np.diff(np.concatenate([offs, [ref.n]])).astype(np.int32)
+    bases = np.empty(n * mate_len, np.uint8)
+    jobs = np.empty(n, RESCUE_JOB_DTYPE)
+    tmpl = np.empty(3 * n, ANCHOR_DTYPE)
+    mreg = np.empty(3 * n, ANCHOR_DTYPE)
+    packed = lib().swbw_rescue_jobs(seed, ref.codes.ctypes.data, ref.n, offs.ctypes.data, len(offs), n, mate_len,
+                                    ins_mean, ins_sd, sub, no_hit_frac, hit_frac, bases.ctypes.data,
+                                    jobs.ctypes.data, tmpl.ctypes.data, mreg.ctypes.data)
+    nt, nm = int(packed >> 32), int(packed & 0xFFFFFFFF)
+    stats = np.zeros(4, ORIENTATION_DTYPE)
+    stats["failed"] = 1
+    lo, hi = max(1, int(ins_mean - 4 * ins_sd + 0.5)), int(ins_mean + 4 * ins_sd + 0.5)
+    stats[1] = (0, 0, lo, hi)
+    if more_orientations:
+        stats[0] = (0, 0, lo, hi)
+        stats[3] = (0, 0, lo, hi)
+    return RescueJobs(ref, bases, jobs, tmpl[:nt].copy(), mreg[:nm].copy(), stats, 1, offs, lens)
+
+
+def config3_jobs(rank: int = 0, n: int = 1_000_000, ref_len: int = 100_000_000) -> RescueJobs:
+    """MateRescue.rescue over 1M 150 bp mates (config-3 insert 400 +- 50, 2%
+    substitutions, 10% random mates) against a 100 Mbp reference in 24 contigs."""
+    ref = reference(SEED_BASE + 3 + 1000 * rank, ref_len)
+    wl = rescue_jobs(ref, SEED_BASE + 3 + 1000 * rank + 7, n, 150, n_contigs=24)
+    wl.name = f"config3 rescue driver: {n} mates, {len(wl.templates)} template regions, {ref_len // 10**6} Mbp reference, 24 contigs"
     return wl
