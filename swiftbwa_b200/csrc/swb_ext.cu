@@ -44,6 +44,7 @@
 
 #include "swb_device.cuh"
 #include "swb_ext_dp.cuh"
+#include "swb_ext_pair.cuh"
 #include "swb_internal.h"
 
 namespace swb {
@@ -64,22 +65,22 @@ __device__ __forceinline__ bool fits8(int qlen, int h0, int max_mat) {
     return h0 >= 0 && (long long)h0 + (long long)qlen * (max_mat > 0 ? max_mat : 0) <= 255;
 }
 
-__device__ __forceinline__ int ext_bin(const swb_ext_task &t, int max_mat) {
+__device__ __forceinline__ int ext_bin(const swb_ext_task &t, int max_mat, bool u8_ok) {
     if (t.qlen <= 0 || t.tlen <= 0) return 0;
     if (t.qlen > kExtSmemMaxQ || !fits16(t.qlen, t.h0, max_mat)) return kBigBin;
     int b = 0;
     while (t.qlen > kFastQDev[b]) ++b;
-    return fits8(t.qlen, t.h0, max_mat) ? b : kLenClasses + b;
+    return u8_ok && fits8(t.qlen, t.h0, max_mat) ? b : kLenClasses + b;
 }
 
 // Sort key: bin in bits 27-31, query length in 15-26, target length in 0-14.
-__global__ void ext_keys_kernel(const swb_ext_task *__restrict__ tasks, size_t n, int max_mat,
+__global__ void ext_keys_kernel(const swb_ext_task *__restrict__ tasks, size_t n, int max_mat, int u8_ok,
                                 uint32_t *__restrict__ keys, uint32_t *__restrict__ idx,
                                 int *__restrict__ big_max_q) {
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const swb_ext_task t = tasks[i];
-    const int b = ext_bin(t, max_mat);
+    const int b = ext_bin(t, max_mat, u8_ok != 0);
     const uint32_t q = (uint32_t)min(max(t.qlen, 0), 4095);
     const uint32_t tl = (uint32_t)min(max(t.tlen, 0), 32767);
     keys[i] = ((uint32_t)b << 27) | (q << 15) | tl;
@@ -257,7 +258,12 @@ __global__ void __launch_bounds__(T) ext_fast_kernel(ExtArgs a, int bin) {
             const uint32_t ti = a.order[pos];
             const swb_ext_task tk = a.tasks[ti];
             swb_ext_result r;
-            ext_fast_one<T, U8>(a, tk, he, qs, r, cells);
+            if (!U8)
+                ext_fast_one<T, false>(a, tk, he, qs, r, cells);
+            else if (a.sc.o_del + a.sc.e_del == a.sc.o_ins + a.sc.e_ins)
+                ext_pair_one<T, true>(a, tk, he, r, cells);
+            else
+                ext_pair_one<T, false>(a, tk, he, r, cells);
             a.out[ti] = r;
         }
     }
@@ -344,7 +350,10 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     const unsigned tb = 256;
     {
         ProfScope ps(ctx, s, "ext_keys", -1);
-        ext_keys_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(d_tasks, n, sc.max_mat, keys, idx, big_max_q);
+        // int8 rows run two target rows per pass on 16-bit lanes: the gap costs must fit a lane.
+        const int u8_ok = sc.o_del + sc.e_del <= 32767 && sc.o_ins + sc.e_ins <= 32767;
+        ext_keys_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(d_tasks, n, sc.max_mat, u8_ok, keys, idx,
+                                                                       big_max_q);
     }
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());

@@ -1,0 +1,282 @@
+// swb_ext_pair.cuh -- BandedSWScalar.align (Sources/Alignment/BandedSWScalar.swift:21-191)
+// for int8-bounded tasks, two target rows per pass.
+//
+// Row layout (shared memory, one 32-bit word per query column, [column][thread]):
+//   bits  0-15  prmt selector of the column's query base q: nibbles (q, q|8, 5, 5),
+//               i.e. the row's score for q as a 16-bit value ([s, sign, 0, 0])
+//   bits 16-23  H of the previous row at the previous column (the diagonal input)
+//   bits 24-31  E into this column
+// exactly the reference's h[j] / e[j] storage (`h[j]` holds the left neighbour's
+// H once the row has passed it), with the scores bounded by 255.
+//
+// Rows i and i+1 advance together, row i+1 one column behind row i: at step c
+// row i computes column c from the word it loads, and row i+1 computes
+// column c-1 from the values row i produced for column c-1 one step earlier
+// (the word row i would have stored).  The two cells are independent, so they
+// run as the low and high 16-bit lanes of one register through the DPX
+// s16x2 forms: one shared load, one 16-bit shared store and ~13 ALU
+// operations per two cells.  Row i's words are never stored: row i+1
+// consumes them from registers and overwrites the same columns.
+//
+// What the reference does between rows is kept exactly:
+//   * row i+1 starts at max(first nonzero column of row i, i+1-w): the first
+//     nonzero word of row i is known before row i+1 reaches it (it trails);
+//   * row i+1 ends at min(last nonzero word of row i + 2, i+w+2, qlen); the
+//     last nonzero word of row i is one past the last column where H > 0,
+//     tracked per lane.  Until row i is complete, row i+1 runs on through
+//     row i's zero tail; those cells see M = 0 and E = 0, so their H is F
+//     decaying by eIns per column, below the last valid H of the row, and so
+//     they never change the row maximum.  Once the end is known their words
+//     are reset to what the reference holds there (zero), and the row-end
+//     word h[end] = H(end-1), e[end] = 0 is written;
+//   * rowMax == 0 and z-drop stop the task after row i before row i+1's
+//     results are used; row i+1's own checks follow in order;
+//   * band narrowing after row i+1 scans the stored words as the reference.
+#pragma once
+
+#include "swb_device.cuh"
+#include "swb_ext_dp.cuh"
+
+namespace swb {
+namespace {
+
+// Score of query selector `sel` (low 16 bits) against a row table, as
+// [s, sign(s), 0, 0] (one 16-bit lane).
+__device__ __forceinline__ uint32_t lane_score(const RowTable &rt, uint32_t sel) { return prmt(rt.lo, rt.hi, sel); }
+
+struct PairConsts {
+    uint32_t negOeDel, negOeIns, negEDel, negEIns;   // replicated in both 16-bit lanes
+};
+
+// One cell in the low lane only (the high lane's inputs are zero).  `w` is the
+// column's word as the reference's loop reads it; returns the new word's
+// upper half (h1 before, E') and updates h1, f, key, lastJ.  SYM: the open
+// costs oDel+eDel and oIns+eIns are equal, so E' and F' share one operand.
+template <bool SYM>
+__device__ __forceinline__ uint32_t single_cell(const PairConsts &pc, const RowTable &rt, uint32_t w, int j,
+                                                uint32_t &h1, uint32_t &f, uint32_t &key, uint32_t &lastJ) {
+    const uint32_t s = lane_score(rt, w);
+    const uint32_t M = __byte_perm(w, 0u, 0x4442);          // [H, 0, 0, 0]
+    const uint32_t e = __byte_perm(w, 0u, 0x4443);          // [E, 0, 0, 0]
+    const uint32_t d = __viaddmin_s16x2_relu(M, s, M * 128u);
+    const uint32_t H = __vimax3_s16x2(d, e, f);
+    const uint32_t tDel = __viaddmax_s16x2(d, pc.negOeDel, 0x80008000u);
+    const uint32_t nE = __viaddmax_s16x2_relu(e, pc.negEDel, tDel);
+    const uint32_t tIns = SYM ? tDel : __viaddmax_s16x2(d, pc.negOeIns, 0x80008000u);
+    f = __viaddmax_s16x2_relu(f, pc.negEIns, tIns);
+    const uint32_t up = __byte_perm(h1, nE, 0x0040);         // [h1, E'] -> bits 16-31 of the word
+    const uint32_t Hs = H * 256u;
+    key = __vimax3_u16x2(key, Hs + (uint32_t)j, key);
+    lastJ = __vimax3_u16x2(lastJ, __vimin3_u16x2((uint32_t)j, Hs, (uint32_t)j), lastJ);
+    h1 = H;
+    return up;
+}
+
+__device__ __forceinline__ void store_up(uint32_t *he, int T, int j, uint32_t up) {
+    reinterpret_cast<uint16_t *>(he + j * T)[1] = (uint16_t)up;
+}
+
+// Row-end bookkeeping of BandedSWScalar.swift:149-172 for row `row`; returns
+// false when the task stops after this row.
+struct RowTrack {
+    int maxScore, maxI, maxJ, gScore, gTle, maxOff;
+    __device__ __forceinline__ bool finish(int row, int rowMax, int rowMaxJ, int h1, bool atEnd, int zDrop,
+                                           int eDel, int eIns) {
+        if (atEnd) {                                                           // :149-152
+            gTle = gScore > h1 ? gTle : row;
+            gScore = gScore > h1 ? gScore : h1;
+        }
+        if (rowMax == 0) return false;                                         // :155
+        if (rowMax > maxScore) {                                               // :158-172
+            maxScore = rowMax;
+            maxI = row;
+            maxJ = rowMaxJ;
+            const int off = abs(rowMaxJ - row);
+            if (off > maxOff) maxOff = off;
+        } else if (zDrop > 0) {
+            const int dI = row - maxI, dJ = rowMaxJ - maxJ;
+            if (dI > dJ) {
+                if (maxScore - rowMax - (dI - dJ) * eDel > zDrop) return false;
+            } else {
+                if (maxScore - rowMax - (dJ - dI) * eIns > zDrop) return false;
+            }
+        }
+        return true;
+    }
+};
+
+template <int T, bool SYM>
+__device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_task &tk, uint32_t *__restrict__ he,
+                                             swb_ext_result &res, unsigned long long &cells) {
+    res = swb_ext_result{0, 0, 0, 0, 0, 0};
+    const int qlen = tk.qlen, tlen = tk.tlen;
+    if (!(qlen > 0 && tlen > 0)) return;                                      // :33-35
+    const DevScoring &sc = a.sc;
+    const int oDel = sc.o_del, eDel = sc.e_del, oIns = sc.o_ins, eIns = sc.e_ins;
+    const int zDrop = sc.zdrop;
+    const int h0 = tk.h0;
+    PairConsts pc;
+    pc.negOeDel = (uint32_t)(uint16_t)(-(oDel + eDel)) * 0x10001u;
+    pc.negOeIns = (uint32_t)(uint16_t)(-(oIns + eIns)) * 0x10001u;
+    pc.negEDel = (uint32_t)(uint16_t)(-eDel) * 0x10001u;
+    pc.negEIns = (uint32_t)(uint16_t)(-eIns) * 0x10001u;
+
+    // Query profile and the first row from h0 (:44-50, :65-77).
+    {
+        int hv = h0;
+        bool ramp = h0 > oIns + eIns;
+        for (int j = 0; j <= qlen; ++j) {
+            int hj = 0;
+            if (j == 0) {
+                hj = h0;
+            } else if (j == 1) {
+                if (ramp) hj = hv = h0 - oIns - eIns;
+            } else if (ramp && hv > eIns) {
+                hj = hv -= eIns;
+            } else {
+                ramp = false;
+            }
+            const uint32_t q = j < qlen ? span_base(a.bases, a.pac, tk.q_off, j, qlen, tk.flags, false) : 4u;
+            he[j * T] = (q | ((q | 8u) << 4) | 0x5500u) | ((uint32_t)hj << 16);
+        }
+    }
+    int w = tk.w;                                                              // :52-62
+    {
+        const int maxIns = (int)((double)(qlen * sc.max_mat + tk.end_bonus - oIns) / (double)eIns + 1.0);
+        w = imin(w, imax(1, maxIns));
+        const int maxDel = (int)((double)(qlen * sc.max_mat + tk.end_bonus - oDel) / (double)eDel + 1.0);
+        w = imin(w, imax(1, maxDel));
+    }
+    const bool tref = (tk.flags & SWB_T_FROM_REF) != 0;
+    const bool tcomp = (tk.flags & SWB_T_COMPLEMENT) != 0;
+    const long long tstep = (tk.flags & SWB_T_REVERSE) ? -1 : 1;
+    const long long tbase = (tk.flags & SWB_T_REVERSE) ? (long long)tk.t_off + tlen - 1 : (long long)tk.t_off;
+    auto row_tab = [&](int i) -> RowTable {
+        const unsigned long long idx = (unsigned long long)(tbase + tstep * i);
+        uint32_t tb = tref ? (a.pac[idx >> 2] >> ((3u - (uint32_t)(idx & 3)) << 1)) & 3u : a.bases[idx];
+        if (tcomp && tb < 4u) tb = 3u - tb;
+        return row_table(sc, tb);
+    };
+    auto h1_init = [&](int row) -> uint32_t {                                  // :99-107
+        return (uint32_t)imax(h0 - (oDel + eDel * (row + 1)), 0);
+    };
+
+    RowTrack tr{h0, -1, -1, -1, -1, 0};
+    int beg = 0, end = qlen;
+    int i = 0;
+    while (i < tlen) {
+        if (beg < i - w) beg = i - w;                                          // :95-97
+        if (end > i + w + 1) end = i + w + 1;
+        if (end > qlen) end = qlen;
+        const int b0 = beg, e0 = end;
+        const RowTable rt0 = row_tab(i);
+        uint32_t h1 = b0 == 0 ? h1_init(i) : 0u, f = 0u, key = 0u, lastJ = 0u;
+        if (e0 > b0) cells += (unsigned long long)(e0 - b0);
+        const bool pair = i + 1 < tlen;
+        // ---- phase A: row i alone until row i+1 may start (or the row ends)
+        const int lo1 = i + 1 - w;
+        int firstNz = -1;                 // first nonzero word of row i
+        int c = b0;
+        uint32_t hPrev = 0u, nEPrev = 0u, wPrev = 0u;   // row i's word for column c-1 (registers)
+        bool started = false;
+        for (; c < e0; ++c) {
+            const uint32_t wd = he[c * T];
+            const uint32_t hb = h1;
+            const uint32_t up = single_cell<SYM>(pc, rt0, wd, c, h1, f, key, lastJ);
+            hPrev = hb;
+            nEPrev = up >> 8;           // E' of row i at column c (byte 1 of up)
+            wPrev = wd;
+            if (firstNz < 0 && (up & 0xFFFFu) != 0u) firstNz = c;
+            if (pair && firstNz >= 0 && c >= lo1) {
+                ++c;
+                started = true;
+                break;
+            }
+        }
+        nEPrev &= 0xFFu;
+        // ---- phase B: rows i and i+1 in lockstep (row i at c, row i+1 at c-1)
+        const int beg1 = started ? c - 1 : -1;                                 // row i+1's first column, if known
+        uint32_t h1p = h1, fp = f, keyp = key, lastJp = lastJ;                 // lane 0 = row i, lane 1 = row i+1
+        const RowTable rt1 = pair ? row_tab(i + 1) : rt0;
+        if (started) {
+            h1p |= (beg1 == 0 ? h1_init(i + 1) : 0u) << 16;
+            uint32_t hPrevP = hPrev;    // lane 0 of h1 before the previous step
+            uint32_t jp = (uint32_t)c | ((uint32_t)(c - 1) << 16);
+#pragma unroll 2
+            for (; c < e0; ++c, jp += 0x10001u) {
+                const uint32_t wd = he[c * T];
+                const uint32_t Mp = __byte_perm(wd, hPrevP, 0x5452);            // [H(i-1,c-1), H(i,c-2)]
+                const uint32_t ep = __byte_perm(wd, nEPrev, 0x5453);            // [E(i,c),     E(i+1,c-1)]
+                const uint32_t sp = lane_score(rt1, wPrev) * 65536u + lane_score(rt0, wd);
+                const uint32_t d = __viaddmin_s16x2_relu(Mp, sp, Mp * 128u);
+                const uint32_t H = __vimax3_s16x2(d, ep, fp);
+                const uint32_t tDel = __viaddmax_s16x2(d, pc.negOeDel, 0x80008000u);
+                const uint32_t nE = __viaddmax_s16x2_relu(ep, pc.negEDel, tDel);
+                const uint32_t tIns = SYM ? tDel : __viaddmax_s16x2(d, pc.negOeIns, 0x80008000u);
+                fp = __viaddmax_s16x2_relu(fp, pc.negEIns, tIns);
+                store_up(he, T, c - 1, __byte_perm(h1p, nE, 0x0062));           // row i+1's word for c-1
+                const uint32_t Hs = H * 256u;
+                keyp = __vimax3_u16x2(keyp, Hs + jp, keyp);
+                lastJp = __vimax3_u16x2(lastJp, __vimin3_u16x2(jp, Hs, jp), lastJp);
+                hPrevP = h1p;
+                wPrev = wd;
+                nEPrev = nE & 0xFFu;
+                h1p = H;
+            }
+            hPrev = hPrevP & 0xFFFFu;
+        }
+        // ---- row i complete
+        const int h1i = (int)(h1p & 0xFFFFu);
+        const int key0 = (int)(keyp & 0xFFFFu);
+        const int rowMax0 = e0 > b0 ? key0 >> 8 : 0;
+        // (the last row's words, h[end] included, are never read again)
+        if (!tr.finish(i, rowMax0, key0 & 0xFF, h1i, e0 == qlen, zDrop, eDel, eIns)) break;
+        if (!pair) break;   // last row
+        // Narrowing after row i (:175-180): first nonzero word, last nonzero word = last H > 0 column + 1.
+        const int lastH = (int)(lastJp & 0xFFFFu);
+        const int bn = firstNz >= 0 ? firstNz : e0;
+        const int en = imin(lastH + 3, qlen);
+        // Row i+1's band (:95-97).
+        int b1 = bn > i + 1 - w ? bn : i + 1 - w;
+        int e1 = en < i + 1 + w + 1 ? en : i + 1 + w + 1;
+        if (e1 > qlen) e1 = qlen;
+        if (e1 > b1) cells += (unsigned long long)(e1 - b1);
+        // ---- drain: row i+1 alone for its columns past the lockstep
+        int s = started ? c - 1 : b1;                                          // next column of row i+1
+        uint32_t f1 = fp >> 16, k1 = keyp >> 16, lj1 = lastJp >> 16;
+        uint32_t h1b = started ? (h1p >> 16) : (b1 == 0 ? h1_init(i + 1) : 0u);
+        if (!started) f1 = 0u, k1 = 0u, lj1 = 0u;
+        for (; s < e1; ++s) {
+            // Row i's word for column s: from registers (c-1 = e0-1), the row-end word, or untouched.
+            uint32_t wd = he[s * T];
+            if (s == e0 - 1) wd = (wd & 0xFFFFu) | (hPrev << 16) | (nEPrev << 24);
+            else if (s == e0) wd = (wd & 0xFFFFu) | ((uint32_t)h1i << 16);
+            const uint32_t up = single_cell<SYM>(pc, rt1, wd, s, h1b, f1, k1, lj1);
+            store_up(he, T, s, up);
+        }
+        // H of row i+1's last valid column: from the register if it was the last
+        // cell computed, else from the word the lockstep stored at column e1.
+        int h1last = (int)(h1b & 0xFFFFu);
+        const bool overran = started && e1 <= e0 - 2;
+        if (overran) h1last = (int)((he[e1 * T] >> 16) & 0xFFu);
+        const int key1 = (int)(k1 & 0xFFFFu);
+        const int rowMax1 = e1 > b1 ? key1 >> 8 : 0;
+        // Words the reference holds after row i+1: h[e1] = H(e1-1), e[e1] = 0,
+        // then row i's zero tail up to e0.
+        he[e1 * T] = (he[e1 * T] & 0xFFFFu) | ((uint32_t)h1last << 16);
+        for (int z = e1 + 1; z <= e0; ++z) he[z * T] &= 0xFFFFu;
+        if (!tr.finish(i + 1, rowMax1, key1 & 0xFF, h1last, e1 == qlen, zDrop, eDel, eIns)) break;
+        // Narrowing after row i+1 (:175-180).
+        int nb = b1;
+        while (nb < e1 && (he[nb * T] >> 16) == 0u) ++nb;
+        beg = nb;
+        int ne = e1;
+        while (ne >= beg && (he[ne * T] >> 16) == 0u) --ne;
+        end = imin(ne + 2, qlen);
+        i += 2;
+    }
+    res = swb_ext_result{tr.maxScore, tr.maxJ + 1, tr.maxI + 1, tr.gTle + 1, tr.gScore, tr.maxOff};   // :183-190
+}
+
+}  // namespace
+}  // namespace swb
