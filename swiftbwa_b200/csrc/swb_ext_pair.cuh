@@ -31,7 +31,8 @@
 //     word h[end] = H(end-1), e[end] = 0 is written;
 //   * rowMax == 0 and z-drop stop the task after row i before row i+1's
 //     results are used; row i+1's own checks follow in order;
-//   * band narrowing after row i+1 scans the stored words as the reference.
+//   * band narrowing after row i+1: the first nonzero word by the reference's
+//     scan, the last one from lane 1's last column with H > 0.
 #pragma once
 
 #include "swb_device.cuh"
@@ -66,7 +67,7 @@ __device__ __forceinline__ uint32_t single_cell(const PairConsts &pc, const RowT
     f = __viaddmax_s16x2_relu(f, pc.negEIns, tIns);
     const uint32_t up = __byte_perm(h1, nE, 0x0040);         // [h1, E'] -> bits 16-31 of the word
     const uint32_t Hs = H * 256u;
-    key = __vimax3_u16x2(key, Hs + (uint32_t)j, key);
+    key = __viaddmax_u16x2(Hs, (uint32_t)j, key);
     lastJ = __vimax3_u16x2(lastJ, __vimin3_u16x2((uint32_t)j, Hs, (uint32_t)j), lastJ);
     h1 = H;
     return up;
@@ -216,11 +217,11 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
                 fp = __viaddmax_s16x2_relu(fp, pc.negEIns, tIns);
                 store_up(he, T, c - 1, __byte_perm(h1p, nE, 0x0062));           // row i+1's word for c-1
                 const uint32_t Hs = H * 256u;
-                keyp = __vimax3_u16x2(keyp, Hs + jp, keyp);
+                keyp = __viaddmax_u16x2(Hs, jp, keyp);
                 lastJp = __vimax3_u16x2(lastJp, __vimin3_u16x2(jp, Hs, jp), lastJp);
                 hPrevP = h1p;
                 wPrev = wd;
-                nEPrev = nE & 0xFFu;
+                nEPrev = nE;    // byte 0 = row i's E', byte 1 = 0 (lane values <= 255)
                 h1p = H;
             }
             hPrev = hPrevP & 0xFFFFu;
@@ -270,8 +271,9 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
         int nb = b1;
         while (nb < e1 && (he[nb * T] >> 16) == 0u) ++nb;
         beg = nb;
-        int ne = e1;
-        while (ne >= beg && (he[ne * T] >> 16) == 0u) --ne;
+        // The last nonzero word is one past the last column with H > 0 (lane 1's
+        // tracker; columns past e1 computed ahead of row i's end only decay from it).
+        const int ne = imin((int)(lj1 & 0xFFFFu), e1 - 1) + 1;
         end = imin(ne + 2, qlen);
         i += 2;
     }
