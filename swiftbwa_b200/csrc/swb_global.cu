@@ -263,14 +263,30 @@ __device__ int global_dp_smem(const DevScoring &sc, int2 *he, const uint8_t *qs,
     return he[qlen * T].x;                                                       // :144
 }
 
-__global__ void __launch_bounds__(256) global_smem_kernel(GlobalArgs a, uint32_t *z, size_t nslots, int qcap) {
+// Sort key: shared-memory tasks first, then by query length, target length
+// and band, so the threads of a warp align tasks of the same shape.
+__global__ void global_keys_kernel(const swb_global_task *__restrict__ tasks, size_t n, uint32_t *__restrict__ keys,
+                                   uint32_t *__restrict__ idx) {
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const swb_global_task t = tasks[i];
+    const uint32_t big = t.qlen > kGlbSmemMaxQ ? 1u : 0u;
+    keys[i] = (big << 31) | ((uint32_t)min(max(t.qlen, 0), 2047) << 20) | ((uint32_t)min(max(t.tlen, 0), 4095) << 8) |
+              (uint32_t)min(max(t.w, 0), 255);
+    idx[i] = (uint32_t)i;
+}
+
+// Tasks order[0 .. n_small) (all with qlen <= qcap) in sorted order.
+__global__ void __launch_bounds__(256) global_smem_kernel(GlobalArgs a, const uint32_t *__restrict__ order,
+                                                          size_t n_small, uint32_t *z, size_t nslots, int qcap) {
     extern __shared__ int2 smem[];
     const int T = blockDim.x;
     int2 *he = smem + threadIdx.x;
     uint8_t *qs = reinterpret_cast<uint8_t *>(smem + (size_t)(qcap + 1) * T) + threadIdx.x;
     const size_t slot = blockIdx.x * (size_t)T + threadIdx.x;
     unsigned long long cells = 0;
-    for (size_t k = slot; k < a.n; k += nslots) {
+    for (size_t p = slot; p < n_small; p += nslots) {
+        const size_t k = order[p];
         const swb_global_task tk = a.tasks[k];
         if (tk.qlen > qcap) continue;                                    // the global-scratch kernel's
         swb_global_result r{0, 0, tk.w, 1, a.cigar_off[k]};
@@ -313,6 +329,7 @@ __global__ void cigar_offsets_kernel(const swb_global_task *__restrict__ tasks, 
 }  // namespace
 }  // namespace swb
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 namespace swb {
@@ -332,6 +349,16 @@ int launch_global(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     SWB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, lens, offs, (int)n, st));
     if ((rc = ensure_dev(ctx, ctx->d_sort_tmp, tmp))) return rc;
     SWB_CUDA(cub::DeviceScan::ExclusiveSum(ctx->d_sort_tmp.p, tmp, lens, offs, (int)n, st));
+    // Shape order (the scan is done with `lens`, so its buffer holds the keys).
+    if ((rc = ensure_dev(ctx, ctx->d_idx, n * 4)) || (rc = ensure_dev(ctx, ctx->d_idx2, n * 4))) return rc;
+    uint32_t *skeys = (uint32_t *)ctx->d_keys.p, *skeys2 = skeys + n;
+    uint32_t *sidx = (uint32_t *)ctx->d_idx.p, *order = (uint32_t *)ctx->d_idx2.p;
+    global_keys_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_tasks, n, skeys, sidx);
+    ctx->launches++;
+    SWB_CUDA(cudaGetLastError());
+    SWB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, skeys, skeys2, sidx, order, (int)n, 0, 32, st));
+    if ((rc = ensure_dev(ctx, ctx->d_sort_tmp, tmp))) return rc;
+    SWB_CUDA(cub::DeviceRadixSort::SortPairs(ctx->d_sort_tmp.p, tmp, skeys, skeys2, sidx, order, (int)n, 0, 32, st));
     GlobalArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_res, d_cigar, offs, d_cells + kCntGlobal, n, kGlbSmemMaxQ};
     const size_t avail0 = ctx->budget > ctx->allocated ? (ctx->budget - ctx->allocated) / 2 : 0;
 
@@ -388,7 +415,8 @@ int launch_global(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     if ((rc = ensure_dev(ctx, ctx->d_scratch, z_bytes + big_bytes + 256))) return rc;
     ProfScope ps(ctx, st, "global_nw_traceback", kCntGlobal);
     if (shape.n_small > 0) {
-        global_smem_kernel<<<(unsigned)grid_s, T, smem, st>>>(a, (uint32_t *)ctx->d_scratch.p, z_nslots, qcap);
+        global_smem_kernel<<<(unsigned)grid_s, T, smem, st>>>(a, order, shape.n_small, (uint32_t *)ctx->d_scratch.p,
+                                                              z_nslots, qcap);
         ctx->launches++;
         SWB_CUDA(cudaGetLastError());
     }
