@@ -252,6 +252,7 @@ extern "C" int swb_cigar_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_
     std::vector<swb_global_task> dp;
     std::vector<int32_t> dp_index(n_tasks, -1);
     GlobalShape shape;
+    const int cost16 = nw_i16_cost(sc->a, sc->b, sc->o_del, sc->e_del, sc->o_ins, sc->e_ins);
     size_t raw_words = 0;
     for (size_t i = 0; i < n_tasks; ++i) {
         if (fast[i]) continue;
@@ -264,7 +265,7 @@ extern "C" int swb_cigar_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_
                                      (t.flags & (SWB_Q_REVERSE | SWB_T_REVERSE | SWB_T_COMPLEMENT | SWB_T_FROM_REF)) |
                                          SWB_GLB_RETRY,
                                      0});
-        shape.add(t.qlen, t.rlen);
+        shape.add(t.qlen, t.rlen, cost16);
         raw_words += (size_t)t.qlen + (size_t)t.rlen;
     }
 

@@ -9,6 +9,8 @@
 // backpointer matrix of the last attempt is walked by the same thread; ops
 // are written in traceback order into the task's CIGAR window, merged into
 // runs on the fly, and reversed in place at the end (CIGARBuilder.swift).
+#include <type_traits>
+
 #include "swb_device.cuh"
 #include "swb_internal.h"
 
@@ -210,35 +212,88 @@ struct ZPacked {
     }
 };
 
-__device__ int global_dp_smem(const DevScoring &sc, int2 *he, const uint8_t *qs, int T, const GlobalArgs &a,
+// Row stores of the shared-memory kernel, [column][thread].
+//   RowI32: H and E as int32 (the reference's types, sentinel -2^30).
+//   RowI16: H and E as the two int16 halves of one word, with -16384 standing
+//   in for the sentinel.  Exact when fits_i16() holds: every real H/E/F lies
+//   in [-(q+t+2)P, a(q+t)] (P = the largest cost of one step), every value
+//   derived from the sentinel stays within (q+t+2)(a+P) of it, so real values
+//   still exceed all sentinel-derived ones, and sentinel-derived values keep
+//   their order (they differ from the reference's only by the same shift).
+//   A sentinel-derived final score is shifted back.
+struct RowI32 {
+    int2 *he;
+    int T;
+    static constexpr int kNeg = kNegInf;
+    __device__ __forceinline__ void load(int j, int &h, int &e) const {
+        const int2 v = he[j * T];
+        h = v.x;
+        e = v.y;
+    }
+    __device__ __forceinline__ void store(int j, int h, int e) const { he[j * T] = make_int2(h, e); }
+    __device__ __forceinline__ int getH(int j) const { return he[j * T].x; }
+    __device__ __forceinline__ void setH(int j, int h) const { he[j * T].x = h; }
+    __device__ __forceinline__ int final_score(int s, int) const { return s; }
+};
+
+struct RowI16 {
+    uint32_t *he;
+    int T;
+    static constexpr int kNeg = -16384;
+    __device__ __forceinline__ void load(int j, int &h, int &e) const {
+        const uint32_t w = he[j * T];
+        h = (int)(int16_t)(w & 0xFFFFu);
+        e = (int)w >> 16;
+    }
+    __device__ __forceinline__ void store(int j, int h, int e) const {
+        he[j * T] = ((uint32_t)h & 0xFFFFu) | ((uint32_t)e << 16);
+    }
+    __device__ __forceinline__ int getH(int j) const { return (int)(int16_t)(he[j * T] & 0xFFFFu); }
+    __device__ __forceinline__ void setH(int j, int h) const { reinterpret_cast<int16_t *>(he + j * T)[0] = (int16_t)h; }
+    // thr: every real value is above it, every sentinel-derived one at or below.
+    __device__ __forceinline__ int final_score(int s, int thr) const { return s <= thr ? kNegInf + (s - kNeg) : s; }
+};
+
+__device__ __forceinline__ int step_cost(const DevScoring &sc) {
+    return nw_i16_cost(sc.a, sc.b, sc.o_del, sc.e_del, sc.o_ins, sc.e_ins) - sc.a;
+}
+
+__device__ __forceinline__ bool fits_i16(const DevScoring &sc, int qlen, int tlen) {
+    return nw_fits_i16(qlen, tlen, nw_i16_cost(sc.a, sc.b, sc.o_del, sc.e_del, sc.o_ins, sc.e_ins));
+}
+
+template <class Row>
+__device__ int global_dp_smem(const DevScoring &sc, const Row &row, const uint8_t *qs, int T, const GlobalArgs &a,
                               const swb_global_task &tk, int w, const ZPacked &zp, unsigned long long &cells) {
+    constexpr int kNeg = Row::kNeg;
     const int qlen = tk.qlen, tlen = tk.tlen;
     const int oDel = sc.o_del, eDel = sc.e_del, oIns = sc.o_ins, eIns = sc.e_ins;
     const int oeDel = oDel + eDel, oeIns = oIns + eIns;
-    for (int j = 0; j <= qlen; ++j) he[j * T] = make_int2(kNegInf, kNegInf);    // :75-76
-    he[0].x = 0;                                                                 // :80-84
+    for (int j = 0; j <= qlen; ++j) row.store(j, kNeg, kNeg);                    // :75-76
+    row.setH(0, 0);                                                              // :80-84
     const int initEnd = imin(w, qlen);
-    for (int j = 1; j <= initEnd; ++j) he[j * T].x = 0 - (oIns + eIns * j);
+    for (int j = 1; j <= initEnd; ++j) row.setH(j, 0 - (oIns + eIns * j));
     const size_t rstride = (size_t)zp.ncw * zp.nslots;
     for (int i = 0; i < tlen; ++i) {                                             // :89-142
         const int beg = imax(0, i - w);
         const int end = (int)min((long long)qlen, (long long)i + w + 1);
         const RowTable rt = row_table(sc, span_base(a.bases, a.pac, tk.t_off, i, tlen, tk.flags, true));
-        int f = kNegInf;
-        int hDiag = he[beg * T].x;
-        const int hBeg = beg == 0 ? 0 - (oeDel + eDel * i) : kNegInf;
-        he[beg * T].x = hBeg;
+        int f = kNeg;
+        int hDiag = row.getH(beg);
+        const int hBeg = beg == 0 ? 0 - (oeDel + eDel * i) : kNeg;
+        row.setH(beg, hBeg);
         if (end > beg) cells += (unsigned long long)(end - beg);
         int hLeft = hBeg;
         uint32_t *zrow = zp.z + (size_t)i * rstride;
         uint32_t word = 0;
         int col = 0;
         for (int j = beg; j < end; ++j, ++col) {
-            const int2 v = he[(j + 1) * T];
+            int vh, ve;
+            row.load(j + 1, vh, ve);
             int hCur = hDiag + row_score(rt, qs[j * T]);
-            hDiag = v.x;
-            const int eOpen = v.x - oeDel;
-            const int eExtend = v.y - eDel;
+            hDiag = vh;
+            const int eOpen = vh - oeDel;
+            const int eExtend = ve - eDel;
             const uint32_t eFlag = eOpen > eExtend ? 0u : 1u;
             const int eVal = eOpen > eExtend ? eOpen : eExtend;
             const int fOpen = hLeft - oeIns;
@@ -250,7 +305,7 @@ __device__ int global_dp_smem(const DevScoring &sc, int2 *he, const uint8_t *qs,
             hCur = eVal > hCur ? eVal : hCur;
             const uint32_t fromF = fVal > hCur ? 8u : 0u;
             hCur = fVal > hCur ? fVal : hCur;
-            he[(j + 1) * T] = make_int2(hCur, eVal);
+            row.store(j + 1, hCur, eVal);
             hLeft = hCur;
             word |= (eFlag | fFlag | fromE | fromF) << ((col & 7) << 2);
             if ((col & 7) == 7) {
@@ -260,7 +315,8 @@ __device__ int global_dp_smem(const DevScoring &sc, int2 *he, const uint8_t *qs,
         }
         if (col & 7) zrow[(size_t)(col >> 3) * zp.nslots] = word;
     }
-    return he[qlen * T].x;                                                       // :144
+    const int thr = -(qlen + tlen + 2) * step_cost(sc) - 1;
+    return row.final_score(row.getH(qlen), thr);                                 // :144
 }
 
 // Sort key: shared-memory tasks first, then by query length, target length
@@ -276,19 +332,27 @@ __global__ void global_keys_kernel(const swb_global_task *__restrict__ tasks, si
     idx[i] = (uint32_t)i;
 }
 
-// Tasks order[0 .. n_small) (all with qlen <= qcap) in sorted order.
+// Tasks order[0 .. n_small) (all with qlen <= qcap) in sorted order; the
+// int16 instance takes those fits_i16() accepts, the int32 one the rest.
+template <bool I16>
 __global__ void __launch_bounds__(256) global_smem_kernel(GlobalArgs a, const uint32_t *__restrict__ order,
                                                           size_t n_small, uint32_t *z, size_t nslots, int qcap) {
     extern __shared__ int2 smem[];
     const int T = blockDim.x;
-    int2 *he = smem + threadIdx.x;
-    uint8_t *qs = reinterpret_cast<uint8_t *>(smem + (size_t)(qcap + 1) * T) + threadIdx.x;
+    const size_t row_bytes = (size_t)(qcap + 1) * T * (I16 ? 4 : 8);
+    using Row = typename std::conditional<I16, RowI16, RowI32>::type;
+    Row row;
+    row.T = T;
+    if constexpr (I16) row.he = reinterpret_cast<uint32_t *>(smem) + threadIdx.x;
+    else row.he = smem + threadIdx.x;
+    uint8_t *qs = reinterpret_cast<uint8_t *>(smem) + row_bytes + threadIdx.x;
     const size_t slot = blockIdx.x * (size_t)T + threadIdx.x;
     unsigned long long cells = 0;
     for (size_t p = slot; p < n_small; p += nslots) {
         const size_t k = order[p];
         const swb_global_task tk = a.tasks[k];
         if (tk.qlen > qcap) continue;                                    // the global-scratch kernel's
+        if (fits_i16(a.sc, tk.qlen, tk.tlen) != I16) continue;            // the other instance's
         swb_global_result r{0, 0, tk.w, 1, a.cigar_off[k]};
         const int qlen = tk.qlen, tlen = tk.tlen;
         if (qlen > 0 && tlen > 0) {                                      // :29-31
@@ -297,7 +361,7 @@ __global__ void __launch_bounds__(256) global_smem_kernel(GlobalArgs a, const ui
             int w = imax(w0, abs(qlen - tlen));                          // :47
             int nCol = (int)min((long long)qlen, 2ll * w + 1);           // :48
             ZPacked zp{z + slot, nslots, (nCol + 7) >> 3};
-            int score = global_dp_smem(a.sc, he, qs, T, a, tk, w, zp, cells);
+            int score = global_dp_smem(a.sc, row, qs, T, a, tk, w, zp, cells);
             if (tk.flags & SWB_GLB_RETRY) {                              // CIGARGenerator.swift:88-96
                 int retries = 0;
                 while (score < tk.true_score && retries < 3) {
@@ -307,7 +371,7 @@ __global__ void __launch_bounds__(256) global_smem_kernel(GlobalArgs a, const ui
                     w = imax(w0, abs(qlen - tlen));
                     nCol = (int)min((long long)qlen, 2ll * w + 1);
                     zp.ncw = (nCol + 7) >> 3;
-                    score = global_dp_smem(a.sc, he, qs, T, a, tk, w, zp, cells);
+                    score = global_dp_smem(a.sc, row, qs, T, a, tk, w, zp, cells);
                 }
             }
             r.score = score;
@@ -362,37 +426,48 @@ int launch_global(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     GlobalArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_res, d_cigar, offs, d_cells + kCntGlobal, n, kGlbSmemMaxQ};
     const size_t avail0 = ctx->budget > ctx->allocated ? (ctx->budget - ctx->allocated) / 2 : 0;
 
-    // Shared-memory kernel: block size and blocks per SM that keep the most
-    // threads resident for this query cap.
-    size_t z_bytes = 0, z_nslots = 0;
-    int qcap = 0, T = 0, grid_s = 0;
-    size_t smem = 0;
+    // Shared-memory kernels (int16 rows where exact, int32 rows otherwise):
+    // block size and blocks per SM that keep the most threads resident.
+    struct SmemCfg {
+        int T = 0, grid = 0;
+        size_t smem = 0, nslots = 0;
+    } cfg[2];   // [0] int32 rows, [1] int16 rows
+    size_t z_bytes = 0;
+    int qcap = 0;
+    const size_t n_small_of[2] = {shape.n_small - shape.n_small16, shape.n_small16};
     if (shape.n_small > 0) {
         qcap = imax(shape.small_q, 1);
-        const size_t per_thread = (size_t)(qcap + 1) * 8 + (size_t)((qcap + 7) & ~7);
         int sm_bytes = 0, blk_bytes = 0;
         SWB_CUDA(cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device));
         SWB_CUDA(cudaDeviceGetAttribute(&blk_bytes, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-        int best = 0;
-        for (int t = 32; t <= 256; t += 32) {
-            const size_t b = (size_t)t * per_thread;
-            if (b > (size_t)blk_bytes) break;
-            const int blocks = imin((int)((size_t)sm_bytes / (b + 1024)), 2048 / t);
-            if (blocks * t > best) {
-                best = blocks * t;
-                T = t;
-            }
-        }
-        if (T == 0) return set_error(SWB_ERR_TOO_LARGE, "global alignment rows do not fit shared memory");
-        smem = (size_t)T * per_thread;
-        const int bps = best / T;
-        grid_s = (int)std::min<size_t>((size_t)ctx->sm_count * bps, (shape.n_small + T - 1) / T);
         const size_t per_slot = (size_t)imax(shape.small_t, 1) * (size_t)((qcap + 7) >> 3) * 4;
-        while (grid_s > 1 && (size_t)grid_s * T * per_slot > avail0) grid_s /= 2;
-        z_nslots = (size_t)grid_s * T;
-        z_bytes = (z_nslots * per_slot + 1023) & ~(size_t)1023;
+        size_t max_slots = 0;
+        for (int v = 0; v < 2; ++v) {
+            if (n_small_of[v] == 0) continue;
+            const size_t per_thread = (size_t)(qcap + 1) * (v ? 4 : 8) + (size_t)((qcap + 7) & ~7);
+            int best = 0, T = 0;
+            for (int t = 32; t <= 256; t += 32) {
+                const size_t b = (size_t)t * per_thread;
+                if (b > (size_t)blk_bytes) break;
+                const int blocks = imin((int)((size_t)sm_bytes / (b + 1024)), 2048 / t);
+                if (blocks * t > best) {
+                    best = blocks * t;
+                    T = t;
+                }
+            }
+            if (T == 0) return set_error(SWB_ERR_TOO_LARGE, "global alignment rows do not fit shared memory");
+            SmemCfg &c = cfg[v];
+            c.T = T;
+            c.smem = (size_t)T * per_thread;
+            c.grid = (int)std::min<size_t>((size_t)ctx->sm_count * (best / T), (n_small_of[v] + T - 1) / T);
+            while (c.grid > 1 && (size_t)c.grid * T * per_slot > avail0) c.grid /= 2;
+            c.nslots = (size_t)c.grid * T;
+            max_slots = std::max(max_slots, c.nslots);
+            if (v) SWB_CUDA(cudaFuncSetAttribute(global_smem_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
+            else SWB_CUDA(cudaFuncSetAttribute(global_smem_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c.smem));
+        }
+        z_bytes = (max_slots * per_slot + 1023) & ~(size_t)1023;
         if (z_bytes > avail0) return set_error(SWB_ERR_OOM, "global alignment scratch does not fit the memory budget");
-        SWB_CUDA(cudaFuncSetAttribute(global_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     }
     // Global-scratch kernel for longer queries.
     Scratch s{};
@@ -414,9 +489,15 @@ int launch_global(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     }
     if ((rc = ensure_dev(ctx, ctx->d_scratch, z_bytes + big_bytes + 256))) return rc;
     ProfScope ps(ctx, st, "global_nw_traceback", kCntGlobal);
-    if (shape.n_small > 0) {
-        global_smem_kernel<<<(unsigned)grid_s, T, smem, st>>>(a, order, shape.n_small, (uint32_t *)ctx->d_scratch.p,
-                                                              z_nslots, qcap);
+    for (int v = 1; v >= 0; --v) {   // both instances walk the sorted small tasks, each taking its own
+        if (n_small_of[v] == 0) continue;
+        const SmemCfg &c = cfg[v];
+        if (v)
+            global_smem_kernel<true><<<(unsigned)c.grid, c.T, c.smem, st>>>(a, order, shape.n_small,
+                                                                            (uint32_t *)ctx->d_scratch.p, c.nslots, qcap);
+        else
+            global_smem_kernel<false><<<(unsigned)c.grid, c.T, c.smem, st>>>(a, order, shape.n_small,
+                                                                             (uint32_t *)ctx->d_scratch.p, c.nslots, qcap);
         ctx->launches++;
         SWB_CUDA(cudaGetLastError());
     }

@@ -146,12 +146,24 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
 // run in the shared-memory kernel, longer ones in the global-scratch kernel;
 // the shape gives each group's count and largest query / target.
 constexpr int kGlobalSmemMaxQ = 256;
+// The int16-row NW kernel is exact for a task when (qlen + tlen + 2) times
+// (a + the largest single-step cost) stays below 16000 (swb_global.cu).
+__host__ __device__ inline int nw_i16_cost(int a, int b, int o_del, int e_del, int o_ins, int e_ins) {
+    int p = o_del + e_del;
+    p = p > o_ins + e_ins ? p : o_ins + e_ins;
+    p = p > b ? p : b;
+    return a + (p > 1 ? p : 1);
+}
+__host__ __device__ inline bool nw_fits_i16(int qlen, int tlen, int cost) {
+    return (long long)(qlen + tlen + 2) * cost < 16000;
+}
 struct GlobalShape {
-    size_t n_small = 0, n_big = 0;
+    size_t n_small = 0, n_small16 = 0, n_big = 0;
     int small_q = 0, small_t = 0, big_q = 0, big_t = 0;
-    void add(int qlen, int tlen) {
+    void add(int qlen, int tlen, int cost16) {
         if (qlen <= kGlobalSmemMaxQ) {
             ++n_small;
+            if (nw_fits_i16(qlen, tlen, cost16)) ++n_small16;
             small_q = std::max(small_q, qlen);
             small_t = std::max(small_t, tlen);
         } else {

@@ -470,10 +470,11 @@ int swb_global_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, 
     if ((rc = validate_spans(ctx, tasks, n_tasks, n_bases, &max_q, &max_t))) return rc;
     size_t need = 0;
     GlobalShape shape;
+    const int cost16 = nw_i16_cost(sc->a, sc->b, sc->o_del, sc->e_del, sc->o_ins, sc->e_ins);
     for (size_t i = 0; i < n_tasks; ++i) {
         need += (size_t)tasks[i].qlen + (size_t)tasks[i].tlen;
         const swb_global_task &t = tasks[i];
-        shape.add(t.qlen, t.tlen);
+        shape.add(t.qlen, t.tlen, cost16);
         if (t.qlen > 0 && t.tlen > 0 && std::max(t.w, std::abs(t.qlen - t.tlen)) < 1)
             return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": band width below 1 with equal lengths");
     }

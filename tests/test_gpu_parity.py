@@ -104,12 +104,17 @@ def test_ext_fuzz_int32_path(engine, oracle_mod):
     assert bad.size == 0, f"{bad.size} mismatches: {got[bad[:3]]} vs {exp[bad[:3]]}"
 
 
-@pytest.mark.parametrize("si,qmax", [(0, 200), (3, 200), (4, 200), (0, 420), (5, 420)])
+# Gap and mismatch costs high enough that long tasks leave the int16 rows.
+BIG_PENALTIES = dict(a=1, b=60, o_ins=50, e_ins=30, o_del=45, e_del=35)
+
+
+@pytest.mark.parametrize("si,qmax", [(0, 200), (3, 200), (4, 200), (0, 420), (5, 420), ("big", 200)])
 def test_global_fuzz(engine, oracle_mod, si, qmax):
-    """qmax 420 mixes both kernels in one batch: queries up to 256 bases in
-    the shared-memory kernel, longer ones in the global-scratch kernel."""
-    sc = Scoring.default(**SCORINGS[si])
-    d = gen.global_tasks(2000 + si + qmax, 1500, qmax=qmax)
+    """qmax 420 mixes the shared-memory kernels (queries up to 256 bases) with
+    the global-scratch kernel; the "big" scoring mixes int16 and int32 rows
+    within the shared-memory kernels."""
+    sc = Scoring.default(**(BIG_PENALTIES if si == "big" else SCORINGS[si]))
+    d = gen.global_tasks(2000 + (7 if si == "big" else si) + qmax, 1500, qmax=qmax)
     res, cig = engine.global_batch(sc, d["bases"], d["tasks"])
     eres, ecig, _ = oracle_mod.global_batch(sc, d["bases"], d["tasks"], n_threads=8)
     for k in range(len(res)):
