@@ -412,16 +412,19 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
 
 // Host-side twin of the device bin test, used to size the scratch bin
 // (several host threads for large batches).
+// Longest query among tasks[lo, hi) that the int32 global-scratch bin takes.
+int ext_big_max_q_range(const swb_ext_task *tasks, size_t lo, size_t hi, int max_mat) {
+    int m = 0;
+    for (size_t i = lo; i < hi; ++i) {
+        const swb_ext_task &t = tasks[i];
+        if (t.qlen <= 0 || t.tlen <= 0) continue;
+        if (t.qlen > kExtSmemMaxQ || !fits16(t.qlen, t.h0, max_mat)) m = t.qlen > m ? t.qlen : m;
+    }
+    return m;
+}
+
 int ext_big_max_q(const swb_ext_task *tasks, size_t n, int max_mat) {
-    auto range = [&](size_t lo, size_t hi) {
-        int m = 0;
-        for (size_t i = lo; i < hi; ++i) {
-            const swb_ext_task &t = tasks[i];
-            if (t.qlen <= 0 || t.tlen <= 0) continue;
-            if (t.qlen > kExtSmemMaxQ || !fits16(t.qlen, t.h0, max_mat)) m = t.qlen > m ? t.qlen : m;
-        }
-        return m;
-    };
+    auto range = [&](size_t lo, size_t hi) { return ext_big_max_q_range(tasks, lo, hi, max_mat); };
     const size_t kChunk = 1 << 18;
     const size_t nth = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), (n + kChunk - 1) / kChunk);
     if (nth <= 1) return range(0, n);

@@ -20,6 +20,7 @@
 namespace swb {
 
 int ext_big_max_q(const swb_ext_task *tasks, size_t n, int max_mat);
+int ext_big_max_q_range(const swb_ext_task *tasks, size_t lo, size_t hi, int max_mat);
 
 static thread_local std::string g_last_error;
 
@@ -382,33 +383,56 @@ int swb_ext_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, siz
     ctx->last_ms = 0;
     ctx->last_cells = 0;
     if (n_tasks == 0) return SWB_OK;
-    if ((rc = validate_spans(ctx, tasks, n_tasks, n_bases, nullptr, nullptr))) return rc;
     SWB_CUDA(cudaSetDevice(ctx->device));
     const DevScoring dsc = make_dev_scoring(*sc);
-    const int big_q = ext_big_max_q(tasks, n_tasks, dsc.max_mat);
 
-    // Chunks of at least 1M tasks, at most kMaxChunks; chunk k may start once
-    // the prefix of `bases` its tasks (and all earlier ones) reference is on
-    // the device.
-    const size_t kMinChunk = 1u << 20;
+    // Up to kMaxChunks chunks of at least 512K tasks.  The host checks chunk k
+    // (spans, the bases prefix it needs, the longest query of the int32 bin)
+    // while the GPU works on the chunks before it; chunk k starts once the
+    // prefix of `bases` its tasks reference is on the device.
+    const size_t kMinChunk = 1u << 19;
     const size_t nchunks = std::min<size_t>(kMaxChunks, std::max<size_t>(1, n_tasks / kMinChunk));
     const size_t per = (n_tasks + nchunks - 1) / nchunks;
-    std::vector<size_t> need(nchunks, 0);
-    {
-        std::vector<std::thread> th;
-        for (size_t k = 0; k < nchunks; ++k)
-            th.emplace_back([&, k] {
-                size_t m = 0;
-                for (size_t i = k * per; i < std::min(n_tasks, (k + 1) * per); ++i) {
-                    const swb_ext_task &t = tasks[i];
-                    if (t.qlen > 0) m = std::max<size_t>(m, t.q_off + (size_t)t.qlen);
-                    if (t.tlen > 0 && !(t.flags & SWB_T_FROM_REF)) m = std::max<size_t>(m, t.t_off + (size_t)t.tlen);
-                }
-                need[k] = m;
-            });
-        for (auto &t : th) t.join();
-        for (size_t k = 1; k < nchunks; ++k) need[k] = std::max(need[k], need[k - 1]);
-    }
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    struct Part {
+        int code = 0, big_q = 0;
+        size_t need = 0;
+        std::string err;
+    };
+    std::vector<Part> parts(hw);
+    auto scan_chunk = [&](size_t lo, size_t hi, size_t &need, int &big_q) -> int {
+        const size_t nth = std::min<size_t>(hw, std::max<size_t>(1, (hi - lo) / 16384));
+        const size_t sub = (hi - lo + nth - 1) / nth;
+        auto work = [&](size_t t) {
+            Part &pt = parts[t];
+            pt = Part{};
+            const size_t a = lo + t * sub, b = std::min(hi, a + sub);
+            if (a >= b) return;
+            int mq, mt;
+            if ((pt.code = validate_range(ctx, tasks, a, b, n_bases, &mq, &mt, &pt.err, &pt.code))) return;
+            pt.big_q = ext_big_max_q_range(tasks, a, b, dsc.max_mat);
+            size_t m = 0;
+            for (size_t i = a; i < b; ++i) {
+                const swb_ext_task &tk = tasks[i];
+                if (tk.qlen > 0) m = std::max<size_t>(m, tk.q_off + (size_t)tk.qlen);
+                if (tk.tlen > 0 && !(tk.flags & SWB_T_FROM_REF)) m = std::max<size_t>(m, tk.t_off + (size_t)tk.tlen);
+            }
+            pt.need = m;
+        };
+        if (nth == 1) {
+            work(0);
+        } else {
+            std::vector<std::thread> th;
+            for (size_t t = 0; t < nth; ++t) th.emplace_back(work, t);
+            for (auto &x : th) x.join();
+        }
+        for (size_t t = 0; t < nth; ++t) {
+            if (parts[t].code) return set_error(parts[t].code, parts[t].err);
+            need = std::max(need, parts[t].need);
+            big_q = std::max(big_q, parts[t].big_q);
+        }
+        return SWB_OK;
+    };
     const size_t bases_bytes = align256(std::max<size_t>(n_bases, 1));
     if ((rc = ensure_dev(ctx, ctx->d_bases, bases_bytes + align256(n_tasks * sizeof(swb_ext_task)) + 256))) return rc;
     if ((rc = ensure_dev(ctx, ctx->d_out, n_tasks * sizeof(swb_ext_result)))) return rc;
@@ -420,12 +444,20 @@ int swb_ext_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, siz
     // Copies must not overtake work still using these buffers.
     SWB_CUDA(cudaEventRecord(ctx->fork_ev, ctx->stream));
     SWB_CUDA(cudaStreamWaitEvent(ctx->h2d, ctx->fork_ev, 0));
-    size_t copied = 0;
+    size_t copied = 0, need = 0;
     for (size_t k = 0; k < nchunks; ++k) {
         const size_t lo = k * per, hi = std::min(n_tasks, lo + per);
-        if (need[k] > copied) {
-            SWB_CUDA(cudaMemcpyAsync(d_b + copied, bases + copied, need[k] - copied, cudaMemcpyHostToDevice, ctx->h2d));
-            copied = need[k];
+        if (lo >= hi) break;
+        int big_q = 0;
+        if ((rc = scan_chunk(lo, hi, need, big_q))) {
+            // Let the chunks already queued finish before reporting (they write `out`).
+            cudaStreamSynchronize(ctx->d2h);
+            cudaStreamSynchronize(ctx->stream);
+            return rc;
+        }
+        if (need > copied) {
+            SWB_CUDA(cudaMemcpyAsync(d_b + copied, bases + copied, need - copied, cudaMemcpyHostToDevice, ctx->h2d));
+            copied = need;
         }
         SWB_CUDA(cudaMemcpyAsync(d_t + lo, tasks + lo, (hi - lo) * sizeof(swb_ext_task), cudaMemcpyHostToDevice, ctx->h2d));
         SWB_CUDA(cudaEventRecord(ctx->chunk_in[k], ctx->h2d));
