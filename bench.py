@@ -117,11 +117,7 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- helpers
-def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+from swiftbwa_b200.sharding import dist_env, max_over_ranks, whole_job_rate  # noqa: E402
 
 
 def traffic_per_launch(kernel: str):
@@ -547,11 +543,7 @@ def run_ours(args):
     launches = eng.kernel_launches() - launches0
     prof = eng.profile_read()
     eng.profile(False)
-    ms_max = ms
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, dist, dev)
     gpu_out = d_out.cpu().numpy().view(EXT_RESULT_DTYPE)
 
     cells_step = sum(v[2] for v in prof.values()) / args.steps
@@ -580,13 +572,9 @@ def run_ours(args):
         t0 = time.perf_counter()
         for _ in range(args.steps):
             eng.ext_batch(sc, hb, ht, out=ho)
-        wall = (time.perf_counter() - t0) / args.steps
-        if dist:
-            t = torch.tensor([wall], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            wall = float(t.item())
+        wall = max_over_ranks((time.perf_counter() - t0) / args.steps, dist, dev)
         assert np.array_equal(ho, gpu_out), "host and device entry points disagree"
-        e2e = {"value": n * ws / wall, "unit": "ext/s", "h2d_bytes_per_step": int(hb.nbytes + ht.nbytes),
+        e2e = {"value": whole_job_rate(n, ws, wall), "unit": "ext/s", "h2d_bytes_per_step": int(hb.nbytes + ht.nbytes),
                "d2h_bytes_per_step": int(ho.nbytes), "ms_per_step": wall * 1e3}
 
     cpu = None
@@ -601,7 +589,7 @@ def run_ours(args):
     if rank == 0:
         line = {
             "metric": "extensions/s (bit-exact banded SW extension, config 1)",
-            "value": n * ws / (ms_max * 1e-3), "unit": "ext/s", "n_gpus": ws, "steps": args.steps,
+            "value": whole_job_rate(n, ws, ms_max * 1e-3), "unit": "ext/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "wall_ms_per_step": wall_ms,
             "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32",
