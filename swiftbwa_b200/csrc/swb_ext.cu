@@ -247,6 +247,8 @@ __global__ void __launch_bounds__(T) ext_fast_kernel(ExtArgs a, int bin) {
     extern __shared__ uint32_t sm[];
     uint32_t *he = sm + threadIdx.x;
     uint16_t *qs = U8 ? nullptr : (uint16_t *)(sm + (QMAX + 1) * T) + threadIdx.x;
+    uint16_t *he16 = reinterpret_cast<uint16_t *>(sm) + threadIdx.x;                        // int8 rows
+    uint8_t *qc = reinterpret_cast<uint8_t *>(sm) + (size_t)(QMAX + 1) * T * 2 + threadIdx.x;
     const uint32_t lo = a.bin_start[bin], hi = a.bin_start[bin + 1];
     unsigned long long cells = 0;
     const uint32_t span = hi - lo;
@@ -261,9 +263,9 @@ __global__ void __launch_bounds__(T) ext_fast_kernel(ExtArgs a, int bin) {
             if (!U8)
                 ext_fast_one<T, false>(a, tk, he, qs, r, cells);
             else if (a.sc.o_del + a.sc.e_del == a.sc.o_ins + a.sc.e_ins)
-                ext_pair_one<T, true>(a, tk, he, r, cells);
+                ext_pair_one<T, true>(a, tk, he16, qc, r, cells);
             else
-                ext_pair_one<T, false>(a, tk, he, r, cells);
+                ext_pair_one<T, false>(a, tk, he16, qc, r, cells);
             a.out[ti] = r;
         }
     }
@@ -293,7 +295,10 @@ __global__ void __launch_bounds__(kBigT) ext_global_kernel(ExtArgs a, int *h, in
 
 template <int QMAX, bool U8>
 constexpr size_t fast_smem_bytes() {
-    return (size_t)(QMAX + 1) * kFastT * sizeof(uint32_t) + (U8 ? 0 : (size_t)QMAX * kFastT * sizeof(uint16_t));
+    // int8 rows: a 16-bit word and a query byte per column; int16 rows: a
+    // 32-bit word and a 16-bit selector per column.
+    return U8 ? ((size_t)(QMAX + 1) * kFastT * sizeof(uint16_t) + (size_t)QMAX * kFastT + 15) & ~(size_t)15
+              : (size_t)(QMAX + 1) * kFastT * sizeof(uint32_t) + (size_t)QMAX * kFastT * sizeof(uint16_t);
 }
 
 const char *const kBinNames[kNumBins] = {

@@ -1,20 +1,22 @@
 // swb_ext_pair.cuh -- BandedSWScalar.align (Sources/Alignment/BandedSWScalar.swift:21-191)
 // for int8-bounded tasks, two target rows per pass.
 //
-// Row layout (shared memory, one 32-bit word per query column, [column][thread]):
-//   bits  0-15  prmt selector of the column's query base q: nibbles (q, q|8, 5, 5),
-//               i.e. the row's score for q as a 16-bit value ([s, sign, 0, 0])
-//   bits 16-23  H of the previous row at the previous column (the diagonal input)
-//   bits 24-31  E into this column
-// exactly the reference's h[j] / e[j] storage (`h[j]` holds the left neighbour's
-// H once the row has passed it), with the scores bounded by 255.
+// Row layout (shared memory, [column][thread]):
+//   16-bit word per column: bits 0-7 H of the previous row at the previous
+//   column (the diagonal input), bits 8-15 E into this column -- exactly the
+//   reference's h[j] / e[j] storage (`h[j]` holds the left neighbour's H once
+//   the row has passed it), with the scores bounded by 255;
+//   one byte per column: the query base q, from which the prmt selector
+//   (q, q|8, 5, 5) -- the row's score for q as a 16-bit value [s, sign, 0, 0]
+//   -- is formed with one multiply-add.
+// Three bytes per column keep ~17 one-warp blocks resident per SM.
 //
 // Rows i and i+1 advance together, row i+1 one column behind row i: at step c
 // row i computes column c from the word it loads, and row i+1 computes
 // column c-1 from the values row i produced for column c-1 one step earlier
 // (the word row i would have stored).  The two cells are independent, so they
 // run as the low and high 16-bit lanes of one register through the DPX
-// s16x2 forms: one shared load, one 16-bit shared store and ~13 ALU
+// s16x2 forms: two shared loads (word, query byte), one 16-bit store and ~13 ALU
 // operations per two cells.  Row i's words are never stored: row i+1
 // consumes them from registers and overwrites the same columns.
 //
@@ -54,18 +56,18 @@ struct PairConsts {
 // upper half (h1 before, E') and updates h1, f, key, lastJ.  SYM: the open
 // costs oDel+eDel and oIns+eIns are equal, so E' and F' share one operand.
 template <bool SYM>
-__device__ __forceinline__ uint32_t single_cell(const PairConsts &pc, const RowTable &rt, uint32_t w, int j,
-                                                uint32_t &h1, uint32_t &f, uint32_t &key, uint32_t &lastJ) {
-    const uint32_t s = lane_score(rt, w);
-    const uint32_t M = __byte_perm(w, 0u, 0x4442);          // [H, 0, 0, 0]
-    const uint32_t e = __byte_perm(w, 0u, 0x4443);          // [E, 0, 0, 0]
+__device__ __forceinline__ uint32_t single_cell(const PairConsts &pc, const RowTable &rt, uint32_t w, uint32_t sel,
+                                                int j, uint32_t &h1, uint32_t &f, uint32_t &key, uint32_t &lastJ) {
+    const uint32_t s = lane_score(rt, sel);
+    const uint32_t M = __byte_perm(w, 0u, 0x4440);          // [H, 0, 0, 0]
+    const uint32_t e = __byte_perm(w, 0u, 0x4441);          // [E, 0, 0, 0]
     const uint32_t d = __viaddmin_s16x2_relu(M, s, M * 128u);
     const uint32_t H = __vimax3_s16x2(d, e, f);
     const uint32_t tDel = __viaddmax_s16x2(d, pc.negOeDel, 0x80008000u);
     const uint32_t nE = __viaddmax_s16x2_relu(e, pc.negEDel, tDel);
     const uint32_t tIns = SYM ? tDel : __viaddmax_s16x2(d, pc.negOeIns, 0x80008000u);
     f = __viaddmax_s16x2_relu(f, pc.negEIns, tIns);
-    const uint32_t up = __byte_perm(h1, nE, 0x0040);         // [h1, E'] -> bits 16-31 of the word
+    const uint32_t up = __byte_perm(h1, nE, 0x0040);         // [h1, E'] -> the column's new word
     const uint32_t Hs = H * 256u;
     key = __viaddmax_u16x2(Hs, (uint32_t)j, key);
     lastJ = __vimax3_u16x2(lastJ, __vimin3_u16x2((uint32_t)j, Hs, (uint32_t)j), lastJ);
@@ -73,9 +75,10 @@ __device__ __forceinline__ uint32_t single_cell(const PairConsts &pc, const RowT
     return up;
 }
 
-__device__ __forceinline__ void store_up(uint32_t *he, int T, int j, uint32_t up) {
-    reinterpret_cast<uint16_t *>(he + j * T)[1] = (uint16_t)up;
-}
+__device__ __forceinline__ void store_up(uint16_t *he, int T, int j, uint32_t up) { he[j * T] = (uint16_t)up; }
+
+// prmt selector (q, q|8, 5, 5) of query code q (0-4).
+__device__ __forceinline__ uint32_t sel_of(uint32_t q) { return q * 0x11u + 0x5580u; }
 
 // Row-end bookkeeping of BandedSWScalar.swift:149-172 for row `row`; returns
 // false when the task stops after this row.
@@ -107,8 +110,9 @@ struct RowTrack {
 };
 
 template <int T, bool SYM>
-__device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_task &tk, uint32_t *__restrict__ he,
-                                             swb_ext_result &res, unsigned long long &cells) {
+__device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_task &tk, uint16_t *__restrict__ he,
+                                             uint8_t *__restrict__ qc, swb_ext_result &res,
+                                             unsigned long long &cells) {
     res = swb_ext_result{0, 0, 0, 0, 0, 0};
     const int qlen = tk.qlen, tlen = tk.tlen;
     if (!(qlen > 0 && tlen > 0)) return;                                      // :33-35
@@ -137,8 +141,8 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
             } else {
                 ramp = false;
             }
-            const uint32_t q = j < qlen ? span_base(a.bases, a.pac, tk.q_off, j, qlen, tk.flags, false) : 4u;
-            he[j * T] = (q | ((q | 8u) << 4) | 0x5500u) | ((uint32_t)hj << 16);
+            if (j < qlen) qc[j * T] = (uint8_t)span_base(a.bases, a.pac, tk.q_off, j, qlen, tk.flags, false);
+            he[j * T] = (uint16_t)hj;
         }
     }
     int w = tk.w;                                                              // :52-62
@@ -178,15 +182,16 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
         const int lo1 = i + 1 - w;
         int firstNz = -1;                 // first nonzero word of row i
         int c = b0;
-        uint32_t hPrev = 0u, nEPrev = 0u, wPrev = 0u;   // row i's word for column c-1 (registers)
+        uint32_t hPrev = 0u, nEPrev = 0u, sPrev = 0u;   // row i's word and selector for column c-1
         bool started = false;
         for (; c < e0; ++c) {
             const uint32_t wd = he[c * T];
+            const uint32_t sel = sel_of(qc[c * T]);
             const uint32_t hb = h1;
-            const uint32_t up = single_cell<SYM>(pc, rt0, wd, c, h1, f, key, lastJ);
+            const uint32_t up = single_cell<SYM>(pc, rt0, wd, sel, c, h1, f, key, lastJ);
             hPrev = hb;
             nEPrev = up >> 8;           // E' of row i at column c (byte 1 of up)
-            wPrev = wd;
+            sPrev = sel;
             if (firstNz < 0 && (up & 0xFFFFu) != 0u) firstNz = c;
             if (pair && firstNz >= 0 && c >= lo1) {
                 ++c;
@@ -206,9 +211,10 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
 #pragma unroll 2
             for (; c < e0; ++c, jp += 0x10001u) {
                 const uint32_t wd = he[c * T];
-                const uint32_t Mp = __byte_perm(wd, hPrevP, 0x5452);            // [H(i-1,c-1), H(i,c-2)]
-                const uint32_t ep = __byte_perm(wd, nEPrev, 0x5453);            // [E(i,c),     E(i+1,c-1)]
-                const uint32_t sp = lane_score(rt1, wPrev) * 65536u + lane_score(rt0, wd);
+                const uint32_t sel = sel_of(qc[c * T]);
+                const uint32_t Mp = __byte_perm(wd, hPrevP, 0x5450);            // [H(i-1,c-1), H(i,c-2)]
+                const uint32_t ep = __byte_perm(wd, nEPrev, 0x5451);            // [E(i,c),     E(i+1,c-1)]
+                const uint32_t sp = lane_score(rt1, sPrev) * 65536u + lane_score(rt0, sel);
                 const uint32_t d = __viaddmin_s16x2_relu(Mp, sp, Mp * 128u);
                 const uint32_t H = __vimax3_s16x2(d, ep, fp);
                 const uint32_t tDel = __viaddmax_s16x2(d, pc.negOeDel, 0x80008000u);
@@ -220,7 +226,7 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
                 keyp = __viaddmax_u16x2(Hs, jp, keyp);
                 lastJp = __vimax3_u16x2(lastJp, __vimin3_u16x2(jp, Hs, jp), lastJp);
                 hPrevP = h1p;
-                wPrev = wd;
+                sPrev = sel;
                 nEPrev = nE;    // byte 0 = row i's E', byte 1 = 0 (lane values <= 255)
                 h1p = H;
             }
@@ -250,26 +256,26 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
         for (; s < e1; ++s) {
             // Row i's word for column s: from registers (c-1 = e0-1), the row-end word, or untouched.
             uint32_t wd = he[s * T];
-            if (s == e0 - 1) wd = (wd & 0xFFFFu) | (hPrev << 16) | (nEPrev << 24);
-            else if (s == e0) wd = (wd & 0xFFFFu) | ((uint32_t)h1i << 16);
-            const uint32_t up = single_cell<SYM>(pc, rt1, wd, s, h1b, f1, k1, lj1);
+            if (s == e0 - 1) wd = hPrev | ((nEPrev & 0xFFu) << 8);
+            else if (s == e0) wd = (uint32_t)h1i;
+            const uint32_t up = single_cell<SYM>(pc, rt1, wd, sel_of(qc[s * T]), s, h1b, f1, k1, lj1);
             store_up(he, T, s, up);
         }
         // H of row i+1's last valid column: from the register if it was the last
         // cell computed, else from the word the lockstep stored at column e1.
         int h1last = (int)(h1b & 0xFFFFu);
         const bool overran = started && e1 <= e0 - 2;
-        if (overran) h1last = (int)((he[e1 * T] >> 16) & 0xFFu);
+        if (overran) h1last = (int)(he[e1 * T] & 0xFFu);
         const int key1 = (int)(k1 & 0xFFFFu);
         const int rowMax1 = e1 > b1 ? key1 >> 8 : 0;
         // Words the reference holds after row i+1: h[e1] = H(e1-1), e[e1] = 0,
         // then row i's zero tail up to e0.
-        he[e1 * T] = (he[e1 * T] & 0xFFFFu) | ((uint32_t)h1last << 16);
-        for (int z = e1 + 1; z <= e0; ++z) he[z * T] &= 0xFFFFu;
+        he[e1 * T] = (uint16_t)h1last;
+        for (int z = e1 + 1; z <= e0; ++z) he[z * T] = 0;
         if (!tr.finish(i + 1, rowMax1, key1 & 0xFF, h1last, e1 == qlen, zDrop, eDel, eIns)) break;
         // Narrowing after row i+1 (:175-180).
         int nb = b1;
-        while (nb < e1 && (he[nb * T] >> 16) == 0u) ++nb;
+        while (nb < e1 && he[nb * T] == 0) ++nb;
         beg = nb;
         // The last nonzero word is one past the last column with H > 0 (lane 1's
         // tracker; columns past e1 computed ahead of row i's end only decay from it).
