@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--c4-ref-len", type=int, default=1_000_000_000)
     ap.add_argument("--c4-pool", type=int, default=3_000_000)
     ap.add_argument("--sat-requests", type=int, default=120)
+    ap.add_argument("--c4-wave", type=int, default=1 << 18, help="served mode: tasks per wave")
     ap.add_argument("--c5-chains", type=int, default=1_000_000)
     ap.add_argument("--c3-jobs", type=int, default=1_000_000)
     ap.add_argument("--suite-only", default="",
@@ -399,7 +400,7 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
         pt = torch.from_numpy(pool.tasks.view(np.uint8)).pin_memory().numpy().view(pool.tasks.dtype)
         po = torch.empty(len(pool.tasks) * EXT_RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy().view(EXT_RESULT_DTYPE)
         reqs = S.request_stream(W.SEED_BASE + 4 + 2, len(pool.tasks), rate=200.0, duration=args.serve_seconds)
-        srv = S.Server(eng, sc, arena_bytes=1 << 30, max_wave_tasks=1 << 19)
+        srv = S.Server(eng, sc, arena_bytes=1 << 30, max_wave_tasks=args.c4_wave)
         res, span = S.run_pool_stream(srv, pb, pt, po, reqs, open_loop=True)
         st = srv.stats()
         srv.stop()
@@ -409,13 +410,14 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
               "ext_per_s": sum(n for n, _ in res) / span, "p50_ms": _pct(lat, 50) * 1e3, "p99_ms": _pct(lat, 99) * 1e3,
               "p50_ms_50k_200k": _pct(mid, 50) * 1e3 if mid else None,
               "p99_ms_50k_200k": _pct(mid, 99) * 1e3 if mid else None, "n_50k_200k": len(mid),
-              "waves": st["waves"], "wave_device_ms_sum": st["busy_ms"], "span_s": span,
+              "waves": st["waves"], "wave_tasks": args.c4_wave, "wave_device_ms_sum": st["busy_ms"], "span_s": span,
               "stream": "Poisson 200 req/s, sizes log-uniform 1k-1M tasks, qlen log-uniform 30-250, w 10-100, h0 19-60, "
                         "1 Gbp resident 2-bit reference"}
         # saturation: the same size distribution submitted at once, served vs plain
         sat = S.request_stream(W.SEED_BASE + 4 + 3, len(pool.tasks), rate=1e6, duration=args.sat_requests / 1e6)
         for mode, plain in (("served", 0), ("plain_batching", 1), ("plain_kernel", 2)):
-            srv = S.Server(eng, sc, arena_bytes=1 << 30, max_wave_tasks=1 << 19 if plain == 0 else 1 << 20, plain=plain)
+            srv = S.Server(eng, sc, arena_bytes=1 << 30, max_wave_tasks=args.c4_wave if plain == 0 else 1 << 20,
+                           plain=plain)
             r_, span_ = S.run_pool_stream(srv, pb, pt, po, sat, open_loop=False)
             srv.stop()
             c4[f"saturation_{mode}_ext_per_s"] = sum(n for n, _ in r_) / span_

@@ -7,14 +7,15 @@
 //     into a device arena (first-fit, arena_bytes), which is the admission
 //     budget: a request whose bases do not fit waits until earlier ones free
 //     their space;
-//   * forms waves of at most max_wave_tasks tasks from the head of the
-//     queue, splitting large requests across waves so that small ones do not
-//     wait behind them;
+//   * forms waves of at most max_wave_tasks tasks, taking requests by least
+//     remaining work (those waiting longer than 50 ms first, by arrival) and
+//     splitting large requests across waves, so that short requests do not
+//     wait behind the waves of long ones;
 //   * copies each piece of a wave straight from the caller's buffers when
 //     they are pinned (the task offsets are then rebased into the arena by a
 //     small kernel), or through a pinned bounce buffer when they are not;
 //   * runs a wave as one sort + binned extension pass over all its tasks
-//     (the launch sequence of swb_ext_batch), alternating between two lanes
+//     (the launch sequence of swb_ext_batch), rotating over three lanes
 //     -- internal contexts with their own streams and buffers sharing the
 //     resident reference -- so one wave's copies overlap the other's kernels;
 //   * copies each request's slice of a wave's results back (directly into a
@@ -43,6 +44,8 @@ using namespace swb;
 namespace {
 
 constexpr int kMaxPieces = 4096;   // pieces (request slices) per wave
+constexpr int kLanes = 3;          // waves in flight at once
+constexpr uint64_t kAgeNs = 50'000'000;   // a request waiting longer than this is served in arrival order
 
 inline size_t align_up256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -162,7 +165,7 @@ struct swb_server {
     size_t max_wave = 1u << 20;
     uint8_t *d_arena = nullptr;
     Arena arena;
-    Lane lanes[2];
+    Lane lanes[kLanes];
     int next_lane = 0;
     std::thread worker;
     std::mutex mu;
@@ -222,7 +225,24 @@ bool launch_wave(swb_server *s, Lane &L) {
     size_t wn = 0;
     int npin = 0;
     bool host_staged = false;
-    for (Req *r : s->queue) {
+    // Wave order: requests that have waited longer than kAgeNs first, by
+    // arrival; then the others by least remaining work (so a short request
+    // does not queue behind the waves of a long one).  Plain mode keeps the
+    // arrival order, one request per wave.
+    std::vector<Req *> order;
+    order.reserve(s->queue.size());
+    for (Req *r : s->queue)
+        if (r->dispatched < r->n) order.push_back(r);
+    if (!s->plain) {
+        const uint64_t now = now_ns();
+        std::stable_sort(order.begin(), order.end(), [&](const Req *x, const Req *y) {
+            const bool ox = now - x->t_submit > kAgeNs, oy = now - y->t_submit > kAgeNs;
+            if (ox != oy) return ox;
+            if (ox) return false;   // both old: arrival order (the queue's)
+            return x->n - x->dispatched < y->n - y->dispatched;
+        });
+    }
+    for (Req *r : order) {
         if (wn >= s->max_wave || (int)L.pieces.size() >= kMaxPieces) break;
         if (r->dispatched == r->n) continue;
         if (!r->staged) {
@@ -296,7 +316,8 @@ bool launch_wave(swb_server *s, Lane &L) {
     L.launch_rc = rc;
     cudaEventRecord(L.ev_done, rc ? st : d2h);
     L.busy = true;
-    while (!s->queue.empty() && s->queue.front()->dispatched == s->queue.front()->n) s->queue.pop_front();
+    s->queue.erase(std::remove_if(s->queue.begin(), s->queue.end(), [](const Req *r) { return r->dispatched == r->n; }),
+                   s->queue.end());
     return true;
 }
 
@@ -313,7 +334,7 @@ void worker_loop(swb_server *s) {
         const bool have_work = !s->paused && std::any_of(s->queue.begin(), s->queue.end(),
                                                           [](Req *r) { return r->dispatched < r->n; });
         if (have_work) {
-            const int nl = s->plain ? 1 : 2;
+            const int nl = s->plain ? 1 : kLanes;
             for (int k = 0; k < nl; ++k) {
                 Lane &L = s->lanes[(s->next_lane + k) % nl];
                 if (!L.busy) {
@@ -325,7 +346,7 @@ void worker_loop(swb_server *s) {
                 }
             }
         }
-        const bool inflight = s->lanes[0].busy || s->lanes[1].busy;
+        const bool inflight = std::any_of(std::begin(s->lanes), std::end(s->lanes), [](const Lane &L) { return L.busy; });
         if (s->stopping && !inflight && !have_work) break;
         if (!progressed) {
             if (inflight) {
