@@ -249,13 +249,18 @@ __global__ void __launch_bounds__(T) ext_fast_kernel(ExtArgs a, int bin) {
     uint16_t *qs = U8 ? nullptr : (uint16_t *)(sm + (QMAX + 1) * T) + threadIdx.x;
     uint16_t *he16 = reinterpret_cast<uint16_t *>(sm) + threadIdx.x;                        // int8 rows
     uint8_t *qc = reinterpret_cast<uint8_t *>(sm) + (size_t)(QMAX + 1) * T * 2 + threadIdx.x;
+    static_assert(T == 32, "one warp per block: the warp claims its tasks together");
     const uint32_t lo = a.bin_start[bin], hi = a.bin_start[bin + 1];
     unsigned long long cells = 0;
     const uint32_t span = hi - lo;
-    const uint32_t per_iter = gridDim.x * (uint32_t)T;
-    const uint32_t iters = (span + per_iter - 1) / per_iter;
-    for (uint32_t it = 0; it < iters; ++it) {
-        const uint32_t pos = lo + it * per_iter + blockIdx.x * T + threadIdx.x;
+    // Resident blocks claim the next 32 sorted tasks of the bin from a
+    // counter, so blocks that draw long tasks do not hold up the bin.
+    for (;;) {
+        uint32_t base = 0;
+        if (threadIdx.x == 0) base = atomicAdd(a.claim + bin, (uint32_t)T);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= span) break;
+        const uint32_t pos = lo + base + threadIdx.x;
         if (pos < hi) {
             const uint32_t ti = a.order[pos];
             const swb_ext_task tk = a.tasks[ti];
@@ -317,8 +322,7 @@ int launch_fast(swb_ctx *ctx, const ExtArgs &a, int bin, size_t n, cudaStream_t 
         SWB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ext_fast_kernel<QMAX, kFastT, U8>, kFastT, smem));
         if (occ < 1) occ = 1;
     }
-    const size_t need = (n + kFastT - 1) / kFastT;
-    const size_t grid = std::min<size_t>(need, (size_t)ctx->sm_count * occ);
+    const size_t grid = std::min<size_t>((n + kFastT - 1) / kFastT, (size_t)ctx->sm_count * occ);
     if (grid == 0) return SWB_OK;
     ProfScope ps(ctx, s, kBinNames[bin], kCntExtBin0 + bin);
     ext_fast_kernel<QMAX, kFastT, U8><<<(unsigned)grid, kFastT, smem, s>>>(a, bin);
@@ -351,7 +355,8 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     uint32_t *idx = (uint32_t *)ctx->d_idx.p, *idx2 = (uint32_t *)ctx->d_idx2.p;
     uint32_t *bin_start = (uint32_t *)ctx->d_misc.p;          // kNumBins+1 words
     int *big_max_q = (int *)((char *)ctx->d_misc.p + 128);
-    SWB_CUDA(cudaMemsetAsync(big_max_q, 0, sizeof(int), s));
+    uint32_t *claim = (uint32_t *)((char *)ctx->d_misc.p + 160);   // kNumBins claim counters
+    SWB_CUDA(cudaMemsetAsync(big_max_q, 0, 128, s));                  // big_max_q and the counters
     const unsigned tb = 256;
     {
         ProfScope ps(ctx, s, "ext_keys", -1);
@@ -392,7 +397,7 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     }
 
     // Fork: every bin runs on its own stream after the sort, then joins back.
-    ExtArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_out, idx2, bin_start, d_cells};
+    ExtArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_out, idx2, bin_start, d_cells, claim};
     ProfScope pass(ctx, s, "ext_pass", -1);   // fork to join, on the launching stream
     SWB_CUDA(cudaEventRecord(ctx->fork_ev, s));
     for (int b = 0; b < kNumBins; ++b) {

@@ -18,6 +18,7 @@ struct ExtArgs {
     const uint32_t *order;      // sorted task indices
     const uint32_t *bin_start;  // kNumBins + 1 entries
     unsigned long long *cells;
+    uint32_t *claim = nullptr;  // per-bin claim counters (zeroed per pass)
 };
 
 // True when every H/E of the task fits int16: H <= h0 + qlen*maxMat
