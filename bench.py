@@ -554,7 +554,7 @@ def run_ours(args):
     # launching stream (one "ext_pass" launch per step), all bins' cells.
     pass_launches, pass_ms, _ = prof["ext_pass"]
     bin_cells = sum(v[2] for k, v in prof.items() if k.startswith("ext_"))
-    dom_name = "ext_pass (ext_fast_q32..q256 + ext_global_i32, concurrent bins)"
+    dom_name = "ext_pass (ext_fast_q32..q256 + ext_big_i32, concurrent bins)"
     achieved = (bin_cells / pass_launches) * OPS_PER_CELL_EXT / (pass_ms / pass_launches * 1e-3)
     step_ms_sum = sum(v[1] for k, v in prof.items() if k in ("ext_keys", "cub_radix_sort", "bin_bounds", "ext_pass"))
     kernels = {k: {"launches": v[0], "ms_per_step": v[1] / args.steps,

@@ -45,6 +45,7 @@
 #include "swb_device.cuh"
 #include "swb_ext_dp.cuh"
 #include "swb_ext_pair.cuh"
+#include "swb_ext_warp.cuh"
 #include "swb_internal.h"
 
 namespace swb {
@@ -277,8 +278,39 @@ __global__ void __launch_bounds__(T) ext_fast_kernel(ExtArgs a, int bin) {
     add_cells(a.cells + kCntExtBin0 + bin, cells);
 }
 
+// Queries above 256 bases or scores beyond int16, up to kWarpMaxQ bases: one
+// warp per extension (swb_ext_warp.cuh), rows in shared memory, warps claim
+// tasks of the bin one at a time.
+__global__ void __launch_bounds__(256) ext_warp_kernel(ExtArgs a, int qcap) {
+    extern __shared__ __align__(16) uint8_t wsm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const size_t stride = ((size_t)(qcap + 1) * 8 + (size_t)qcap + 15) & ~(size_t)15;
+    int *h = reinterpret_cast<int *>(wsm + warp * stride);
+    int *e = h + (qcap + 1);
+    uint8_t *qc = reinterpret_cast<uint8_t *>(e + (qcap + 1));
+    const uint32_t lo = a.bin_start[kBigBin], hi = a.bin_start[kBigBin + 1];
+    const uint32_t span = hi - lo;
+    unsigned long long cells = 0;
+    for (;;) {
+        uint32_t k = 0;
+        if (lane == 0) k = atomicAdd(a.claim + kBigBin, 1u);
+        k = __shfl_sync(0xFFFFFFFFu, k, 0);
+        if (k >= span) break;
+        const uint32_t ti = a.order[lo + k];
+        const swb_ext_task tk = a.tasks[ti];
+        if (tk.qlen > qcap) continue;                 // the global-scratch kernel's
+        swb_ext_result r;
+        ext_warp_one(a, tk, h, e, qc, r, cells);
+        if (lane == 0) a.out[ti] = r;
+        __syncwarp();
+    }
+    add_cells(a.cells + kCntExtBin0 + kBigBin, cells);
+}
+
+// Queries above kWarpMaxQ: one thread per extension over int32 rows in
+// global scratch (tasks with qlen <= skip_le belong to the warp kernel).
 __global__ void __launch_bounds__(kBigT) ext_global_kernel(ExtArgs a, int *h, int *e, uint8_t *q,
-                                                           size_t nslots) {
+                                                           size_t nslots, int skip_le) {
     const uint32_t lo = a.bin_start[kBigBin], hi = a.bin_start[kBigBin + 1];
     const size_t slot = blockIdx.x * (size_t)kBigT + threadIdx.x;
     Global32 st{h, e, q, nslots, slot};
@@ -290,6 +322,7 @@ __global__ void __launch_bounds__(kBigT) ext_global_kernel(ExtArgs a, int *h, in
         if (pos < hi) {
             const uint32_t ti = a.order[pos];
             const swb_ext_task tk = a.tasks[ti];
+            if (tk.qlen <= skip_le) continue;
             swb_ext_result r;
             ext_one(a, tk, st, r, cells);
             a.out[ti] = r;
@@ -310,7 +343,7 @@ const char *const kBinNames[kNumBins] = {
     "ext_u8_q32",  "ext_u8_q48",  "ext_u8_q64",  "ext_u8_q80",  "ext_u8_q96",  "ext_u8_q112",  "ext_u8_q128",
     "ext_u8_q160", "ext_u8_q192", "ext_u8_q256", "ext_i16_q32", "ext_i16_q48", "ext_i16_q64",  "ext_i16_q80",
     "ext_i16_q96", "ext_i16_q112", "ext_i16_q128", "ext_i16_q160", "ext_i16_q192", "ext_i16_q256",
-    "ext_global_i32"};
+    "ext_big_i32"};
 
 template <int QMAX, bool U8>
 int launch_fast(swb_ctx *ctx, const ExtArgs &a, int bin, size_t n, cudaStream_t s) {
@@ -391,9 +424,21 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     if (max_q > kMaxLen) return set_error(SWB_ERR_TOO_LARGE, "query longer than 65535 bases");
     const size_t nslots = (size_t)ctx->sm_count * 4 * kBigT;
     const size_t cols = (size_t)max_q + 1;
-    if (max_q > 0) {
+    if (max_q > kWarpMaxQ) {
         const size_t bytes = cols * nslots * (2 * sizeof(int) + 1) + 256;
         if ((rc = ensure_dev(ctx, ctx->d_scratch, bytes))) return rc;
+    }
+    // Warp kernel shape for the big bin: warps per block from the rows' size.
+    const int wq = imin(max_q, kWarpMaxQ);
+    const size_t wstride = ((size_t)(wq + 1) * 8 + (size_t)wq + 15) & ~(size_t)15;
+    int wwarps = 0, wblocks = 0;
+    if (max_q > 0) {
+        wwarps = (int)std::max<size_t>(1, std::min<size_t>(8, (size_t)(200 * 1024) / wstride));
+        SWB_CUDA(cudaFuncSetAttribute(ext_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(wwarps * wstride)));
+        SWB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wblocks, ext_warp_kernel, wwarps * 32,
+                                                               wwarps * wstride));
+        wblocks = imax(wblocks, 1) * ctx->sm_count;
     }
 
     // Fork: every bin runs on its own stream after the sort, then joins back.
@@ -406,13 +451,18 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
         if (b < kFastBins) {
             if ((rc = kFastLaunch[b](ctx, a, b, n, sb))) return rc;
         } else if (max_q > 0) {
-            int *hbuf = (int *)ctx->d_scratch.p;
-            int *ebuf = hbuf + cols * nslots;
-            uint8_t *qbuf = (uint8_t *)(ebuf + cols * nslots);
             ProfScope ps(ctx, sb, kBinNames[kBigBin], kCntExtBin0 + kBigBin);
-            ext_global_kernel<<<(unsigned)(nslots / kBigT), kBigT, 0, sb>>>(a, hbuf, ebuf, qbuf, nslots);
+            ext_warp_kernel<<<(unsigned)wblocks, wwarps * 32, wwarps * wstride, sb>>>(a, wq);
             ctx->launches++;
             SWB_CUDA(cudaGetLastError());
+            if (max_q > kWarpMaxQ) {
+                int *hbuf = (int *)ctx->d_scratch.p;
+                int *ebuf = hbuf + cols * nslots;
+                uint8_t *qbuf = (uint8_t *)(ebuf + cols * nslots);
+                ext_global_kernel<<<(unsigned)(nslots / kBigT), kBigT, 0, sb>>>(a, hbuf, ebuf, qbuf, nslots, wq);
+                ctx->launches++;
+                SWB_CUDA(cudaGetLastError());
+            }
         }
         SWB_CUDA(cudaEventRecord(ctx->join_ev[b], sb));
         SWB_CUDA(cudaStreamWaitEvent(s, ctx->join_ev[b], 0));
