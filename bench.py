@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--c4-pool", type=int, default=3_000_000)
     ap.add_argument("--sat-requests", type=int, default=120)
     ap.add_argument("--c4-wave", type=int, default=1 << 18, help="served mode: tasks per wave")
+    ap.add_argument("--c4-latency-cells", type=int, default=0,
+                    help="served mode: tasks above this many DP cells run one warp per extension")
     ap.add_argument("--c5-chains", type=int, default=1_000_000)
     ap.add_argument("--c3-jobs", type=int, default=1_000_000)
     ap.add_argument("--suite-only", default="",
@@ -169,6 +171,13 @@ def _cuda_time(torch, stream, fn, reps):
     e1.record(stream)
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / reps
+
+
+def _warm_server(S, srv, pb, pt, po, reqs):
+    """Runs the stream's largest requests once so that a fresh server's lanes
+    have grown their buffers before anything is timed."""
+    big = sorted(reqs, key=lambda r: r.hi - r.lo)[-4:]
+    S.run_pool_stream(srv, pb, pt, po, [S.Request(r.lo, r.hi, 0.0) for r in big], open_loop=False)
 
 
 def _pct(xs, q):
@@ -400,24 +409,29 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
         pt = torch.from_numpy(pool.tasks.view(np.uint8)).pin_memory().numpy().view(pool.tasks.dtype)
         po = torch.empty(len(pool.tasks) * EXT_RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy().view(EXT_RESULT_DTYPE)
         reqs = S.request_stream(W.SEED_BASE + 4 + 2, len(pool.tasks), rate=200.0, duration=args.serve_seconds)
-        srv = S.Server(eng, sc, arena_bytes=1 << 30, max_wave_tasks=args.c4_wave)
+        srv = S.Server(eng, sc, arena_bytes=1 << 30, max_wave_tasks=args.c4_wave, latency_cells=args.c4_latency_cells)
+        _warm_server(S, srv, pb, pt, po, reqs)
         res, span = S.run_pool_stream(srv, pb, pt, po, reqs, open_loop=True)
         st = srv.stats()
         srv.stop()
         lat = [l for _, l in res]
         mid = [l for n, l in res if 50_000 <= n <= 200_000]
+        near100k = [l for n, l in res if 70_000 <= n <= 140_000]
         c4 = {"requests": len(reqs), "tasks": int(sum(n for n, _ in res)), "offered_req_per_s": 200.0,
               "ext_per_s": sum(n for n, _ in res) / span, "p50_ms": _pct(lat, 50) * 1e3, "p99_ms": _pct(lat, 99) * 1e3,
               "p50_ms_50k_200k": _pct(mid, 50) * 1e3 if mid else None,
               "p99_ms_50k_200k": _pct(mid, 99) * 1e3 if mid else None, "n_50k_200k": len(mid),
-              "waves": st["waves"], "wave_tasks": args.c4_wave, "wave_device_ms_sum": st["busy_ms"], "span_s": span,
+              "p50_ms_70k_140k": _pct(near100k, 50) * 1e3 if near100k else None,
+              "p99_ms_70k_140k": _pct(near100k, 99) * 1e3 if near100k else None, "n_70k_140k": len(near100k),
+              "waves": st["waves"], "wave_tasks": args.c4_wave, "latency_cells": args.c4_latency_cells, "wave_device_ms_sum": st["busy_ms"], "span_s": span,
               "stream": "Poisson 200 req/s, sizes log-uniform 1k-1M tasks, qlen log-uniform 30-250, w 10-100, h0 19-60, "
                         "1 Gbp resident 2-bit reference"}
         # saturation: the same size distribution submitted at once, served vs plain
         sat = S.request_stream(W.SEED_BASE + 4 + 3, len(pool.tasks), rate=1e6, duration=args.sat_requests / 1e6)
         for mode, plain in (("served", 0), ("plain_batching", 1), ("plain_kernel", 2)):
             srv = S.Server(eng, sc, arena_bytes=1 << 30, max_wave_tasks=args.c4_wave if plain == 0 else 1 << 20,
-                           plain=plain)
+                           plain=plain, latency_cells=args.c4_latency_cells if plain == 0 else 0)
+            _warm_server(S, srv, pb, pt, po, sat)
             r_, span_ = S.run_pool_stream(srv, pb, pt, po, sat, open_loop=False)
             srv.stop()
             c4[f"saturation_{mode}_ext_per_s"] = sum(n for n, _ in r_) / span_

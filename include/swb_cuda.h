@@ -380,11 +380,15 @@ typedef struct swb_server swb_server;
 typedef struct swb_server_opts {
     size_t   arena_bytes;      /* device bytes for request bases (0 = 1 GiB)   */
     size_t   max_wave_tasks;   /* tasks per wave (0 = 1M)                      */
-    int32_t  plain;            /* 0 = served (waves, two lanes); 1 = one request
+    int32_t  plain;            /* 0 = served (waves, three lanes); 1 = one request
                                   at a time through the binned launch sequence;
                                   2 = one request at a time through the plain
                                   single-launch kernel (swb_ext_batch_static)  */
     int32_t  start_paused;     /* 1 = admit nothing until swb_server_resume    */
+    uint32_t latency_cells;    /* served mode: tasks with more DP cells than this
+                                  (qlen * tlen) run one warp per extension, so no
+                                  single long task holds a wave open; 0 = off  */
+    uint32_t reserved;
 } swb_server_opts;
 typedef struct swb_server_stats {
     uint64_t submitted, completed, tasks_completed, waves;

@@ -141,7 +141,7 @@ EXPORTED_SYMBOLS = (
 
 class ServerOpts(C.Structure):
     _fields_ = [("arena_bytes", C.c_size_t), ("max_wave_tasks", C.c_size_t), ("plain", C.c_int32),
-                ("start_paused", C.c_int32)]
+                ("start_paused", C.c_int32), ("latency_cells", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class ServerStats(C.Structure):

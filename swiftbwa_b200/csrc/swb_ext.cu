@@ -66,25 +66,28 @@ __device__ __forceinline__ bool fits8(int qlen, int h0, int max_mat) {
     return h0 >= 0 && (long long)h0 + (long long)qlen * (max_mat > 0 ? max_mat : 0) <= 255;
 }
 
-__device__ __forceinline__ int ext_bin(const swb_ext_task &t, int max_mat, bool u8_ok) {
+__device__ __forceinline__ int ext_bin(const swb_ext_task &t, int max_mat, bool u8_ok, uint32_t warp_cells) {
     if (t.qlen <= 0 || t.tlen <= 0) return 0;
     if (t.qlen > kExtSmemMaxQ || !fits16(t.qlen, t.h0, max_mat)) return kBigBin;
+    if (warp_cells && (unsigned long long)t.qlen * (unsigned long long)t.tlen > warp_cells) return kBigBin;
     int b = 0;
     while (t.qlen > kFastQDev[b]) ++b;
     return u8_ok && fits8(t.qlen, t.h0, max_mat) ? b : kLenClasses + b;
 }
 
-// Sort key: bin in bits 27-31, query length in 15-26, target length in 0-14.
+// Sort key: bin in bits 27-31, then query and target length, longest first.
 __global__ void ext_keys_kernel(const swb_ext_task *__restrict__ tasks, size_t n, int max_mat, int u8_ok,
-                                uint32_t *__restrict__ keys, uint32_t *__restrict__ idx,
+                                uint32_t warp_cells, uint32_t *__restrict__ keys, uint32_t *__restrict__ idx,
                                 int *__restrict__ big_max_q) {
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const swb_ext_task t = tasks[i];
-    const int b = ext_bin(t, max_mat, u8_ok != 0);
+    const int b = ext_bin(t, max_mat, u8_ok != 0, warp_cells);
     const uint32_t q = (uint32_t)min(max(t.qlen, 0), 4095);
     const uint32_t tl = (uint32_t)min(max(t.tlen, 0), 32767);
-    keys[i] = ((uint32_t)b << 27) | (q << 15) | tl;
+    // Within a bin the longest tasks come first: they are claimed first, so
+    // they overlap the rest instead of finishing the bin alone.
+    keys[i] = ((uint32_t)b << 27) | ((4095u - q) << 15) | (32767u - tl);
     idx[i] = (uint32_t)i;
     if (b == kBigBin) atomicMax(big_max_q, t.qlen);
 }
@@ -376,7 +379,7 @@ const FastLauncher kFastLaunch[kFastBins] = {
 
 int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
                const swb_ext_task *d_tasks, size_t n, swb_ext_result *d_out,
-               unsigned long long *d_cells, cudaStream_t s, int max_q_hint) {
+               unsigned long long *d_cells, cudaStream_t s, int max_q_hint, uint32_t warp_cells) {
     if (n == 0) return SWB_OK;
     if (n > 0x7FFFFFF0ull) return set_error(SWB_ERR_TOO_LARGE, "more than 2^31-16 tasks in one batch");
     int rc;
@@ -395,8 +398,8 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
         ProfScope ps(ctx, s, "ext_keys", -1);
         // int8 rows run two target rows per pass on 16-bit lanes: the gap costs must fit a lane.
         const int u8_ok = sc.o_del + sc.e_del <= 32767 && sc.o_ins + sc.e_ins <= 32767;
-        ext_keys_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(d_tasks, n, sc.max_mat, u8_ok, keys, idx,
-                                                                       big_max_q);
+        ext_keys_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(d_tasks, n, sc.max_mat, u8_ok, warp_cells, keys,
+                                                                       idx, big_max_q);
     }
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());

@@ -138,9 +138,12 @@ int ensure_host(swb_ctx *ctx, HostBuf &b, size_t bytes);
 // is a device counter (unsigned long long) the kernels add DP cells to.
 
 // Extension (kernel 1).  d_tasks/d_out are device arrays of n tasks/results.
+// warp_cells > 0: tasks with more DP cells (qlen * tlen) run one warp per
+// extension (latency), otherwise their length bin's thread-per-task kernel.
 int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
                const swb_ext_task *d_tasks, size_t n, swb_ext_result *d_out,
-               unsigned long long *d_cells, cudaStream_t stream, int max_q_hint);
+               unsigned long long *d_cells, cudaStream_t stream, int max_q_hint,
+               uint32_t warp_cells = 0);
 
 // Banded global + traceback (kernel 2).  Tasks with qlen <= kGlobalSmemMaxQ
 // run in the shared-memory kernel, longer ones in the global-scratch kernel;

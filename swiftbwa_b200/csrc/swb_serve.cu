@@ -163,6 +163,7 @@ struct swb_server {
     DevScoring dsc{};
     int plain = 0;
     size_t max_wave = 1u << 20;
+    uint32_t latency_cells = 0;
     uint8_t *d_arena = nullptr;
     Arena arena;
     Lane lanes[kLanes];
@@ -301,7 +302,7 @@ bool launch_wave(swb_server *s, Lane &L) {
             // wave's requests (an upper bound of the bin's), known since submit.
             int max_q = 0;
             for (const Piece &p : L.pieces) max_q = std::max(max_q, p.r->max_q);
-            rc = launch_ext(c, s->dsc, s->d_arena, d_tasks, wn, d_out, c->d_counters, st, max_q);
+            rc = launch_ext(c, s->dsc, s->d_arena, d_tasks, wn, d_out, c->d_counters, st, max_q, s->latency_cells);
         }
     }
     if (!rc) cudaEventRecord(L.ev_t1, st);
@@ -380,6 +381,7 @@ int swb_server_start(swb_ctx *ctx, const swb_scoring *sc, const swb_server_opts 
     s->plain = o.plain;
     s->paused = o.start_paused != 0;
     s->max_wave = o.max_wave_tasks ? o.max_wave_tasks : (1u << 20);
+    s->latency_cells = o.latency_cells;
     const size_t arena = o.arena_bytes ? o.arena_bytes : ((size_t)1 << 30);
     SWB_CUDA(cudaSetDevice(ctx->device));
     int rc = SWB_OK;

@@ -21,10 +21,10 @@ class Server:
     arrays alive until its ticket has been waited for."""
 
     def __init__(self, engine: Engine, scoring: Scoring, arena_bytes: int = 0, max_wave_tasks: int = 0,
-                 plain: int = 0, start_paused: bool = False):
+                 plain: int = 0, start_paused: bool = False, latency_cells: int = 0):
         self.lib = engine.lib
         self.engine = engine
-        opts = abi.ServerOpts(arena_bytes, max_wave_tasks, int(plain), int(start_paused))
+        opts = abi.ServerOpts(arena_bytes, max_wave_tasks, int(plain), int(start_paused), int(latency_cells), 0)
         h = C.c_void_p()
         _check(self.lib.swb_server_start(engine.h, C.byref(scoring), C.byref(opts), C.byref(h)), "swb_server_start")
         self.h = h
