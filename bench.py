@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--c4-ref-len", type=int, default=1_000_000_000)
     ap.add_argument("--c4-pool", type=int, default=3_000_000)
     ap.add_argument("--sat-requests", type=int, default=120)
-    ap.add_argument("--c4-wave", type=int, default=1 << 18, help="served mode: tasks per wave")
+    ap.add_argument("--c4-wave", type=int, default=1 << 17, help="served mode: tasks per wave")
     ap.add_argument("--c4-latency-cells", type=int, default=0,
                     help="served mode: tasks above this many DP cells run one warp per extension")
     ap.add_argument("--c5-chains", type=int, default=1_000_000)
