@@ -15,7 +15,9 @@ e2e      the same metric through the C ABI's host entry point
          the kernels, D2H of results, every step.
 roofline the dominant kernel's algorithmic int ops (13 per DP cell) per
          launch / its average launch time, against the measured int32
-         add/max rate of the same GPU (swb_int_alu_peak).
+         add/max rate of the same GPU (swb_int_alu_peak); roofline.int16x2
+         gives the same work against the packed 16-bit DPX add/max rate in
+         lane operations (swb_int16x2_alu_peak).
 For N > 1 the driver launches one process per GPU (torchrun); each rank
 extends its own shard (weak scaling, no data-path collective).
 """
@@ -518,6 +520,7 @@ def run_ours(args):
     eng = Engine(local)
     eng.upload_reference(wl.ref.pac, wl.ref.n)
     alu_peak = eng.int_alu_peak()
+    alu16_peak = eng.int16x2_alu_peak()
 
     # HBM-resident inputs (torch only allocates; the library computes).
     dev = torch.device("cuda", local)
@@ -622,7 +625,9 @@ def run_ours(args):
                          "frac": achieved / alu_peak, "traffic": traffic_per_launch("ext_pass"),
                          "ops_per_cell": OPS_PER_CELL_EXT,
                          "peak_source": "measured in this run: swb_int_alu_peak (int32 add/max probe); "
-                                        "MEASURED_PEAKS.json has no integer figure"},
+                                        "MEASURED_PEAKS.json has no integer figure",
+                         "int16x2": {"peak": alu16_peak / 1e12, "frac": achieved / alu16_peak,
+                                     "unit": "T 16-bit lane ops/s (s16x2 DPX add/max probe, swb_int16x2_alu_peak)"}},
             "kernels": kernels,
             "gpu_launches": int(launches),
             "clocks": clk,

@@ -451,6 +451,9 @@ int swb_profile_read(swb_ctx *ctx, swb_kernel_stat *stats, int cap, int *n_stats
 /* Measured int32 add+max issue rate of the context's GPU (ops/s): the
  * denominator of the kernels' integer-ALU roofline. */
 int swb_int_alu_peak(swb_ctx *ctx, double *ops_per_s);
+/* Measured packed-16-bit (s16x2 DPX add+max) rate of the context's GPU, in
+ * 16-bit lane operations/s: the int16 roofline of the two-row kernel. */
+int swb_int16x2_alu_peak(swb_ctx *ctx, double *lane_ops_per_s);
 
 /* Kernel launches issued by this context so far (for launch accounting). */
 uint64_t swb_kernel_launches(const swb_ctx *ctx);

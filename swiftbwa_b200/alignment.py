@@ -261,6 +261,12 @@ class Engine:
         _check(self.lib.swb_int_alu_peak(self.h, C.byref(v)), "swb_int_alu_peak")
         return v.value
 
+    def int16x2_alu_peak(self) -> float:
+        """Packed 16-bit (s16x2 DPX add+max) lane operations/s."""
+        v = C.c_double()
+        _check(self.lib.swb_int16x2_alu_peak(self.h, C.byref(v)), "swb_int16x2_alu_peak")
+        return v.value
+
     def ext_batch_device(self, sc: Scoring, d_bases: int, d_tasks: int, n: int, d_out: int, stream: int = 0):
         """swb_ext_batch_device on device pointers (HBM-resident inputs)."""
         _check(self.lib.swb_ext_batch_device(self.h, C.byref(sc), C.c_void_p(d_bases), C.c_void_p(d_tasks), n,

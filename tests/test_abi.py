@@ -66,6 +66,9 @@ def test_null_arguments_are_rejected_without_crash(lib):
     assert lib.swb_ext_batch(None, C.byref(sc), None, 0, None, 0, None) == abi.SWB_ERR_INVALID_ARG
     assert lib.swb_last_batch_stats(None, None, None) == abi.SWB_ERR_INVALID_ARG
     assert lib.swb_kernel_launches(None) == 0
+    v = C.c_double()
+    assert lib.swb_int_alu_peak(None, C.byref(v)) == abi.SWB_ERR_INVALID_ARG
+    assert lib.swb_int16x2_alu_peak(None, C.byref(v)) == abi.SWB_ERR_INVALID_ARG
     lib.swb_destroy(None)
 
 

@@ -188,3 +188,12 @@ def test_cigar_generate_fuzz(engine, oracle_mod, si):
         g = got[k]
         assert (g["cigar"], g["nm"], g["md"], g["score"], g["pos"], g["used_dp"]) == \
             (exp["cigar"], exp["nm"], exp["md"], exp["score"], exp["pos"], exp["used_dp"]), (k, g, exp)
+
+
+def test_alu_probes(engine):
+    """The roofline denominators: int32 add/max and packed 16-bit DPX add/max
+    rates are positive and of B200 magnitude (tens of T ops/s)."""
+    i32 = engine.int_alu_peak()
+    i16 = engine.int16x2_alu_peak()
+    assert 5e12 < i32 < 5e14
+    assert 5e12 < i16 < 5e14
