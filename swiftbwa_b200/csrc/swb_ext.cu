@@ -377,21 +377,42 @@ const FastLauncher kFastLaunch[kFastBins] = {
 
 }  // namespace
 
+int ext_reserve(swb_ctx *ctx, size_t cap) {
+    if (cap > 0x7FFFFFF0ull) return set_error(SWB_ERR_TOO_LARGE, "more than 2^31-16 tasks in one batch");
+    int rc;
+    size_t tmp_bytes = 0;
+    SWB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (uint32_t *)nullptr, (uint32_t *)nullptr,
+                                             (uint32_t *)nullptr, (uint32_t *)nullptr, (int)cap, 0, 32, ctx->stream));
+    if ((rc = ensure_dev(ctx, ctx->d_keys, cap * 4)) || (rc = ensure_dev(ctx, ctx->d_keys2, cap * 4)) ||
+        (rc = ensure_dev(ctx, ctx->d_idx, cap * 4)) || (rc = ensure_dev(ctx, ctx->d_idx2, 2 * cap * 4)) ||
+        (rc = ensure_dev(ctx, ctx->d_misc, 512)) || (rc = ensure_dev(ctx, ctx->d_sort_tmp, tmp_bytes)))
+        return rc;
+    return SWB_OK;
+}
+
 int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
                const swb_ext_task *d_tasks, size_t n, swb_ext_result *d_out,
-               unsigned long long *d_cells, cudaStream_t s, int max_q_hint, uint32_t warp_cells) {
+               unsigned long long *d_cells, cudaStream_t s, int max_q_hint, uint32_t warp_cells,
+               const ExtPipe *pipe) {
     if (n == 0) return SWB_OK;
     if (n > 0x7FFFFFF0ull) return set_error(SWB_ERR_TOO_LARGE, "more than 2^31-16 tasks in one batch");
+    if (pipe && n > pipe->cap) return set_error(SWB_ERR_INVALID_ARG, "pass larger than its scratch set");
     int rc;
+    // keys, keys2, idx and the sort's temporary storage are used by the
+    // launching stream only; the sorted order (idx2) and the bin bounds and
+    // claim counters (misc) are read by the bins, one set per pipelined slot.
+    const size_t set = pipe ? pipe->cap : n;
+    const int slot = pipe ? pipe->slot : 0;
     if ((rc = ensure_dev(ctx, ctx->d_keys, n * 4)) || (rc = ensure_dev(ctx, ctx->d_keys2, n * 4)) ||
-        (rc = ensure_dev(ctx, ctx->d_idx, n * 4)) || (rc = ensure_dev(ctx, ctx->d_idx2, n * 4)) ||
-        (rc = ensure_dev(ctx, ctx->d_misc, 256)))
+        (rc = ensure_dev(ctx, ctx->d_idx, n * 4)) || (rc = ensure_dev(ctx, ctx->d_idx2, (slot + 1) * set * 4)) ||
+        (rc = ensure_dev(ctx, ctx->d_misc, (slot + 1) * 256)))
         return rc;
     uint32_t *keys = (uint32_t *)ctx->d_keys.p, *keys2 = (uint32_t *)ctx->d_keys2.p;
-    uint32_t *idx = (uint32_t *)ctx->d_idx.p, *idx2 = (uint32_t *)ctx->d_idx2.p;
-    uint32_t *bin_start = (uint32_t *)ctx->d_misc.p;          // kNumBins+1 words
-    int *big_max_q = (int *)((char *)ctx->d_misc.p + 128);
-    uint32_t *claim = (uint32_t *)((char *)ctx->d_misc.p + 160);   // kNumBins claim counters
+    uint32_t *idx = (uint32_t *)ctx->d_idx.p, *idx2 = (uint32_t *)ctx->d_idx2.p + (size_t)slot * set;
+    char *misc = (char *)ctx->d_misc.p + slot * 256;
+    uint32_t *bin_start = (uint32_t *)misc;                   // kNumBins+1 words
+    int *big_max_q = (int *)(misc + 128);
+    uint32_t *claim = (uint32_t *)(misc + 160);               // kNumBins claim counters
     SWB_CUDA(cudaMemsetAsync(big_max_q, 0, 128, s));                  // big_max_q and the counters
     const unsigned tb = 256;
     {
@@ -444,9 +465,11 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
         wblocks = imax(wblocks, 1) * ctx->sm_count;
     }
 
-    // Fork: every bin runs on its own stream after the sort, then joins back.
+    // Fork: every bin runs on its own stream after the sort, then joins back
+    // (into the pipeline's join stream for pipelined passes).
     ExtArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_out, idx2, bin_start, d_cells, claim};
-    ProfScope pass(ctx, s, "ext_pass", -1);   // fork to join, on the launching stream
+    const cudaStream_t js = pipe ? pipe->join : s;
+    ProfScope pass(ctx, s, pipe ? nullptr : "ext_pass", -1);   // fork to join, on the launching stream
     SWB_CUDA(cudaEventRecord(ctx->fork_ev, s));
     for (int b = 0; b < kNumBins; ++b) {
         cudaStream_t sb = ctx->side[b];
@@ -468,7 +491,7 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
             }
         }
         SWB_CUDA(cudaEventRecord(ctx->join_ev[b], sb));
-        SWB_CUDA(cudaStreamWaitEvent(s, ctx->join_ev[b], 0));
+        SWB_CUDA(cudaStreamWaitEvent(js, ctx->join_ev[b], 0));
     }
     return SWB_OK;
 }

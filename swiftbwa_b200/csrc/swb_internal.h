@@ -140,10 +140,20 @@ int ensure_host(swb_ctx *ctx, HostBuf &b, size_t bytes);
 // Extension (kernel 1).  d_tasks/d_out are device arrays of n tasks/results.
 // warp_cells > 0: tasks with more DP cells (qlen * tlen) run one warp per
 // extension (latency), otherwise their length bin's thread-per-task kernel.
+// Pipelined passes: two scratch sets let pass k+1 sort and start its bins
+// while pass k's bins finish.  The caller sizes the scratch with
+// ext_reserve(cap) first and makes `stream` wait for pass k-2 to finish
+// before pass k reuses its set; the bins join into `join` instead of `stream`.
+struct ExtPipe {
+    int slot;            // scratch set 0 or 1
+    size_t cap;          // tasks per scratch set (every pass has n <= cap)
+    cudaStream_t join;   // stream that waits for the bins
+};
+int ext_reserve(swb_ctx *ctx, size_t cap);
 int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
                const swb_ext_task *d_tasks, size_t n, swb_ext_result *d_out,
                unsigned long long *d_cells, cudaStream_t stream, int max_q_hint,
-               uint32_t warp_cells = 0);
+               uint32_t warp_cells = 0, const ExtPipe *pipe = nullptr);
 
 // Banded global + traceback (kernel 2).  Tasks with qlen <= kGlobalSmemMaxQ
 // run in the shared-memory kernel, longer ones in the global-scratch kernel;

@@ -230,7 +230,7 @@ static cudaEvent_t pooled_event(swb_ctx *ctx) {
 }
 
 ProfScope::ProfScope(swb_ctx *c, cudaStream_t st, const char *name, int counter) : ctx(c), s(st) {
-    if (!ctx->prof_on) return;
+    if (!ctx->prof_on || !name) return;
     cudaEvent_t a = pooled_event(ctx), b = pooled_event(ctx);
     if (!a || !b) return;
     ctx->prof.push_back(swb_ctx::ProfRec{name, counter, a, b});
@@ -439,12 +439,16 @@ int swb_ext_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, siz
     uint8_t *d_b = (uint8_t *)ctx->d_bases.p;
     swb_ext_task *d_t = (swb_ext_task *)((char *)ctx->d_bases.p + bases_bytes);
     swb_ext_result *d_o = (swb_ext_result *)ctx->d_out.p;
+    // Sort and bin scratch for two chunks in flight, sized before the first
+    // launch (growing a buffer synchronizes).
+    if ((rc = ext_reserve(ctx, per))) return rc;
     Timer tm{ctx, nullptr};
     if ((rc = tm.begin())) return rc;
     // Copies must not overtake work still using these buffers.
     SWB_CUDA(cudaEventRecord(ctx->fork_ev, ctx->stream));
     SWB_CUDA(cudaStreamWaitEvent(ctx->h2d, ctx->fork_ev, 0));
-    size_t copied = 0, need = 0;
+    SWB_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->fork_ev, 0));
+    size_t copied = 0, need = 0, last = 0;
     for (size_t k = 0; k < nchunks; ++k) {
         const size_t lo = k * per, hi = std::min(n_tasks, lo + per);
         if (lo >= hi) break;
@@ -462,11 +466,21 @@ int swb_ext_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, siz
         SWB_CUDA(cudaMemcpyAsync(d_t + lo, tasks + lo, (hi - lo) * sizeof(swb_ext_task), cudaMemcpyHostToDevice, ctx->h2d));
         SWB_CUDA(cudaEventRecord(ctx->chunk_in[k], ctx->h2d));
         SWB_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->chunk_in[k], 0));
-        if ((rc = launch_ext(ctx, dsc, d_b, d_t + lo, hi - lo, d_o + lo, tm.d_cells, ctx->stream, big_q))) return rc;
-        SWB_CUDA(cudaEventRecord(ctx->chunk_done[k], ctx->stream));
-        SWB_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->chunk_done[k], 0));
+        // Chunk k reuses chunk k-2's scratch set: its bins must be done.  Chunk
+        // k-1's bins may still run while chunk k sorts and starts its own.
+        if (k >= 2) SWB_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->chunk_done[k - 2], 0));
+        const ExtPipe pipe{(int)(k & 1), per, ctx->d2h};
+        if ((rc = launch_ext(ctx, dsc, d_b, d_t + lo, hi - lo, d_o + lo, tm.d_cells, ctx->stream, big_q, 0, &pipe))) {
+            cudaStreamSynchronize(ctx->d2h);
+            cudaStreamSynchronize(ctx->stream);
+            return rc;
+        }
+        // The D2H stream has waited for every bin of chunk k.
+        SWB_CUDA(cudaEventRecord(ctx->chunk_done[k], ctx->d2h));
         SWB_CUDA(cudaMemcpyAsync(out + lo, d_o + lo, (hi - lo) * sizeof(swb_ext_result), cudaMemcpyDeviceToHost, ctx->d2h));
+        last = k;
     }
+    SWB_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->chunk_done[last], 0));
     if ((rc = tm.end())) return rc;
     SWB_CUDA(cudaStreamSynchronize(ctx->d2h));
     SWB_CUDA(cudaStreamSynchronize(ctx->stream));
