@@ -321,22 +321,29 @@ __device__ int global_dp_smem(const DevScoring &sc, const Row &row, const uint8_
 
 // Sort key: shared-memory tasks first, then by query length, target length
 // and band, so the threads of a warp align tasks of the same shape.
-__global__ void global_keys_kernel(const swb_global_task *__restrict__ tasks, size_t n, uint32_t *__restrict__ keys,
-                                   uint32_t *__restrict__ idx) {
+// Sort key: the shared-memory kernels' int16-row alignments first, then
+// their int32-row ones, then the long queries; within a class the largest
+// shapes first (they are claimed first and overlap the rest), and equal
+// shapes together so a warp's 32 alignments walk similar matrices.
+__global__ void global_keys_kernel(const swb_global_task *__restrict__ tasks, size_t n, DevScoring sc,
+                                   uint32_t *__restrict__ keys, uint32_t *__restrict__ idx) {
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const swb_global_task t = tasks[i];
     const uint32_t big = t.qlen > kGlbSmemMaxQ ? 1u : 0u;
-    keys[i] = (big << 31) | ((uint32_t)min(max(t.qlen, 0), 2047) << 20) | ((uint32_t)min(max(t.tlen, 0), 4095) << 8) |
-              (uint32_t)min(max(t.w, 0), 255);
+    const uint32_t wide = !big && !fits_i16(sc, t.qlen, t.tlen) ? 1u : 0u;
+    keys[i] = (big << 31) | (wide << 30) | ((2047u - (uint32_t)min(max(t.qlen, 0), 2047)) << 19) |
+              ((4095u - (uint32_t)min(max(t.tlen, 0), 4095)) << 7) | (127u - (uint32_t)min(max(t.w, 0), 127));
     idx[i] = (uint32_t)i;
 }
 
-// Tasks order[0 .. n_small) (all with qlen <= qcap) in sorted order; the
-// int16 instance takes those fits_i16() accepts, the int32 one the rest.
+// Sorted tasks order[begin, begin + count) of one row width (all with
+// qlen <= qcap).  Each warp claims the next 32 from `claim`, so warps that
+// draw large matrices never hold the launch up.
 template <bool I16>
 __global__ void __launch_bounds__(256) global_smem_kernel(GlobalArgs a, const uint32_t *__restrict__ order,
-                                                          size_t n_small, uint32_t *z, size_t nslots, int qcap) {
+                                                          size_t begin, uint32_t count, uint32_t *claim,
+                                                          uint32_t *z, size_t nslots, int qcap) {
     extern __shared__ int2 smem[];
     const int T = blockDim.x;
     const size_t row_bytes = (size_t)(qcap + 1) * T * (I16 ? 4 : 8);
@@ -347,12 +354,17 @@ __global__ void __launch_bounds__(256) global_smem_kernel(GlobalArgs a, const ui
     else row.he = smem + threadIdx.x;
     uint8_t *qs = reinterpret_cast<uint8_t *>(smem) + row_bytes + threadIdx.x;
     const size_t slot = blockIdx.x * (size_t)T + threadIdx.x;
+    const int lane = threadIdx.x & 31;
     unsigned long long cells = 0;
-    for (size_t p = slot; p < n_small; p += nslots) {
-        const size_t k = order[p];
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(claim, 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= count) break;
+        if (base + (uint32_t)lane >= count) continue;
+        const size_t k = order[begin + base + lane];
         const swb_global_task tk = a.tasks[k];
-        if (tk.qlen > qcap) continue;                                    // the global-scratch kernel's
-        if (fits_i16(a.sc, tk.qlen, tk.tlen) != I16) continue;            // the other instance's
+        if (tk.qlen > qcap) continue;                                    // (never: sorted by class)
         swb_global_result r{0, 0, tk.w, 1, a.cigar_off[k]};
         const int qlen = tk.qlen, tlen = tk.tlen;
         if (qlen > 0 && tlen > 0) {                                      // :29-31
@@ -417,7 +429,7 @@ int launch_global(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     if ((rc = ensure_dev(ctx, ctx->d_idx, n * 4)) || (rc = ensure_dev(ctx, ctx->d_idx2, n * 4))) return rc;
     uint32_t *skeys = (uint32_t *)ctx->d_keys.p, *skeys2 = skeys + n;
     uint32_t *sidx = (uint32_t *)ctx->d_idx.p, *order = (uint32_t *)ctx->d_idx2.p;
-    global_keys_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_tasks, n, skeys, sidx);
+    global_keys_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_tasks, n, sc, skeys, sidx);
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
     SWB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, skeys, skeys2, sidx, order, (int)n, 0, 32, st));
@@ -488,16 +500,20 @@ int launch_global(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
         s.tmax = tmax;
     }
     if ((rc = ensure_dev(ctx, ctx->d_scratch, z_bytes + big_bytes + 256))) return rc;
+    uint32_t *claim = (uint32_t *)((char *)ctx->d_scratch.p + z_bytes + big_bytes);   // one counter per row width
+    SWB_CUDA(cudaMemsetAsync(claim, 0, 2 * sizeof(uint32_t), st));
     ProfScope ps(ctx, st, "global_nw_traceback", kCntGlobal);
-    for (int v = 1; v >= 0; --v) {   // both instances walk the sorted small tasks, each taking its own
+    // The sorted order holds the int16-row alignments, then the int32-row ones.
+    const size_t begin_of[2] = {shape.n_small16, 0};
+    for (int v = 1; v >= 0; --v) {
         if (n_small_of[v] == 0) continue;
         const SmemCfg &c = cfg[v];
         if (v)
-            global_smem_kernel<true><<<(unsigned)c.grid, c.T, c.smem, st>>>(a, order, shape.n_small,
-                                                                            (uint32_t *)ctx->d_scratch.p, c.nslots, qcap);
+            global_smem_kernel<true><<<(unsigned)c.grid, c.T, c.smem, st>>>(
+                a, order, begin_of[v], (uint32_t)n_small_of[v], claim + v, (uint32_t *)ctx->d_scratch.p, c.nslots, qcap);
         else
-            global_smem_kernel<false><<<(unsigned)c.grid, c.T, c.smem, st>>>(a, order, shape.n_small,
-                                                                             (uint32_t *)ctx->d_scratch.p, c.nslots, qcap);
+            global_smem_kernel<false><<<(unsigned)c.grid, c.T, c.smem, st>>>(
+                a, order, begin_of[v], (uint32_t)n_small_of[v], claim + v, (uint32_t *)ctx->d_scratch.p, c.nslots, qcap);
         ctx->launches++;
         SWB_CUDA(cudaGetLastError());
     }
