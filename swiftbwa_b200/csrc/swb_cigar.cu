@@ -197,76 +197,93 @@ extern "C" int swb_cigar_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_
     if ((rc = validate_scoring(sc))) return rc;
     if (n_tasks == 0) return SWB_OK;
     if (n_tasks > 0x7FFFFFF0ull) return set_error(SWB_ERR_TOO_LARGE, "more than 2^31-16 tasks in one batch");
-    // Validation, the capacity rule and the fast-path decision (:44-80), in parallel.
+    // One pass per host thread over a contiguous range: validation, the
+    // capacity rule, the fast-path decision (:44-80) and, for the tasks that
+    // need DP, the inferred band (:82-96), the band rule and the DP shapes.
+    const size_t nth = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()),
+                                        std::max<size_t>(1, n_tasks / 4096));
+    struct Range {
+        size_t lo = 0, hi = 0, nd = 0, dp0 = 0, raw = 0;
+        int code = 0;
+        std::string msg;
+        size_t band_bad = SIZE_MAX;   // first task breaking the band rule
+        unsigned long long cc = 0, cm = 0;
+        GlobalShape shape;
+    };
+    std::vector<Range> rg(nth);
     std::vector<uint8_t> fast(n_tasks, 0);
-    std::vector<int> bad_code(std::max(1u, std::thread::hardware_concurrency()), 0);
-    std::vector<std::string> bad_msg(bad_code.size());
-    std::vector<unsigned long long> cap_c(bad_code.size(), 0), cap_m(bad_code.size(), 0);
     const int32_t min_indel = sc->o_ins + sc->e_ins + sc->o_del + sc->e_del;
     const bool have_ref = ctx->d_pac != nullptr;
-    {
-        const size_t nth = bad_code.size();
-        const size_t per = (n_tasks + nth - 1) / nth;
+    const int cost16 = nw_i16_cost(sc->a, sc->b, sc->o_del, sc->e_del, sc->o_ins, sc->e_ins);
+    auto band_of = [&](const swb_cigar_task &t) {
+        return std::max(infer_band_width(t.qe - t.qb, t.rlen, t.true_score, *sc), t.initial_w);
+    };
+    auto parallel = [&](auto &&fn) {
+        if (nth == 1) return fn((size_t)0);
         std::vector<std::thread> th;
-        for (size_t w = 0; w < nth; ++w)
-            th.emplace_back([&, w] {
-                const size_t lo = std::min(n_tasks, w * per), hi = std::min(n_tasks, lo + per);
-                unsigned long long cc = 0, cm = 0;
-                for (size_t i = lo; i < hi; ++i) {
-                    const swb_cigar_task &t = tasks[i];
-                    const char *why = nullptr;
-                    int code = SWB_ERR_INVALID_ARG;
-                    if (t.qlen < 0 || t.rlen < 0) why = "negative length";
-                    else if (t.qlen > kMaxLen || t.rlen > kMaxLen) why = "length above 65535", code = SWB_ERR_TOO_LARGE;
-                    else if (t.qlen > 0 && t.q_off + (uint64_t)t.qlen > n_bases) why = "query span outside bases";
-                    else if (t.rlen > 0 && (t.flags & SWB_T_FROM_REF) && !have_ref)
-                        why = "task reads the reference but none is uploaded", code = SWB_ERR_NO_REFERENCE;
-                    else if (t.rlen > 0 && (t.flags & SWB_T_FROM_REF) && t.t_off + (uint64_t)t.rlen > ctx->ref_bases)
-                        why = "reference span outside reference";
-                    else if (t.rlen > 0 && !(t.flags & SWB_T_FROM_REF) && t.t_off + (uint64_t)t.rlen > n_bases)
-                        why = "reference span outside bases";
-                    if (why) {
-                        bad_code[w] = code;
-                        bad_msg[w] = "task " + std::to_string(i) + ": " + why;
-                        return;
-                    }
-                    cc += (unsigned long long)t.qlen + (unsigned long long)t.rlen + 2;
-                    cm += 6ull * ((unsigned long long)t.qlen + (unsigned long long)t.rlen) + 8;
-                    const int32_t deficit = t.qlen * sc->a - t.true_score;
-                    fast[i] = t.qlen == t.rlen && t.qlen > 0 && deficit < min_indel;
-                }
-                cap_c[w] = cc;
-                cap_m[w] = cm;
-            });
+        for (size_t w = 0; w < nth; ++w) th.emplace_back(fn, w);
         for (auto &x : th) x.join();
+    };
+    {
+        const size_t per = (n_tasks + nth - 1) / nth;
+        parallel([&](size_t w) {
+            Range &r = rg[w];
+            r.lo = std::min(n_tasks, w * per);
+            r.hi = std::min(n_tasks, r.lo + per);
+            for (size_t i = r.lo; i < r.hi; ++i) {
+                const swb_cigar_task &t = tasks[i];
+                const char *why = nullptr;
+                int code = SWB_ERR_INVALID_ARG;
+                if (t.qlen < 0 || t.rlen < 0) why = "negative length";
+                else if (t.qlen > kMaxLen || t.rlen > kMaxLen) why = "length above 65535", code = SWB_ERR_TOO_LARGE;
+                else if (t.qlen > 0 && t.q_off + (uint64_t)t.qlen > n_bases) why = "query span outside bases";
+                else if (t.rlen > 0 && (t.flags & SWB_T_FROM_REF) && !have_ref)
+                    why = "task reads the reference but none is uploaded", code = SWB_ERR_NO_REFERENCE;
+                else if (t.rlen > 0 && (t.flags & SWB_T_FROM_REF) && t.t_off + (uint64_t)t.rlen > ctx->ref_bases)
+                    why = "reference span outside reference";
+                else if (t.rlen > 0 && !(t.flags & SWB_T_FROM_REF) && t.t_off + (uint64_t)t.rlen > n_bases)
+                    why = "reference span outside bases";
+                if (why) {
+                    r.code = code;
+                    r.msg = "task " + std::to_string(i) + ": " + why;
+                    return;
+                }
+                r.cc += (unsigned long long)t.qlen + (unsigned long long)t.rlen + 2;
+                r.cm += 6ull * ((unsigned long long)t.qlen + (unsigned long long)t.rlen) + 8;
+                const int32_t deficit = t.qlen * sc->a - t.true_score;
+                fast[i] = t.qlen == t.rlen && t.qlen > 0 && deficit < min_indel;
+                if (fast[i]) continue;
+                if (r.band_bad == SIZE_MAX && t.qlen > 0 && t.rlen > 0 && std::max(band_of(t), std::abs(t.qlen - t.rlen)) < 1)
+                    r.band_bad = i;
+                ++r.nd;
+                r.raw += (size_t)t.qlen + (size_t)t.rlen;
+                r.shape.add(t.qlen, t.rlen, cost16);
+            }
+        });
     }
     unsigned long long need_c = 0, need_m = 0;
-    for (size_t w = 0; w < bad_code.size(); ++w) {
-        if (bad_code[w]) return set_error(bad_code[w], bad_msg[w]);
-        need_c += cap_c[w];
-        need_m += cap_m[w];
+    for (const Range &r : rg) {
+        if (r.code) return set_error(r.code, r.msg);
+        need_c += r.cc;
+        need_m += r.cm;
     }
     if (need_c > cigar_cap) return set_error(SWB_ERR_INVALID_ARG, "cigar_cap below sum of (qlen + rlen + 2)");
     if (need_m > md_cap) return set_error(SWB_ERR_INVALID_ARG, "md_cap below sum of (6*(qlen+rlen)+8)");
-    // Global tasks for the rest, with the inferred band (:82-96).
-    std::vector<swb_global_task> dp;
-    std::vector<int32_t> dp_index(n_tasks, -1);
+    size_t nd = 0, raw_words = 0;
     GlobalShape shape;
-    const int cost16 = nw_i16_cost(sc->a, sc->b, sc->o_del, sc->e_del, sc->o_ins, sc->e_ins);
-    size_t raw_words = 0;
-    for (size_t i = 0; i < n_tasks; ++i) {
-        if (fast[i]) continue;
-        const swb_cigar_task &t = tasks[i];
-        const int32_t w = std::max(infer_band_width(t.qe - t.qb, t.rlen, t.true_score, *sc), t.initial_w);
-        if (t.qlen > 0 && t.rlen > 0 && std::max(w, std::abs(t.qlen - t.rlen)) < 1)
-            return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(i) + ": band width below 1 with equal lengths");
-        dp_index[i] = (int32_t)dp.size();
-        dp.push_back(swb_global_task{t.q_off, t.t_off, t.qlen, t.rlen, w, t.true_score,
-                                     (t.flags & (SWB_Q_REVERSE | SWB_T_REVERSE | SWB_T_COMPLEMENT | SWB_T_FROM_REF)) |
-                                         SWB_GLB_RETRY,
-                                     0});
-        shape.add(t.qlen, t.rlen, cost16);
-        raw_words += (size_t)t.qlen + (size_t)t.rlen;
+    for (Range &r : rg) {
+        if (r.band_bad != SIZE_MAX)
+            return set_error(SWB_ERR_INVALID_ARG, "task " + std::to_string(r.band_bad) + ": band width below 1 with equal lengths");
+        r.dp0 = nd;
+        nd += r.nd;
+        raw_words += r.raw;
+        shape.n_small += r.shape.n_small;
+        shape.n_small16 += r.shape.n_small16;
+        shape.n_big += r.shape.n_big;
+        shape.small_q = std::max(shape.small_q, r.shape.small_q);
+        shape.small_t = std::max(shape.small_t, r.shape.small_t);
+        shape.big_q = std::max(shape.big_q, r.shape.big_q);
+        shape.big_t = std::max(shape.big_t, r.shape.big_t);
     }
 
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -274,7 +291,7 @@ extern "C" int swb_cigar_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_
     ctx->last_cells = 0;
     SWB_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
-    const size_t n = n_tasks, nd = dp.size();
+    const size_t n = n_tasks;
     size_t off = 0;
     auto carve = [&](size_t bytes) {
         const size_t o = off;
@@ -287,18 +304,45 @@ extern "C" int swb_cigar_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_
     const size_t o_res = carve(n * sizeof(swb_cigar_result));
     const size_t o_cl = carve(n * 8), o_ml = carve(n * 8), o_co = carve(n * 8), o_mo = carve(n * 8);
     if ((rc = ensure_dev(ctx, ctx->d_chain, off)) ||
-        (rc = ensure_dev(ctx, ctx->d_cigar, std::max<size_t>(raw_words, 1) * sizeof(uint32_t))))
+        (rc = ensure_dev(ctx, ctx->d_cigar, std::max<size_t>(raw_words, 1) * sizeof(uint32_t))) ||
+        (rc = ensure_host(ctx, ctx->h_in, o_gres)))
         return rc;
     char *base = (char *)ctx->d_chain.p;
     unsigned long long *d_cl = (unsigned long long *)(base + o_cl), *d_ml = (unsigned long long *)(base + o_ml);
     unsigned long long *d_co = (unsigned long long *)(base + o_co), *d_mo = (unsigned long long *)(base + o_mo);
+    // Inputs staged in pinned memory in the device layout (bases, tasks, DP
+    // index, DP tasks) by the host threads, then one copy.
+    char *stage = (char *)ctx->h_in.p;
+    {
+        const size_t bper = (n_bases + nth - 1) / nth;
+        parallel([&](size_t w) {
+            const Range &r = rg[w];
+            const size_t b0 = std::min(n_bases, w * bper), b1 = std::min(n_bases, b0 + bper);
+            if (b1 > b0) std::memcpy(stage + o_bases + b0, bases + b0, b1 - b0);
+            if (r.hi > r.lo)
+                std::memcpy(stage + o_tasks + r.lo * sizeof(swb_cigar_task), tasks + r.lo,
+                            (r.hi - r.lo) * sizeof(swb_cigar_task));
+            int32_t *dpi = (int32_t *)(stage + o_dpi);
+            swb_global_task *dp = (swb_global_task *)(stage + o_dp);
+            size_t k = r.dp0;
+            for (size_t i = r.lo; i < r.hi; ++i) {
+                if (fast[i]) {
+                    dpi[i] = -1;
+                    continue;
+                }
+                const swb_cigar_task &t = tasks[i];
+                dpi[i] = (int32_t)k;
+                dp[k++] = swb_global_task{t.q_off, t.t_off, t.qlen, t.rlen, band_of(t), t.true_score,
+                                          (t.flags & (SWB_Q_REVERSE | SWB_T_REVERSE | SWB_T_COMPLEMENT | SWB_T_FROM_REF)) |
+                                              SWB_GLB_RETRY,
+                                          0};
+            }
+        });
+    }
     SWB_CUDA(cudaMemsetAsync(ctx->d_counters, 0, sizeof(unsigned long long) * kNumCounters, st));
     SWB_CUDA(cudaEventRecord(ctx->ev_start, st));
-    if (n_bases) SWB_CUDA(cudaMemcpyAsync(base + o_bases, bases, n_bases, cudaMemcpyHostToDevice, st));
-    SWB_CUDA(cudaMemcpyAsync(base + o_tasks, tasks, n * sizeof(swb_cigar_task), cudaMemcpyHostToDevice, st));
-    SWB_CUDA(cudaMemcpyAsync(base + o_dpi, dp_index.data(), n * 4, cudaMemcpyHostToDevice, st));
+    SWB_CUDA(cudaMemcpyAsync(base, stage, o_dp + nd * sizeof(swb_global_task), cudaMemcpyHostToDevice, st));
     if (nd) {
-        SWB_CUDA(cudaMemcpyAsync(base + o_dp, dp.data(), nd * sizeof(swb_global_task), cudaMemcpyHostToDevice, st));
         if ((rc = launch_global(ctx, make_dev_scoring(*sc), (const uint8_t *)(base + o_bases),
                                 (const swb_global_task *)(base + o_dp), nd, (swb_global_result *)(base + o_gres),
                                 (uint32_t *)ctx->d_cigar.p, ctx->d_counters, st, shape)))
@@ -343,11 +387,24 @@ extern "C" int swb_cigar_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_
         ctx->launches++;
         SWB_CUDA(cudaGetLastError());
     }
-    SWB_CUDA(cudaMemcpyAsync(results, base + o_res, n * sizeof(swb_cigar_result), cudaMemcpyDeviceToHost, st));
-    if (tot_c) SWB_CUDA(cudaMemcpyAsync(cigar_out, d_cig, tot_c * 4, cudaMemcpyDeviceToHost, st));
-    if (tot_m) SWB_CUDA(cudaMemcpyAsync(md_out, d_md, tot_m, cudaMemcpyDeviceToHost, st));
+    // Results, CIGAR words and MD bytes back through pinned memory.
+    const size_t r_bytes = n * sizeof(swb_cigar_result), c_bytes = tot_c * 4;
+    if ((rc = ensure_host(ctx, ctx->h_out, al256(r_bytes) + al256(c_bytes) + al256(tot_m)))) return rc;
+    char *back = (char *)ctx->h_out.p;
+    SWB_CUDA(cudaMemcpyAsync(back, base + o_res, r_bytes, cudaMemcpyDeviceToHost, st));
+    if (tot_c) SWB_CUDA(cudaMemcpyAsync(back + al256(r_bytes), d_cig, c_bytes, cudaMemcpyDeviceToHost, st));
+    if (tot_m) SWB_CUDA(cudaMemcpyAsync(back + al256(r_bytes) + al256(c_bytes), d_md, tot_m, cudaMemcpyDeviceToHost, st));
     SWB_CUDA(cudaEventRecord(ctx->ev_stop, st));
     SWB_CUDA(cudaStreamSynchronize(st));
+    parallel([&](size_t w) {
+        auto part = [&](void *dst, const char *src, size_t bytes) {
+            const size_t per = (bytes + nth - 1) / nth, a0 = std::min(bytes, w * per), a1 = std::min(bytes, a0 + per);
+            if (a1 > a0) std::memcpy((char *)dst + a0, src + a0, a1 - a0);
+        };
+        part(results, back, r_bytes);
+        part(cigar_out, back + al256(r_bytes), c_bytes);
+        part(md_out, back + al256(r_bytes) + al256(c_bytes), tot_m);
+    });
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) ctx->last_ms = ms;
     unsigned long long c[kNumCounters] = {0};
