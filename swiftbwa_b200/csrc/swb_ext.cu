@@ -66,23 +66,25 @@ __device__ __forceinline__ bool fits8(int qlen, int h0, int max_mat) {
     return h0 >= 0 && (long long)h0 + (long long)qlen * (max_mat > 0 ? max_mat : 0) <= 255;
 }
 
-__device__ __forceinline__ int ext_bin(const swb_ext_task &t, int max_mat, bool u8_ok, uint32_t warp_cells) {
+// pair_ok: the gap costs fit a 16-bit lane (the two-row kernels of both row
+// widths); otherwise every task takes the int32 bin.
+__device__ __forceinline__ int ext_bin(const swb_ext_task &t, int max_mat, bool pair_ok, uint32_t warp_cells) {
     if (t.qlen <= 0 || t.tlen <= 0) return 0;
-    if (t.qlen > kExtSmemMaxQ || !fits16(t.qlen, t.h0, max_mat)) return kBigBin;
+    if (!pair_ok || t.qlen > kExtSmemMaxQ || !fits16(t.qlen, t.h0, max_mat)) return kBigBin;
     if (warp_cells && (unsigned long long)t.qlen * (unsigned long long)t.tlen > warp_cells) return kBigBin;
     int b = 0;
     while (t.qlen > kFastQDev[b]) ++b;
-    return u8_ok && fits8(t.qlen, t.h0, max_mat) ? b : kLenClasses + b;
+    return fits8(t.qlen, t.h0, max_mat) ? b : kLenClasses + b;
 }
 
 // Sort key: bin in bits 27-31, then query and target length, longest first.
-__global__ void ext_keys_kernel(const swb_ext_task *__restrict__ tasks, size_t n, int max_mat, int u8_ok,
+__global__ void ext_keys_kernel(const swb_ext_task *__restrict__ tasks, size_t n, int max_mat, int pair_ok,
                                 uint32_t warp_cells, uint32_t *__restrict__ keys, uint32_t *__restrict__ idx,
                                 int *__restrict__ big_max_q) {
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const swb_ext_task t = tasks[i];
-    const int b = ext_bin(t, max_mat, u8_ok != 0, warp_cells);
+    const int b = ext_bin(t, max_mat, pair_ok != 0, warp_cells);
     const uint32_t q = (uint32_t)min(max(t.qlen, 0), 4095);
     const uint32_t tl = (uint32_t)min(max(t.tlen, 0), 32767);
     // Within a bin the longest tasks come first: they are claimed first, so
@@ -108,151 +110,13 @@ __global__ void bin_bounds_kernel(const uint32_t *__restrict__ sorted_keys, size
         for (int bb = b + 1; bb <= nbins; ++bb) bin_start[bb] = (uint32_t)n;
 }
 
-// One extension over the shared-memory row of this thread.
-//   U8 = false: he[j*T] = H | E << 16, qs[j*T] = the column's prmt selector.
-//   U8 = true : he[j*T] = selector | H << 16 | E << 24 (scores <= 255); qs unused.
-template <int T, bool U8>
-__device__ __forceinline__ void ext_fast_one(const ExtArgs &a, const swb_ext_task &tk, uint32_t *__restrict__ he,
-                                             uint16_t *__restrict__ qs, swb_ext_result &res,
-                                             unsigned long long &cells) {
-    res = swb_ext_result{0, 0, 0, 0, 0, 0};
-    const int qlen = tk.qlen, tlen = tk.tlen;
-    if (!(qlen > 0 && tlen > 0)) return;                                   // :33-35
-    const DevScoring &sc = a.sc;
-    const int oDel = sc.o_del, eDel = sc.e_del, oIns = sc.o_ins, eIns = sc.e_ins;
-    const int oeDel = oDel + eDel, oeIns = oIns + eIns;
-    const int zDrop = sc.zdrop;
-    const int h0 = tk.h0;
-
-    // Query profile: the prmt selector of each column's base (:44-50), and
-    // the first row from h0 (:65-77).
-    {
-        int hv = h0;
-        bool ramp = h0 > oIns + eIns;
-        for (int j = 0; j <= qlen; ++j) {
-            int hj = 0;
-            if (j == 0) {
-                hj = h0;
-            } else if (j == 1) {
-                if (ramp) hj = hv = h0 - oIns - eIns;
-            } else if (ramp && hv > eIns) {
-                hj = hv -= eIns;
-            } else {
-                ramp = false;
-            }
-            if (U8) {
-                const uint32_t q = j < qlen ? span_base(a.bases, a.pac, tk.q_off, j, qlen, tk.flags, false) : 5u;
-                he[j * T] = ((q * 0x1111u + 0x8880u) & 0xFFFFu) | ((uint32_t)hj << 16);
-            } else {
-                if (j < qlen) {
-                    const uint32_t q = span_base(a.bases, a.pac, tk.q_off, j, qlen, tk.flags, false);
-                    qs[j * T] = (uint16_t)(q * 0x1111u + 0x8880u);
-                }
-                he[j * T] = (uint32_t)hj;
-            }
-        }
-    }
-    int w = tk.w;                                                          // :52-62
-    {
-        const int maxIns = (int)((double)(qlen * sc.max_mat + tk.end_bonus - oIns) / (double)eIns + 1.0);
-        w = imin(w, imax(1, maxIns));
-        const int maxDel = (int)((double)(qlen * sc.max_mat + tk.end_bonus - oDel) / (double)eDel + 1.0);
-        w = imin(w, imax(1, maxDel));
-    }
-    // Target reader: forward or reversed, bases or resident .pac, optional complement.
-    const bool tref = (tk.flags & SWB_T_FROM_REF) != 0;
-    const bool tcomp = (tk.flags & SWB_T_COMPLEMENT) != 0;
-    const long long tstep = (tk.flags & SWB_T_REVERSE) ? -1 : 1;
-    const long long tbase = (tk.flags & SWB_T_REVERSE) ? (long long)tk.t_off + tlen - 1 : (long long)tk.t_off;
-    // A column is all-zero (h == 0 and e == 0) when its H|E bits are zero.
-    const uint32_t nzmask = U8 ? 0xFFFF0000u : 0xFFFFFFFFu;
-
-    int maxScore = h0, maxI = -1, maxJ = -1, gScore = -1, gTle = -1, maxOff = 0;
-    int beg = 0, end = qlen;
-    for (int i = 0; i < tlen; ++i) {                                       // :90
-        const unsigned long long idx = (unsigned long long)(tbase + tstep * i);
-        uint32_t tb = tref ? (a.pac[idx >> 2] >> ((3u - (uint32_t)(idx & 3)) << 1)) & 3u : a.bases[idx];
-        if (tcomp && tb < 4u) tb = 3u - tb;
-        const RowTable rt = row_table(sc, tb);
-        if (beg < i - w) beg = i - w;                                      // :95-97
-        if (end > i + w + 1) end = i + w + 1;
-        if (end > qlen) end = qlen;
-        int f = 0;
-        int h1 = beg == 0 ? imax(h0 - (oDel + eDel * (i + 1)), 0) : 0;    // :99-107
-        uint32_t key = 0;
-        if (end > beg) cells += (unsigned long long)(end - beg);
-        uint32_t *hp = he + beg * T;
-        if (U8) {
-#pragma unroll 4
-            for (int j = beg; j < end; ++j, hp += T) {                    // :112-143
-                const uint32_t wd = *hp;
-                const int s = (int)prmt(rt.lo, rt.hi, wd);
-                const int M = (int)__byte_perm(wd, 0u, 0x4442);
-                const int e = (int)(wd >> 24);
-                const int d = __viaddmin_s32_relu(M, s, M << 7);
-                const int H = __vimax3_s32(d, e, f);
-                const int nE = __viaddmax_s32_relu(e, -eDel, d - oeDel);
-                *hp = __byte_perm(wd, __byte_perm((uint32_t)h1, (uint32_t)nE, 0x0040), 0x5410);
-                h1 = H;
-                key = max(key, ((uint32_t)H << 16) | (uint32_t)j);
-                f = __viaddmax_s32_relu(f, -eIns, d - oeIns);
-            }
-            he[end * T] = (he[end * T] & 0xFFFFu) | ((uint32_t)h1 << 16);  // :145-146
-        } else {
-            const uint16_t *qp = qs + beg * T;
-#pragma unroll 4
-            for (int j = beg; j < end; ++j, hp += T, qp += T) {           // :112-143
-                const uint32_t wd = *hp;
-                const int M = (int)(wd & 0xFFFFu), e = (int)(wd >> 16);
-                const int s = (int)prmt(rt.lo, rt.hi, (uint32_t)*qp);
-                const int d = __viaddmin_s32_relu(M, s, M << 7);
-                const int H = __vimax3_s32(d, e, f);
-                const int nE = __viaddmax_s32_relu(e, -eDel, d - oeDel);
-                *hp = __byte_perm((uint32_t)h1, (uint32_t)nE, 0x5410);
-                h1 = H;
-                key = max(key, ((uint32_t)H << 16) | (uint32_t)j);
-                f = __viaddmax_s32_relu(f, -eIns, d - oeIns);
-            }
-            he[end * T] = (uint32_t)h1 & 0xFFFFu;                          // :145-146
-        }
-        const int rowMax = end > beg ? (int)(key >> 16) : 0;
-        const int rowMaxJ = (int)(key & 0xFFFFu);
-        if (end == qlen) {                                                 // :149-152
-            gTle = gScore > h1 ? gTle : i;
-            gScore = gScore > h1 ? gScore : h1;
-        }
-        if (rowMax == 0) break;                                            // :155
-        if (rowMax > maxScore) {                                           // :158-172
-            maxScore = rowMax;
-            maxI = i;
-            maxJ = rowMaxJ;
-            const int off = abs(rowMaxJ - i);
-            if (off > maxOff) maxOff = off;
-        } else if (zDrop > 0) {
-            const int dI = i - maxI, dJ = rowMaxJ - maxJ;
-            if (dI > dJ) {
-                if (maxScore - rowMax - (dI - dJ) * eDel > zDrop) break;
-            } else {
-                if (maxScore - rowMax - (dJ - dI) * eIns > zDrop) break;
-            }
-        }
-        int nb = beg;                                                      // :175-180
-        while (nb < end && (he[nb * T] & nzmask) == 0u) ++nb;
-        beg = nb;
-        int ne = end;
-        while (ne >= beg && (he[ne * T] & nzmask) == 0u) --ne;
-        end = imin(ne + 2, qlen);
-    }
-    res = swb_ext_result{maxScore, maxJ + 1, maxI + 1, gTle + 1, gScore, maxOff};   // :183-190
-}
-
 template <int QMAX, int T, bool U8>
 __global__ void __launch_bounds__(T) ext_fast_kernel(ExtArgs a, int bin) {
     extern __shared__ uint32_t sm[];
-    uint32_t *he = sm + threadIdx.x;
-    uint16_t *qs = U8 ? nullptr : (uint16_t *)(sm + (QMAX + 1) * T) + threadIdx.x;
-    uint16_t *he16 = reinterpret_cast<uint16_t *>(sm) + threadIdx.x;                        // int8 rows
-    uint8_t *qc = reinterpret_cast<uint8_t *>(sm) + (size_t)(QMAX + 1) * T * 2 + threadIdx.x;
+    // Rows: (QMAX + 1) words of 2 (int8 scores) or 4 bytes (int16), then QMAX query bytes.
+    uint16_t *he16 = reinterpret_cast<uint16_t *>(sm) + threadIdx.x;
+    uint32_t *he32 = sm + threadIdx.x;
+    uint8_t *qc = reinterpret_cast<uint8_t *>(sm) + (size_t)(QMAX + 1) * T * (U8 ? 2 : 4) + threadIdx.x;
     static_assert(T == 32, "one warp per block: the warp claims its tasks together");
     const uint32_t lo = a.bin_start[bin], hi = a.bin_start[bin + 1];
     unsigned long long cells = 0;
@@ -269,12 +133,14 @@ __global__ void __launch_bounds__(T) ext_fast_kernel(ExtArgs a, int bin) {
             const uint32_t ti = a.order[pos];
             const swb_ext_task tk = a.tasks[ti];
             swb_ext_result r;
-            if (!U8)
-                ext_fast_one<T, false>(a, tk, he, qs, r, cells);
-            else if (a.sc.o_del + a.sc.e_del == a.sc.o_ins + a.sc.e_ins)
-                ext_pair_one<T, true>(a, tk, he16, qc, r, cells);
-            else
-                ext_pair_one<T, false>(a, tk, he16, qc, r, cells);
+            const bool sym = a.sc.o_del + a.sc.e_del == a.sc.o_ins + a.sc.e_ins;
+            if constexpr (U8) {
+                if (sym) ext_pair_one<T, true, false>(a, tk, he16, qc, r, cells);
+                else ext_pair_one<T, false, false>(a, tk, he16, qc, r, cells);
+            } else {
+                if (sym) ext_pair_one<T, true, true>(a, tk, he32, qc, r, cells);
+                else ext_pair_one<T, false, true>(a, tk, he32, qc, r, cells);
+            }
             a.out[ti] = r;
         }
     }
@@ -336,10 +202,9 @@ __global__ void __launch_bounds__(kBigT) ext_global_kernel(ExtArgs a, int *h, in
 
 template <int QMAX, bool U8>
 constexpr size_t fast_smem_bytes() {
-    // int8 rows: a 16-bit word and a query byte per column; int16 rows: a
-    // 32-bit word and a 16-bit selector per column.
-    return U8 ? ((size_t)(QMAX + 1) * kFastT * sizeof(uint16_t) + (size_t)QMAX * kFastT + 15) & ~(size_t)15
-              : (size_t)(QMAX + 1) * kFastT * sizeof(uint32_t) + (size_t)QMAX * kFastT * sizeof(uint16_t);
+    // A 16-bit (int8 scores) or 32-bit (int16) word and a query byte per column.
+    return ((size_t)(QMAX + 1) * kFastT * (U8 ? sizeof(uint16_t) : sizeof(uint32_t)) + (size_t)QMAX * kFastT + 15) &
+           ~(size_t)15;
 }
 
 const char *const kBinNames[kNumBins] = {
@@ -417,9 +282,9 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     const unsigned tb = 256;
     {
         ProfScope ps(ctx, s, "ext_keys", -1);
-        // int8 rows run two target rows per pass on 16-bit lanes: the gap costs must fit a lane.
-        const int u8_ok = sc.o_del + sc.e_del <= 32767 && sc.o_ins + sc.e_ins <= 32767;
-        ext_keys_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(d_tasks, n, sc.max_mat, u8_ok, warp_cells, keys,
+        // Two target rows per pass on 16-bit lanes: the gap costs must fit a lane.
+        const int pair_ok = sc.o_del + sc.e_del <= 32767 && sc.o_ins + sc.e_ins <= 32767;
+        ext_keys_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(d_tasks, n, sc.max_mat, pair_ok, warp_cells, keys,
                                                                        idx, big_max_q);
     }
     ctx->launches++;
@@ -496,31 +361,17 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     return SWB_OK;
 }
 
-// Host-side twin of the device bin test, used to size the scratch bin
-// (several host threads for large batches).
-// Longest query among tasks[lo, hi) that the int32 global-scratch bin takes.
-int ext_big_max_q_range(const swb_ext_task *tasks, size_t lo, size_t hi, int max_mat) {
+// Host-side twin of the device bin test: the longest query among
+// tasks[lo, hi) that the int32 bin takes (sizes its kernels' rows).
+int ext_big_max_q_range(const swb_ext_task *tasks, size_t lo, size_t hi, const DevScoring &sc) {
+    const bool pair_ok = sc.o_del + sc.e_del <= 32767 && sc.o_ins + sc.e_ins <= 32767;
     int m = 0;
     for (size_t i = lo; i < hi; ++i) {
         const swb_ext_task &t = tasks[i];
         if (t.qlen <= 0 || t.tlen <= 0) continue;
-        if (t.qlen > kExtSmemMaxQ || !fits16(t.qlen, t.h0, max_mat)) m = t.qlen > m ? t.qlen : m;
+        if (!pair_ok || t.qlen > kExtSmemMaxQ || !fits16(t.qlen, t.h0, sc.max_mat)) m = t.qlen > m ? t.qlen : m;
     }
     return m;
-}
-
-int ext_big_max_q(const swb_ext_task *tasks, size_t n, int max_mat) {
-    auto range = [&](size_t lo, size_t hi) { return ext_big_max_q_range(tasks, lo, hi, max_mat); };
-    const size_t kChunk = 1 << 18;
-    const size_t nth = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), (n + kChunk - 1) / kChunk);
-    if (nth <= 1) return range(0, n);
-    std::vector<int> part(nth, 0);
-    std::vector<std::thread> th;
-    const size_t per = (n + nth - 1) / nth;
-    for (size_t k = 0; k < nth; ++k)
-        th.emplace_back([&, k] { part[k] = range(k * per, std::min(n, (k + 1) * per)); });
-    for (auto &t : th) t.join();
-    return *std::max_element(part.begin(), part.end());
 }
 
 }  // namespace swb

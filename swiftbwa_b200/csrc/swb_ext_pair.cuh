@@ -1,15 +1,18 @@
 // swb_ext_pair.cuh -- BandedSWScalar.align (Sources/Alignment/BandedSWScalar.swift:21-191)
-// for int8-bounded tasks, two target rows per pass.
+// for int16-bounded tasks, two target rows per pass.
 //
-// Row layout (shared memory, [column][thread]):
-//   16-bit word per column: bits 0-7 H of the previous row at the previous
-//   column (the diagonal input), bits 8-15 E into this column -- exactly the
-//   reference's h[j] / e[j] storage (`h[j]` holds the left neighbour's H once
-//   the row has passed it), with the scores bounded by 255;
-//   one byte per column: the query base q, from which the prmt selector
-//   (q, q|8, 5, 5) -- the row's score for q as a 16-bit value [s, sign, 0, 0]
-//   -- is formed with one multiply-add.
-// Three bytes per column keep ~17 one-warp blocks resident per SM.
+// Row layout (shared memory, [column][thread]), one word per column: H of the
+// previous row at the previous column (the diagonal input) in the low half,
+// E into this column in the high half -- exactly the reference's h[j] / e[j]
+// storage (`h[j]` holds the left neighbour's H once the row has passed it):
+//   W16 = false: a 16-bit word of two bytes, for tasks whose scores are
+//                bounded by 255 (three bytes per column with the query byte
+//                keep ~17 one-warp blocks resident per SM at 128 columns);
+//   W16 = true : a 32-bit word of two 16-bit halves, for scores bounded by
+//                32000.
+// One byte per column holds the query base q, from which the prmt selector
+// (q, q|8, 5, 5) -- the row's score for q as a 16-bit value [s, sign, 0, 0]
+// -- is formed with one multiply-add.
 //
 // Rows i and i+1 advance together, row i+1 one column behind row i: at step c
 // row i computes column c from the word it loads, and row i+1 computes
@@ -35,7 +38,13 @@
 //     results are used; row i+1's own checks follow in order;
 //   * band narrowing after row i+1: the first nonzero word by the reference's
 //     scan, the last one from lane 1's last column with H > 0.
+// The diagonal's M != 0 rule is min(M + s, Mcap) relu with Mcap >= M + s
+// when M > 0 and 0 when M = 0: M*128 for byte scores, a 0/1 lane mask times
+// 0x7FFF for 16-bit ones.  The row max (last column on ties) is a u16x2 key
+// H*256 + j for byte scores and one s32 key (H << 16) + j per row otherwise.
 #pragma once
+
+#include <type_traits>
 
 #include "swb_device.cuh"
 #include "swb_ext_dp.cuh"
@@ -51,31 +60,52 @@ struct PairConsts {
     uint32_t negOeDel, negOeIns, negEDel, negEIns;   // replicated in both 16-bit lanes
 };
 
+// Row words: 16-bit [H byte | E byte] or 32-bit [H16 | E16].
+template <bool W16>
+using RowWord = typename std::conditional<W16, uint32_t, uint16_t>::type;
+
+// Mcap of the M != 0 rule for the lanes of M (see the header).
+template <bool W16>
+__device__ __forceinline__ uint32_t m_cap(uint32_t M) {
+    if constexpr (W16) return __vimin3_u16x2(M, 0x00010001u, 0x00010001u) * 0x7FFFu;
+    else return M * 128u;
+}
+
 // One cell in the low lane only (the high lane's inputs are zero).  `w` is the
-// column's word as the reference's loop reads it; returns the new word's
-// upper half (h1 before, E') and updates h1, f, key, lastJ.  SYM: the open
-// costs oDel+eDel and oIns+eIns are equal, so E' and F' share one operand.
-template <bool SYM>
+// column's word as the reference's loop reads it; returns the new word (h1
+// before, E') and updates h1, f, key, lastJ.  SYM: the open costs oDel+eDel
+// and oIns+eIns are equal, so E' and F' share one operand.
+template <bool SYM, bool W16>
 __device__ __forceinline__ uint32_t single_cell(const PairConsts &pc, const RowTable &rt, uint32_t w, uint32_t sel,
                                                 int j, uint32_t &h1, uint32_t &f, uint32_t &key, uint32_t &lastJ) {
     const uint32_t s = lane_score(rt, sel);
-    const uint32_t M = __byte_perm(w, 0u, 0x4440);          // [H, 0, 0, 0]
-    const uint32_t e = __byte_perm(w, 0u, 0x4441);          // [E, 0, 0, 0]
-    const uint32_t d = __viaddmin_s16x2_relu(M, s, M * 128u);
+    const uint32_t M = W16 ? __byte_perm(w, 0u, 0x4410) : __byte_perm(w, 0u, 0x4440);   // [H, 0]
+    const uint32_t e = W16 ? __byte_perm(w, 0u, 0x4432) : __byte_perm(w, 0u, 0x4441);   // [E, 0]
+    const uint32_t d = __viaddmin_s16x2_relu(M, s, m_cap<W16>(M));
     const uint32_t H = __vimax3_s16x2(d, e, f);
     const uint32_t tDel = __viaddmax_s16x2(d, pc.negOeDel, 0x80008000u);
     const uint32_t nE = __viaddmax_s16x2_relu(e, pc.negEDel, tDel);
     const uint32_t tIns = SYM ? tDel : __viaddmax_s16x2(d, pc.negOeIns, 0x80008000u);
     f = __viaddmax_s16x2_relu(f, pc.negEIns, tIns);
-    const uint32_t up = __byte_perm(h1, nE, 0x0040);         // [h1, E'] -> the column's new word
-    const uint32_t Hs = H * 256u;
-    key = __viaddmax_u16x2(Hs, (uint32_t)j, key);
-    lastJ = __vimax3_u16x2(lastJ, __vimin3_u16x2((uint32_t)j, Hs, (uint32_t)j), lastJ);
+    // [h1, E'] -> the column's new word
+    const uint32_t up = W16 ? __byte_perm(h1, nE, 0x5410) : __byte_perm(h1, nE, 0x0040);
+    if constexpr (W16) {
+        key = (uint32_t)__viaddmax_s32((int)__byte_perm(H, 0u, 0x1044), j, (int)key);   // (H << 16) + j
+        const uint32_t Hz = __vimin3_u16x2(H, 0x00010001u, 0x00010001u) * 0x7FFFu;                     // 0x7FFF where H > 0
+        lastJ = __vimax3_u16x2(lastJ, __vimin3_u16x2((uint32_t)j, Hz, (uint32_t)j), lastJ);
+    } else {
+        const uint32_t Hs = H * 256u;
+        key = __viaddmax_u16x2(Hs, (uint32_t)j, key);
+        lastJ = __vimax3_u16x2(lastJ, __vimin3_u16x2((uint32_t)j, Hs, (uint32_t)j), lastJ);
+    }
     h1 = H;
     return up;
 }
 
-__device__ __forceinline__ void store_up(uint16_t *he, int T, int j, uint32_t up) { he[j * T] = (uint16_t)up; }
+template <bool W16>
+__device__ __forceinline__ void store_up(RowWord<W16> *he, int T, int j, uint32_t up) {
+    he[j * T] = (RowWord<W16>)up;
+}
 
 // prmt selector (q, q|8, 5, 5) of query code q (0-4).
 __device__ __forceinline__ uint32_t sel_of(uint32_t q) { return q * 0x11u + 0x5580u; }
@@ -109,10 +139,12 @@ struct RowTrack {
     }
 };
 
-template <int T, bool SYM>
-__device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_task &tk, uint16_t *__restrict__ he,
+template <int T, bool SYM, bool W16>
+__device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_task &tk, RowWord<W16> *__restrict__ he,
                                              uint8_t *__restrict__ qc, swb_ext_result &res,
                                              unsigned long long &cells) {
+    using Word = RowWord<W16>;
+    constexpr uint32_t kLoMask = W16 ? 0xFFFFu : 0xFFu;      // one score field of a word
     res = swb_ext_result{0, 0, 0, 0, 0, 0};
     const int qlen = tk.qlen, tlen = tk.tlen;
     if (!(qlen > 0 && tlen > 0)) return;                                      // :33-35
@@ -142,7 +174,7 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
                 ramp = false;
             }
             if (j < qlen) qc[j * T] = (uint8_t)span_base(a.bases, a.pac, tk.q_off, j, qlen, tk.flags, false);
-            he[j * T] = (uint16_t)hj;
+            he[j * T] = (Word)hj;
         }
     }
     int w = tk.w;                                                              // :52-62
@@ -188,21 +220,25 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
             const uint32_t wd = he[c * T];
             const uint32_t sel = sel_of(qc[c * T]);
             const uint32_t hb = h1;
-            const uint32_t up = single_cell<SYM>(pc, rt0, wd, sel, c, h1, f, key, lastJ);
+            const uint32_t up = single_cell<SYM, W16>(pc, rt0, wd, sel, c, h1, f, key, lastJ);
             hPrev = hb;
-            nEPrev = up >> 8;           // E' of row i at column c (byte 1 of up)
+            nEPrev = W16 ? up >> 16 : up >> 8;   // E' of row i at column c (the word's high field)
             sPrev = sel;
-            if (firstNz < 0 && (up & 0xFFFFu) != 0u) firstNz = c;
+            if (firstNz < 0 && (W16 ? up : up & 0xFFFFu) != 0u) firstNz = c;
             if (pair && firstNz >= 0 && c >= lo1) {
                 ++c;
                 started = true;
                 break;
             }
         }
-        nEPrev &= 0xFFu;
+        nEPrev &= kLoMask;
         // ---- phase B: rows i and i+1 in lockstep (row i at c, row i+1 at c-1)
         const int beg1 = started ? c - 1 : -1;                                 // row i+1's first column, if known
-        uint32_t h1p = h1, fp = f, keyp = key, lastJp = lastJ;                 // lane 0 = row i, lane 1 = row i+1
+        uint32_t h1p = h1, fp = f, lastJp = lastJ;                             // lane 0 = row i, lane 1 = row i+1
+        // Row-max keys: byte scores one u16x2 key for both rows; 16-bit
+        // scores one s32 key per row, row i+1's counting column + 1 while in
+        // lockstep (corrected below).
+        uint32_t keyp = key, key1w = 0u;
         const RowTable rt1 = pair ? row_tab(i + 1) : rt0;
         if (started) {
             h1p |= (beg1 == 0 ? h1_init(i + 1) : 0u) << 16;
@@ -212,32 +248,41 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
             for (; c < e0; ++c, jp += 0x10001u) {
                 const uint32_t wd = he[c * T];
                 const uint32_t sel = sel_of(qc[c * T]);
-                const uint32_t Mp = __byte_perm(wd, hPrevP, 0x5450);            // [H(i-1,c-1), H(i,c-2)]
-                const uint32_t ep = __byte_perm(wd, nEPrev, 0x5451);            // [E(i,c),     E(i+1,c-1)]
+                const uint32_t Mp = W16 ? __byte_perm(wd, hPrevP, 0x5410) : __byte_perm(wd, hPrevP, 0x5450);   // [H(i-1,c-1), H(i,c-2)]
+                const uint32_t ep = W16 ? __byte_perm(wd, nEPrev, 0x5432) : __byte_perm(wd, nEPrev, 0x5451);   // [E(i,c),     E(i+1,c-1)]
                 const uint32_t sp = lane_score(rt1, sPrev) * 65536u + lane_score(rt0, sel);
-                const uint32_t d = __viaddmin_s16x2_relu(Mp, sp, Mp * 128u);
+                const uint32_t d = __viaddmin_s16x2_relu(Mp, sp, m_cap<W16>(Mp));
                 const uint32_t H = __vimax3_s16x2(d, ep, fp);
                 const uint32_t tDel = __viaddmax_s16x2(d, pc.negOeDel, 0x80008000u);
                 const uint32_t nE = __viaddmax_s16x2_relu(ep, pc.negEDel, tDel);
                 const uint32_t tIns = SYM ? tDel : __viaddmax_s16x2(d, pc.negOeIns, 0x80008000u);
                 fp = __viaddmax_s16x2_relu(fp, pc.negEIns, tIns);
-                store_up(he, T, c - 1, __byte_perm(h1p, nE, 0x0062));           // row i+1's word for c-1
-                const uint32_t Hs = H * 256u;
-                keyp = __viaddmax_u16x2(Hs, jp, keyp);
-                lastJp = __vimax3_u16x2(lastJp, __vimin3_u16x2(jp, Hs, jp), lastJp);
+                // row i+1's word for c-1
+                store_up<W16>(he, T, c - 1, W16 ? __byte_perm(h1p, nE, 0x7632) : __byte_perm(h1p, nE, 0x0062));
+                if constexpr (W16) {
+                    keyp = (uint32_t)__viaddmax_s32((int)__byte_perm(H, 0u, 0x1044), c, (int)keyp);
+                    key1w = (uint32_t)__viaddmax_s32((int)(H & 0xFFFF0000u), c, (int)key1w);
+                    const uint32_t Hz = __vimin3_u16x2(H, 0x00010001u, 0x00010001u) * 0x7FFFu;
+                    lastJp = __vimax3_u16x2(lastJp, __vimin3_u16x2(jp, Hz, jp), lastJp);
+                } else {
+                    const uint32_t Hs = H * 256u;
+                    keyp = __viaddmax_u16x2(Hs, jp, keyp);
+                    lastJp = __vimax3_u16x2(lastJp, __vimin3_u16x2(jp, Hs, jp), lastJp);
+                }
                 hPrevP = h1p;
                 sPrev = sel;
-                nEPrev = nE;    // byte 0 = row i's E', byte 1 = 0 (lane values <= 255)
+                nEPrev = nE;    // low field = row i's E', the high lane's upper bits never reach a word
                 h1p = H;
             }
             hPrev = hPrevP & 0xFFFFu;
         }
         // ---- row i complete
         const int h1i = (int)(h1p & 0xFFFFu);
-        const int key0 = (int)(keyp & 0xFFFFu);
-        const int rowMax0 = e0 > b0 ? key0 >> 8 : 0;
+        const int key0 = W16 ? (int)keyp : (int)(keyp & 0xFFFFu);
+        const int rowMax0 = e0 > b0 ? (W16 ? key0 >> 16 : key0 >> 8) : 0;
+        const int rowMaxJ0 = W16 ? key0 & 0xFFFF : key0 & 0xFF;
         // (the last row's words, h[end] included, are never read again)
-        if (!tr.finish(i, rowMax0, key0 & 0xFF, h1i, e0 == qlen, zDrop, eDel, eIns)) break;
+        if (!tr.finish(i, rowMax0, rowMaxJ0, h1i, e0 == qlen, zDrop, eDel, eIns)) break;
         if (!pair) break;   // last row
         // Narrowing after row i (:175-180): first nonzero word, last nonzero word = last H > 0 column + 1.
         const int lastH = (int)(lastJp & 0xFFFFu);
@@ -250,29 +295,30 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
         if (e1 > b1) cells += (unsigned long long)(e1 - b1);
         // ---- drain: row i+1 alone for its columns past the lockstep
         int s = started ? c - 1 : b1;                                          // next column of row i+1
-        uint32_t f1 = fp >> 16, k1 = keyp >> 16, lj1 = lastJp >> 16;
+        uint32_t f1 = fp >> 16, k1 = W16 ? key1w - 1u : keyp >> 16, lj1 = lastJp >> 16;
         uint32_t h1b = started ? (h1p >> 16) : (b1 == 0 ? h1_init(i + 1) : 0u);
         if (!started) f1 = 0u, k1 = 0u, lj1 = 0u;
         for (; s < e1; ++s) {
             // Row i's word for column s: from registers (c-1 = e0-1), the row-end word, or untouched.
             uint32_t wd = he[s * T];
-            if (s == e0 - 1) wd = hPrev | ((nEPrev & 0xFFu) << 8);
+            if (s == e0 - 1) wd = hPrev | ((nEPrev & kLoMask) << (W16 ? 16 : 8));
             else if (s == e0) wd = (uint32_t)h1i;
-            const uint32_t up = single_cell<SYM>(pc, rt1, wd, sel_of(qc[s * T]), s, h1b, f1, k1, lj1);
-            store_up(he, T, s, up);
+            const uint32_t up = single_cell<SYM, W16>(pc, rt1, wd, sel_of(qc[s * T]), s, h1b, f1, k1, lj1);
+            store_up<W16>(he, T, s, up);
         }
         // H of row i+1's last valid column: from the register if it was the last
         // cell computed, else from the word the lockstep stored at column e1.
         int h1last = (int)(h1b & 0xFFFFu);
         const bool overran = started && e1 <= e0 - 2;
-        if (overran) h1last = (int)(he[e1 * T] & 0xFFu);
-        const int key1 = (int)(k1 & 0xFFFFu);
-        const int rowMax1 = e1 > b1 ? key1 >> 8 : 0;
+        if (overran) h1last = (int)(he[e1 * T] & kLoMask);
+        const int key1 = W16 ? (int)k1 : (int)(k1 & 0xFFFFu);
+        const int rowMax1 = e1 > b1 ? (W16 ? key1 >> 16 : key1 >> 8) : 0;
+        const int rowMaxJ1 = W16 ? key1 & 0xFFFF : key1 & 0xFF;
         // Words the reference holds after row i+1: h[e1] = H(e1-1), e[e1] = 0,
         // then row i's zero tail up to e0.
-        he[e1 * T] = (uint16_t)h1last;
+        he[e1 * T] = (Word)h1last;
         for (int z = e1 + 1; z <= e0; ++z) he[z * T] = 0;
-        if (!tr.finish(i + 1, rowMax1, key1 & 0xFF, h1last, e1 == qlen, zDrop, eDel, eIns)) break;
+        if (!tr.finish(i + 1, rowMax1, rowMaxJ1, h1last, e1 == qlen, zDrop, eDel, eIns)) break;
         // Narrowing after row i+1 (:175-180).
         int nb = b1;
         while (nb < e1 && he[nb * T] == 0) ++nb;

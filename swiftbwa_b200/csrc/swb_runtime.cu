@@ -19,8 +19,7 @@
 
 namespace swb {
 
-int ext_big_max_q(const swb_ext_task *tasks, size_t n, int max_mat);
-int ext_big_max_q_range(const swb_ext_task *tasks, size_t lo, size_t hi, int max_mat);
+int ext_big_max_q_range(const swb_ext_task *tasks, size_t lo, size_t hi, const DevScoring &sc);
 
 static thread_local std::string g_last_error;
 
@@ -410,7 +409,7 @@ int swb_ext_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, siz
             if (a >= b) return;
             int mq, mt;
             if ((pt.code = validate_range(ctx, tasks, a, b, n_bases, &mq, &mt, &pt.err, &pt.code))) return;
-            pt.big_q = ext_big_max_q_range(tasks, a, b, dsc.max_mat);
+            pt.big_q = ext_big_max_q_range(tasks, a, b, dsc);
             size_t m = 0;
             for (size_t i = a; i < b; ++i) {
                 const swb_ext_task &tk = tasks[i];
