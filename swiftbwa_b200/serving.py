@@ -80,6 +80,89 @@ class Server:
             pass
 
 
+class MultiServer:
+    """Requests over several GPUs, one Server each (one per device's Engine):
+    every request goes to the server with the fewest outstanding estimated
+    DP cells, and a request of at least `split_tasks` tasks is cut into
+    cell-balanced contiguous slices, one per server, each writing its own
+    view of the request's output.  No data crosses GPUs; every GPU holds its
+    own copy of the resident reference."""
+
+    def __init__(self, servers, split_tasks: int = 0):
+        if not servers:
+            raise ValueError("MultiServer needs at least one server")
+        self.servers = list(servers)
+        self.split_tasks = int(split_tasks)
+        self._load = [0] * len(self.servers)      # outstanding estimated cells per server
+        self._handles = {}
+        self._next = 0
+        self._lock = threading.Lock()
+
+    def _pick(self) -> int:
+        return min(range(len(self.servers)), key=lambda k: (self._load[k], k))
+
+    def submit(self, bases: np.ndarray, tasks: np.ndarray, out: Optional[np.ndarray] = None,
+               span_origin: int = 0) -> int:
+        from .sharding import partition_by_cells, task_cells_estimate
+        assert tasks.dtype == EXT_TASK_DTYPE and tasks.flags["C_CONTIGUOUS"]
+        if out is None:
+            out = np.zeros(len(tasks), EXT_RESULT_DTYPE)
+        cells = task_cells_estimate(tasks)
+        n_srv = len(self.servers)
+        if n_srv > 1 and self.split_tasks and len(tasks) >= self.split_tasks:
+            b = partition_by_cells(tasks, n_srv)
+            pieces = [(b[k], b[k + 1]) for k in range(n_srv) if b[k + 1] > b[k]]
+        else:
+            pieces = [(0, len(tasks))]
+        parts = []
+        with self._lock:
+            order = sorted(range(n_srv), key=lambda k: (self._load[k], k))
+            for j, (lo, hi) in enumerate(pieces):
+                k = order[j % n_srv] if len(pieces) > 1 else self._pick()
+                c = int(cells[lo:hi].sum())
+                t = self.servers[k].submit(bases, tasks[lo:hi], out[lo:hi], span_origin=span_origin)
+                self._load[k] += c
+                parts.append((k, t, c))
+            h = self._next
+            self._next += 1
+            self._handles[h] = (parts, out)
+        return h
+
+    def poll(self, handle: int):
+        """(done, status): done when every slice is; the first nonzero status."""
+        parts, _ = self._handles[handle]
+        done, status = True, 0
+        for k, t, _ in parts:
+            d, st = self.servers[k].poll(t)
+            done = done and d
+            status = status or st
+        return done, status
+
+    def wait(self, handle: int, timeout_ms: int = 60_000):
+        """-> (results array, first submit_ns, last done_ns)."""
+        with self._lock:
+            parts, out = self._handles.pop(handle)
+        s_ns, d_ns = None, 0
+        for k, t, c in parts:
+            try:
+                _, s, d = self.servers[k].wait(t, timeout_ms)
+            finally:
+                with self._lock:
+                    self._load[k] -= c
+            s_ns = s if s_ns is None else min(s_ns, s)
+            d_ns = max(d_ns, d)
+        return out, s_ns, d_ns
+
+    def load(self):
+        """Outstanding estimated cells per server."""
+        with self._lock:
+            return list(self._load)
+
+    def stop(self):
+        for srv in self.servers:
+            srv.stop()
+
+
 @dataclass
 class Request:
     lo: int          # task range in the pool

@@ -133,3 +133,21 @@ def test_pinned_zero_copy_pool(engine, plain):
     finally:
         srv.stop()
     assert np.array_equal(po, expected)
+
+
+def test_multiserver_on_one_gpu(engine):
+    """The multi-GPU router over this GPU's server (one device here): results
+    equal the direct batch call, whole and split into slices."""
+    from swiftbwa_b200.serving import MultiServer, Server
+    sc = Scoring.default()
+    d = gen.ext_tasks(404, 4000, qmax=200)
+    expected = engine.ext_batch(sc, d["bases"], d["tasks"])
+    srv = Server(engine, sc)
+    try:
+        ms = MultiServer([srv], split_tasks=1000)
+        h = ms.submit(d["bases"], d["tasks"])
+        out, s_ns, d_ns = ms.wait(h)
+        assert np.array_equal(out, expected) and s_ns <= d_ns
+        assert ms.load() == [0]
+    finally:
+        srv.stop()
