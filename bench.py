@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--c4-latency-cells", type=int, default=0,
                     help="served mode: tasks above this many DP cells run one warp per extension")
     ap.add_argument("--c5-chains", type=int, default=1_000_000)
+    ap.add_argument("--no-tune", action="store_true", help="keep the default length classes (no autotuning)")
+    ap.add_argument("--tune-sample", type=int, default=0,
+                    help="tasks the length-class autotuner times (0: the whole workload)")
     ap.add_argument("--c3-jobs", type=int, default=1_000_000)
     ap.add_argument("--suite-only", default="",
                     help="comma list of secondary configs to run alone (config0, config2, config3, config3_rescue_driver, "
@@ -218,6 +221,7 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
     if want("config2"):
         wl2 = W.config2(n=args.c2_tasks)
         eng.upload_reference(wl2.ref.pac, wl2.ref.n)
+        tune2 = None if args.no_tune else eng.tune_ext_bins(sc, wl2.bases, wl2.tasks[: args.tune_sample or None])
         db = torch.from_numpy(wl2.bases).to(dev)
         dt = torch.from_numpy(wl2.tasks.view(np.uint8)).to(dev)
         dpac = torch.from_numpy(wl2.ref.pac).to(dev)
@@ -245,7 +249,7 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
         c2 = {"tasks": n2, "binned_ms": ms_b, "binned_ext_per_s": n2 / ms_b * 1e3, "gcups": cells2 / ms_b / 1e6,
               "plain_kernel_ms": ms_p, "plain_kernel_ext_per_s": n2 / ms_p * 1e3, "speedup_vs_plain": ms_p / ms_b,
               "plain_kernel": "one launch, input order, one 256-column int16 row layout for every task (swb_ext_batch_static)",
-              "binned_equals_plain": same2}
+              "binned_equals_plain": same2, "ext_bins": eng.ext_bins(), "ext_bins_tuning": tune2}
         if cpu_on:
             s2 = 60_000
             t0 = time.perf_counter()
@@ -405,6 +409,7 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
         ref4 = W.reference(W.SEED_BASE + 4, args.c4_ref_len)
         eng.upload_reference(ref4.pac, ref4.n)
         pool = W.uneven(ref4, W.SEED_BASE + 4 + 1, args.c4_pool, name="config4 pool")
+        tune4 = None if args.no_tune else eng.tune_ext_bins(sc, pool.bases, pool.tasks[: args.tune_sample or None])
         # The serving process keeps its read chunks in pinned memory, so requests
         # are zero-copy views of the pool.
         pb = torch.from_numpy(pool.bases).pin_memory().numpy()
@@ -425,7 +430,7 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
               "p99_ms_50k_200k": _pct(mid, 99) * 1e3 if mid else None, "n_50k_200k": len(mid),
               "p50_ms_70k_140k": _pct(near100k, 50) * 1e3 if near100k else None,
               "p99_ms_70k_140k": _pct(near100k, 99) * 1e3 if near100k else None, "n_70k_140k": len(near100k),
-              "waves": st["waves"], "wave_tasks": args.c4_wave, "latency_cells": args.c4_latency_cells, "wave_device_ms_sum": st["busy_ms"], "span_s": span,
+              "waves": st["waves"], "wave_tasks": args.c4_wave, "latency_cells": args.c4_latency_cells, "ext_bins": eng.ext_bins(), "ext_bins_tuning": tune4, "wave_device_ms_sum": st["busy_ms"], "span_s": span,
               "stream": "Poisson 200 req/s, sizes log-uniform 1k-1M tasks, qlen log-uniform 30-250, w 10-100, h0 19-60, "
                         "1 Gbp resident 2-bit reference"}
         # saturation: the same size distribution submitted at once, served vs plain
@@ -519,6 +524,9 @@ def run_ours(args):
     n = len(wl.tasks)
     eng = Engine(local)
     eng.upload_reference(wl.ref.pac, wl.ref.n)
+    # Length classes of the bins, autotuned on a sample of this workload
+    # before any timing (one-time setup, like a library's algorithm search).
+    tune1 = None if args.no_tune else eng.tune_ext_bins(sc, wl.bases, wl.tasks[: args.tune_sample or None])
     alu_peak = eng.int_alu_peak()
     alu16_peak = eng.int16x2_alu_peak()
 
@@ -616,7 +624,8 @@ def run_ours(args):
             "config": {"workload": wl.name, "tasks_per_gpu": n, "reads_per_gpu": args.n_reads, "read_len": 150,
                        "ref_bases": wl.ref.n, "w": 100, "h0": 19, "end_bonus": 5,
                        "l2": f"inputs larger than L2 ({(wl.bases.nbytes + wl.tasks.nbytes) / 1e6:.0f} MB read per step)",
-                       "parallelism": f"replicas x{ws} (task shards, no collective)"},
+                       "parallelism": f"replicas x{ws} (task shards, no collective)",
+                       "ext_bins": eng.ext_bins(), "ext_bins_tuning": tune1},
             "gcups": cells_step * ws / (ms_max * 1e-3) / 1e9,
             "cells_per_step_per_gpu": cells_step,
             "roofline": {"bound": "alu", "kernel": dom_name, "achieved": achieved / 1e12,

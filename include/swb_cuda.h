@@ -241,6 +241,26 @@ int swb_ext_batch_device(swb_ctx *ctx, const swb_scoring *sc,
                          const uint8_t *d_bases, const swb_ext_task *d_tasks,
                          size_t n_tasks, swb_ext_result *d_out, void *stream);
 
+/* Length classes of the extension bins: ascending query-length bounds
+ * (1..15 values within [8, 256]); each class has an int8-row and an
+ * int16-row bin (two target rows per pass, one task per thread), and
+ * queries above the last bound, or with scores beyond int16, run one warp
+ * per extension.  Defaults: 32 48 64 80 96 112 128 160 192 256.  No
+ * reference counterpart: the reference dispatches every batch to one
+ * kernel (BandedSWDispatcher.swift:48,107). */
+int swb_set_ext_bins(swb_ctx *ctx, const int32_t *qmax, int n);
+int swb_get_ext_bins(swb_ctx *ctx, int32_t *qmax, int cap, int *n);
+/* Autotuner: times candidate class sets (the defaults, uniform steps, and
+ * quantiles of the batch's query lengths and estimated cells) on the given
+ * sample batch (host arrays, as swb_ext_batch; best of two runs after a
+ * warm-up each) and keeps the fastest in the context, the defaults unless
+ * another set is more than 2 % faster.  Writes the chosen classes
+ * (qmax_out[0..cap), *n_out), the chosen set's and the defaults' time on
+ * the sample (ms; may be NULL). */
+int swb_tune_ext_bins(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, size_t n_bases,
+                      const swb_ext_task *tasks, size_t n_tasks, int32_t *qmax_out, int cap, int *n_out,
+                      float *best_ms, float *default_ms);
+
 /* Allocation-free variant of swb_ext_batch_device.  It has no counterpart
  * in the reference.  It is for callers that cannot let a library call
  * cudaMalloc: a server whose own arena already holds the free HBM (the

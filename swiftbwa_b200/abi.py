@@ -133,7 +133,7 @@ EXPORTED_SYMBOLS = (
     "swb_global_batch", "swb_local_batch", "swb_ext_batch_device",
     "swb_banded_sw_align", "swb_global_align", "swb_local_align",
     "swb_kernel_launches", "swb_last_batch_stats", "swb_profile", "swb_profile_reset",
-    "swb_profile_read", "swb_int_alu_peak", "swb_int16x2_alu_peak", "swb_ext_batch_static", "swb_cigar_batch",
+    "swb_profile_read", "swb_int_alu_peak", "swb_int16x2_alu_peak", "swb_set_ext_bins", "swb_get_ext_bins", "swb_tune_ext_bins", "swb_ext_batch_static", "swb_cigar_batch",
     "swb_server_start", "swb_server_submit", "swb_server_poll", "swb_server_wait", "swb_server_resume",
     "swb_server_stats_get", "swb_server_stop", "swb_extend_chains", "swb_mate_rescue",
 )
@@ -222,6 +222,13 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.swb_int_alu_peak.restype = C.c_int
     lib.swb_int16x2_alu_peak.argtypes = [vp, P(C.c_double)]
     lib.swb_int16x2_alu_peak.restype = C.c_int
+    lib.swb_set_ext_bins.argtypes = [vp, P(C.c_int32), C.c_int]
+    lib.swb_set_ext_bins.restype = C.c_int
+    lib.swb_get_ext_bins.argtypes = [vp, P(C.c_int32), C.c_int, P(C.c_int)]
+    lib.swb_get_ext_bins.restype = C.c_int
+    lib.swb_tune_ext_bins.argtypes = [vp, P(Scoring), vp, C.c_size_t, vp, C.c_size_t, P(C.c_int32), C.c_int,
+                                      P(C.c_int), P(C.c_float), P(C.c_float)]
+    lib.swb_tune_ext_bins.restype = C.c_int
     lib.swb_ext_batch_static.argtypes = [P(Scoring), vp, vp, vp, C.c_size_t, vp, vp]
     lib.swb_ext_batch_static.restype = C.c_int
     lib.swb_cigar_batch.argtypes = [vp, P(Scoring), u8p, C.c_size_t, vp, C.c_size_t, vp, P(C.c_uint32),

@@ -261,6 +261,30 @@ class Engine:
         _check(self.lib.swb_int_alu_peak(self.h, C.byref(v)), "swb_int_alu_peak")
         return v.value
 
+    def set_ext_bins(self, qmax) -> None:
+        """Length classes of the extension bins (ascending query-length bounds)."""
+        arr = (C.c_int32 * len(qmax))(*qmax)
+        _check(self.lib.swb_set_ext_bins(self.h, arr, len(qmax)), "swb_set_ext_bins")
+
+    def ext_bins(self) -> list:
+        arr = (C.c_int32 * 16)()
+        n = C.c_int()
+        _check(self.lib.swb_get_ext_bins(self.h, arr, 16, C.byref(n)), "swb_get_ext_bins")
+        return list(arr[: n.value])
+
+    def tune_ext_bins(self, sc: Scoring, bases: np.ndarray, tasks: np.ndarray) -> dict:
+        """Autotune the length classes on a sample batch; the context keeps
+        the fastest.  -> {"bins", "ms", "default_ms"}."""
+        assert tasks.dtype == EXT_TASK_DTYPE
+        bases = np.ascontiguousarray(bases, dtype=np.uint8)
+        tasks = np.ascontiguousarray(tasks)
+        arr = (C.c_int32 * 16)()
+        n = C.c_int()
+        best, dflt = C.c_float(), C.c_float()
+        _check(self.lib.swb_tune_ext_bins(self.h, C.byref(sc), ptr(bases), bases.size, tasks.ctypes.data, len(tasks),
+                                          arr, 16, C.byref(n), C.byref(best), C.byref(dflt)), "swb_tune_ext_bins")
+        return {"bins": list(arr[: n.value]), "ms": best.value, "default_ms": dflt.value}
+
     def int16x2_alu_peak(self) -> float:
         """Packed 16-bit (s16x2 DPX add+max) lane operations/s."""
         v = C.c_double()

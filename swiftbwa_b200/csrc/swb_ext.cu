@@ -39,7 +39,11 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
+#include <mutex>
+#include <set>
+#include <string>
 #include <thread>
+#include <utility>
 #include <vector>
 
 #include "swb_device.cuh"
@@ -51,14 +55,13 @@
 namespace swb {
 namespace {
 
-// Bins 0-9: int8 rows (score bound <= 255), 10-19: int16 rows, by query
-// length class; bin 20: int32 rows in global scratch.
-constexpr int kLenClasses = 10;
-__device__ __constant__ int kFastQDev[kLenClasses] = {32, 48, 64, 80, 96, 112, 128, 160, 192, 256};
-constexpr int kFastBins = 2 * kLenClasses;
-constexpr int kBigBin = kFastBins;
-constexpr int kNumBins = kFastBins + 1;
+// Bins for n length classes (ExtBins, from the context): 0..n-1 int8 rows
+// (score bound <= 255), n..2n-1 int16 rows, by query-length class; bin 2n:
+// int32 rows (one warp per extension, or global scratch above kWarpMaxQ).
 constexpr int kFastT = 32;                // threads per block in the shared-memory kernels
+// Per pass: bin bounds (up to 32 words), the int32 bin's longest query at
+// byte 256, the bins' claim counters from byte 320.
+constexpr size_t kMiscBytes = 512;
 constexpr int kBigT = 64;
 
 // True when every H/E of the task fits one byte: H <= h0 + qlen*maxMat.
@@ -68,33 +71,35 @@ __device__ __forceinline__ bool fits8(int qlen, int h0, int max_mat) {
 
 // pair_ok: the gap costs fit a 16-bit lane (the two-row kernels of both row
 // widths); otherwise every task takes the int32 bin.
-__device__ __forceinline__ int ext_bin(const swb_ext_task &t, int max_mat, bool pair_ok, uint32_t warp_cells) {
+__device__ __forceinline__ int ext_bin(const swb_ext_task &t, int max_mat, bool pair_ok, uint32_t warp_cells,
+                                       const ExtBins &bins) {
     if (t.qlen <= 0 || t.tlen <= 0) return 0;
-    if (!pair_ok || t.qlen > kExtSmemMaxQ || !fits16(t.qlen, t.h0, max_mat)) return kBigBin;
-    if (warp_cells && (unsigned long long)t.qlen * (unsigned long long)t.tlen > warp_cells) return kBigBin;
+    const int big = 2 * bins.n;
+    if (!pair_ok || t.qlen > bins.q[bins.n - 1] || !fits16(t.qlen, t.h0, max_mat)) return big;
+    if (warp_cells && (unsigned long long)t.qlen * (unsigned long long)t.tlen > warp_cells) return big;
     int b = 0;
-    while (t.qlen > kFastQDev[b]) ++b;
-    return fits8(t.qlen, t.h0, max_mat) ? b : kLenClasses + b;
+    while (t.qlen > bins.q[b]) ++b;
+    return fits8(t.qlen, t.h0, max_mat) ? b : bins.n + b;
 }
 
 // Sort key: bin in bits 27-31, then query and target length, longest first.
 __global__ void ext_keys_kernel(const swb_ext_task *__restrict__ tasks, size_t n, int max_mat, int pair_ok,
-                                uint32_t warp_cells, uint32_t *__restrict__ keys, uint32_t *__restrict__ idx,
-                                int *__restrict__ big_max_q) {
+                                uint32_t warp_cells, ExtBins bins, uint32_t *__restrict__ keys,
+                                uint32_t *__restrict__ idx, int *__restrict__ big_max_q) {
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const swb_ext_task t = tasks[i];
-    const int b = ext_bin(t, max_mat, pair_ok != 0, warp_cells);
+    const int b = ext_bin(t, max_mat, pair_ok != 0, warp_cells, bins);
     const uint32_t q = (uint32_t)min(max(t.qlen, 0), 4095);
     const uint32_t tl = (uint32_t)min(max(t.tlen, 0), 32767);
     // Within a bin the longest tasks come first: they are claimed first, so
     // they overlap the rest instead of finishing the bin alone.
     keys[i] = ((uint32_t)b << 27) | ((4095u - q) << 15) | (32767u - tl);
     idx[i] = (uint32_t)i;
-    if (b == kBigBin) atomicMax(big_max_q, t.qlen);
+    if (b == 2 * bins.n) atomicMax(big_max_q, t.qlen);
 }
 
-// bin_start[b] = first sorted position whose bin >= b; bin_start[kNumBins] = n.
+// bin_start[b] = first sorted position whose bin >= b; bin_start[nbins] = n.
 __global__ void bin_bounds_kernel(const uint32_t *__restrict__ sorted_keys, size_t n,
                                   uint32_t *__restrict__ bin_start, int nbins) {
     const size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -110,13 +115,17 @@ __global__ void bin_bounds_kernel(const uint32_t *__restrict__ sorted_keys, size
         for (int bb = b + 1; bb <= nbins; ++bb) bin_start[bb] = (uint32_t)n;
 }
 
+// QMAX > 0: the class bound as a constant (the multiples of 16 from 32 to
+// 256); QMAX = 0: any other bound, passed in qcap.
 template <int QMAX, int T, bool U8>
-__global__ void __launch_bounds__(T) ext_fast_kernel(ExtArgs a, int bin) {
+__global__ void __launch_bounds__(T) ext_fast_kernel(ExtArgs a, int bin, int qcap_arg) {
     extern __shared__ uint32_t sm[];
-    // Rows: (QMAX + 1) words of 2 (int8 scores) or 4 bytes (int16), then QMAX query bytes.
+    // Rows: (qcap + 1) words of 2 (int8 scores) or 4 bytes (int16), then qcap
+    // query bytes; qcap is the bin's class bound (the rows' only use of it).
+    const int qcap = QMAX > 0 ? QMAX : qcap_arg;
     uint16_t *he16 = reinterpret_cast<uint16_t *>(sm) + threadIdx.x;
     uint32_t *he32 = sm + threadIdx.x;
-    uint8_t *qc = reinterpret_cast<uint8_t *>(sm) + (size_t)(QMAX + 1) * T * (U8 ? 2 : 4) + threadIdx.x;
+    uint8_t *qc = reinterpret_cast<uint8_t *>(sm) + (size_t)(qcap + 1) * T * (U8 ? 2 : 4) + threadIdx.x;
     static_assert(T == 32, "one warp per block: the warp claims its tasks together");
     const uint32_t lo = a.bin_start[bin], hi = a.bin_start[bin + 1];
     unsigned long long cells = 0;
@@ -150,19 +159,19 @@ __global__ void __launch_bounds__(T) ext_fast_kernel(ExtArgs a, int bin) {
 // Queries above 256 bases or scores beyond int16, up to kWarpMaxQ bases: one
 // warp per extension (swb_ext_warp.cuh), rows in shared memory, warps claim
 // tasks of the bin one at a time.
-__global__ void __launch_bounds__(256) ext_warp_kernel(ExtArgs a, int qcap) {
+__global__ void __launch_bounds__(256) ext_warp_kernel(ExtArgs a, int bin, int qcap) {
     extern __shared__ __align__(16) uint8_t wsm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const size_t stride = ((size_t)(qcap + 1) * 8 + (size_t)qcap + 15) & ~(size_t)15;
     int *h = reinterpret_cast<int *>(wsm + warp * stride);
     int *e = h + (qcap + 1);
     uint8_t *qc = reinterpret_cast<uint8_t *>(e + (qcap + 1));
-    const uint32_t lo = a.bin_start[kBigBin], hi = a.bin_start[kBigBin + 1];
+    const uint32_t lo = a.bin_start[bin], hi = a.bin_start[bin + 1];
     const uint32_t span = hi - lo;
     unsigned long long cells = 0;
     for (;;) {
         uint32_t k = 0;
-        if (lane == 0) k = atomicAdd(a.claim + kBigBin, 1u);
+        if (lane == 0) k = atomicAdd(a.claim + bin, 1u);
         k = __shfl_sync(0xFFFFFFFFu, k, 0);
         if (k >= span) break;
         const uint32_t ti = a.order[lo + k];
@@ -173,14 +182,14 @@ __global__ void __launch_bounds__(256) ext_warp_kernel(ExtArgs a, int qcap) {
         if (lane == 0) a.out[ti] = r;
         __syncwarp();
     }
-    add_cells(a.cells + kCntExtBin0 + kBigBin, cells);
+    add_cells(a.cells + kCntExtBin0 + bin, cells);
 }
 
 // Queries above kWarpMaxQ: one thread per extension over int32 rows in
 // global scratch (tasks with qlen <= skip_le belong to the warp kernel).
-__global__ void __launch_bounds__(kBigT) ext_global_kernel(ExtArgs a, int *h, int *e, uint8_t *q,
+__global__ void __launch_bounds__(kBigT) ext_global_kernel(ExtArgs a, int bin, int *h, int *e, uint8_t *q,
                                                            size_t nslots, int skip_le) {
-    const uint32_t lo = a.bin_start[kBigBin], hi = a.bin_start[kBigBin + 1];
+    const uint32_t lo = a.bin_start[bin], hi = a.bin_start[bin + 1];
     const size_t slot = blockIdx.x * (size_t)kBigT + threadIdx.x;
     Global32 st{h, e, q, nslots, slot};
     unsigned long long cells = 0;
@@ -197,48 +206,70 @@ __global__ void __launch_bounds__(kBigT) ext_global_kernel(ExtArgs a, int *h, in
             a.out[ti] = r;
         }
     }
-    add_cells(a.cells + kCntExtBin0 + kBigBin, cells);
+    add_cells(a.cells + kCntExtBin0 + bin, cells);
 }
 
-template <int QMAX, bool U8>
-constexpr size_t fast_smem_bytes() {
-    // A 16-bit (int8 scores) or 32-bit (int16) word and a query byte per column.
-    return ((size_t)(QMAX + 1) * kFastT * (U8 ? sizeof(uint16_t) : sizeof(uint32_t)) + (size_t)QMAX * kFastT + 15) &
+// A 16-bit (int8 scores) or 32-bit (int16) word and a query byte per column.
+size_t fast_smem_bytes(int qcap, bool u8) {
+    return ((size_t)(qcap + 1) * kFastT * (u8 ? sizeof(uint16_t) : sizeof(uint32_t)) + (size_t)qcap * kFastT + 15) &
            ~(size_t)15;
 }
 
-const char *const kBinNames[kNumBins] = {
-    "ext_u8_q32",  "ext_u8_q48",  "ext_u8_q64",  "ext_u8_q80",  "ext_u8_q96",  "ext_u8_q112",  "ext_u8_q128",
-    "ext_u8_q160", "ext_u8_q192", "ext_u8_q256", "ext_i16_q32", "ext_i16_q48", "ext_i16_q64",  "ext_i16_q80",
-    "ext_i16_q96", "ext_i16_q112", "ext_i16_q128", "ext_i16_q160", "ext_i16_q192", "ext_i16_q256",
-    "ext_big_i32"};
+// Profile names of the bins, kept for the life of the process.
+const char *bin_name(bool u8, int qcap) {
+    static std::mutex mu;
+    static std::set<std::string> names;
+    std::lock_guard<std::mutex> lk(mu);
+    return names.insert(std::string(u8 ? "ext_u8_q" : "ext_i16_q") + std::to_string(qcap)).first->c_str();
+}
 
-template <int QMAX, bool U8>
-int launch_fast(swb_ctx *ctx, const ExtArgs &a, int bin, size_t n, cudaStream_t s) {
-    static int occ = -1;
-    constexpr size_t smem = fast_smem_bytes<QMAX, U8>();
+using FastKernel = void (*)(ExtArgs, int, int);
+
+template <bool U8, int... Q>
+FastKernel fast_kernel_for(int qcap, std::integer_sequence<int, Q...>) {
+    FastKernel k = ext_fast_kernel<0, kFastT, U8>;
+    ((qcap == 32 + 16 * Q ? (void)(k = ext_fast_kernel<32 + 16 * Q, kFastT, U8>) : (void)0), ...);
+    return k;
+}
+
+// The kernel instance for a class bound: the constant-bound one for the
+// multiples of 16 from 32 to 256, else the runtime-bound one.
+FastKernel fast_kernel(bool u8, int qcap) {
+    return u8 ? fast_kernel_for<true>(qcap, std::make_integer_sequence<int, 15>{})
+              : fast_kernel_for<false>(qcap, std::make_integer_sequence<int, 15>{});
+}
+
+// Resident one-warp blocks per SM of the shared-memory kernel for a class bound.
+int fast_occupancy(bool u8, int qcap) {
+    static int cache[2][kExtSmemMaxQ + 1];
+    static std::once_flag once;
+    std::call_once(once, [] {
+        for (auto &row : cache)
+            for (int &v : row) v = -1;
+    });
+    int &occ = cache[u8 ? 1 : 0][qcap];
     if (occ < 0) {
-        SWB_CUDA(cudaFuncSetAttribute(ext_fast_kernel<QMAX, kFastT, U8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
-        SWB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ext_fast_kernel<QMAX, kFastT, U8>, kFastT, smem));
-        if (occ < 1) occ = 1;
+        int o = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fast_kernel(u8, qcap), kFastT, fast_smem_bytes(qcap, u8)) !=
+            cudaSuccess)
+            return -1;
+        occ = o < 1 ? 1 : o;
     }
+    return occ;
+}
+
+int launch_fast(swb_ctx *ctx, const ExtArgs &a, int bin, bool u8, int qcap, size_t n, cudaStream_t s) {
+    const int occ = fast_occupancy(u8, qcap);
+    if (occ < 0) return check_cuda(cudaGetLastError(), "occupancy query");
     const size_t grid = std::min<size_t>((n + kFastT - 1) / kFastT, (size_t)ctx->sm_count * occ);
     if (grid == 0) return SWB_OK;
-    ProfScope ps(ctx, s, kBinNames[bin], kCntExtBin0 + bin);
-    ext_fast_kernel<QMAX, kFastT, U8><<<(unsigned)grid, kFastT, smem, s>>>(a, bin);
+    const size_t smem = fast_smem_bytes(qcap, u8);
+    ProfScope ps(ctx, s, ctx->prof_on ? bin_name(u8, qcap) : nullptr, kCntExtBin0 + bin);
+    fast_kernel(u8, qcap)<<<(unsigned)grid, kFastT, smem, s>>>(a, bin, qcap);
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
     return SWB_OK;
 }
-
-using FastLauncher = int (*)(swb_ctx *, const ExtArgs &, int, size_t, cudaStream_t);
-const FastLauncher kFastLaunch[kFastBins] = {
-    launch_fast<32, true>,   launch_fast<48, true>,   launch_fast<64, true>,  launch_fast<80, true>,
-    launch_fast<96, true>,   launch_fast<112, true>,  launch_fast<128, true>, launch_fast<160, true>,
-    launch_fast<192, true>,  launch_fast<256, true>,  launch_fast<32, false>, launch_fast<48, false>,
-    launch_fast<64, false>,  launch_fast<80, false>,  launch_fast<96, false>, launch_fast<112, false>,
-    launch_fast<128, false>, launch_fast<160, false>, launch_fast<192, false>, launch_fast<256, false>};
 
 }  // namespace
 
@@ -250,7 +281,7 @@ int ext_reserve(swb_ctx *ctx, size_t cap) {
                                              (uint32_t *)nullptr, (uint32_t *)nullptr, (int)cap, 0, 32, ctx->stream));
     if ((rc = ensure_dev(ctx, ctx->d_keys, cap * 4)) || (rc = ensure_dev(ctx, ctx->d_keys2, cap * 4)) ||
         (rc = ensure_dev(ctx, ctx->d_idx, cap * 4)) || (rc = ensure_dev(ctx, ctx->d_idx2, 2 * cap * 4)) ||
-        (rc = ensure_dev(ctx, ctx->d_misc, 512)) || (rc = ensure_dev(ctx, ctx->d_sort_tmp, tmp_bytes)))
+        (rc = ensure_dev(ctx, ctx->d_misc, 2 * kMiscBytes)) || (rc = ensure_dev(ctx, ctx->d_sort_tmp, tmp_bytes)))
         return rc;
     return SWB_OK;
 }
@@ -270,22 +301,26 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     const int slot = pipe ? pipe->slot : 0;
     if ((rc = ensure_dev(ctx, ctx->d_keys, n * 4)) || (rc = ensure_dev(ctx, ctx->d_keys2, n * 4)) ||
         (rc = ensure_dev(ctx, ctx->d_idx, n * 4)) || (rc = ensure_dev(ctx, ctx->d_idx2, (slot + 1) * set * 4)) ||
-        (rc = ensure_dev(ctx, ctx->d_misc, (slot + 1) * 256)))
+        (rc = ensure_dev(ctx, ctx->d_misc, (slot + 1) * kMiscBytes)))
         return rc;
+    // The context's length classes at the time of the call: the keys and the
+    // launches below use the same copy.
+    const ExtBins bins = ctx->ext_bins;
+    const int nbins = 2 * bins.n + 1, big = 2 * bins.n;
     uint32_t *keys = (uint32_t *)ctx->d_keys.p, *keys2 = (uint32_t *)ctx->d_keys2.p;
     uint32_t *idx = (uint32_t *)ctx->d_idx.p, *idx2 = (uint32_t *)ctx->d_idx2.p + (size_t)slot * set;
-    char *misc = (char *)ctx->d_misc.p + slot * 256;
-    uint32_t *bin_start = (uint32_t *)misc;                   // kNumBins+1 words
-    int *big_max_q = (int *)(misc + 128);
-    uint32_t *claim = (uint32_t *)(misc + 160);               // kNumBins claim counters
-    SWB_CUDA(cudaMemsetAsync(big_max_q, 0, 128, s));                  // big_max_q and the counters
+    char *misc = (char *)ctx->d_misc.p + slot * kMiscBytes;
+    uint32_t *bin_start = (uint32_t *)misc;                   // nbins + 1 words
+    int *big_max_q = (int *)(misc + 256);
+    uint32_t *claim = (uint32_t *)(misc + 320);               // nbins claim counters
+    SWB_CUDA(cudaMemsetAsync(misc + 256, 0, kMiscBytes - 256, s));   // big_max_q and the counters
     const unsigned tb = 256;
     {
         ProfScope ps(ctx, s, "ext_keys", -1);
         // Two target rows per pass on 16-bit lanes: the gap costs must fit a lane.
         const int pair_ok = sc.o_del + sc.e_del <= 32767 && sc.o_ins + sc.e_ins <= 32767;
-        ext_keys_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(d_tasks, n, sc.max_mat, pair_ok, warp_cells, keys,
-                                                                       idx, big_max_q);
+        ext_keys_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(d_tasks, n, sc.max_mat, pair_ok, warp_cells, bins,
+                                                                       keys, idx, big_max_q);
     }
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
@@ -299,7 +334,7 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     }
     {
         ProfScope ps(ctx, s, "bin_bounds", -1);
-        bin_bounds_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(keys2, n, bin_start, kNumBins);
+        bin_bounds_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(keys2, n, bin_start, nbins);
     }
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
@@ -336,21 +371,21 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     const cudaStream_t js = pipe ? pipe->join : s;
     ProfScope pass(ctx, s, pipe ? nullptr : "ext_pass", -1);   // fork to join, on the launching stream
     SWB_CUDA(cudaEventRecord(ctx->fork_ev, s));
-    for (int b = 0; b < kNumBins; ++b) {
+    for (int b = 0; b < nbins; ++b) {
         cudaStream_t sb = ctx->side[b];
         SWB_CUDA(cudaStreamWaitEvent(sb, ctx->fork_ev, 0));
-        if (b < kFastBins) {
-            if ((rc = kFastLaunch[b](ctx, a, b, n, sb))) return rc;
+        if (b < big) {
+            if ((rc = launch_fast(ctx, a, b, b < bins.n, bins.q[b % bins.n], n, sb))) return rc;
         } else if (max_q > 0) {
-            ProfScope ps(ctx, sb, kBinNames[kBigBin], kCntExtBin0 + kBigBin);
-            ext_warp_kernel<<<(unsigned)wblocks, wwarps * 32, wwarps * wstride, sb>>>(a, wq);
+            ProfScope ps(ctx, sb, "ext_big_i32", kCntExtBin0 + big);
+            ext_warp_kernel<<<(unsigned)wblocks, wwarps * 32, wwarps * wstride, sb>>>(a, big, wq);
             ctx->launches++;
             SWB_CUDA(cudaGetLastError());
             if (max_q > kWarpMaxQ) {
                 int *hbuf = (int *)ctx->d_scratch.p;
                 int *ebuf = hbuf + cols * nslots;
                 uint8_t *qbuf = (uint8_t *)(ebuf + cols * nslots);
-                ext_global_kernel<<<(unsigned)(nslots / kBigT), kBigT, 0, sb>>>(a, hbuf, ebuf, qbuf, nslots, wq);
+                ext_global_kernel<<<(unsigned)(nslots / kBigT), kBigT, 0, sb>>>(a, big, hbuf, ebuf, qbuf, nslots, wq);
                 ctx->launches++;
                 SWB_CUDA(cudaGetLastError());
             }
@@ -362,14 +397,16 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
 }
 
 // Host-side twin of the device bin test: the longest query among
-// tasks[lo, hi) that the int32 bin takes (sizes its kernels' rows).
-int ext_big_max_q_range(const swb_ext_task *tasks, size_t lo, size_t hi, const DevScoring &sc) {
+// tasks[lo, hi) that the int32 bin takes under the context's length classes
+// (sizes its kernels' rows).
+int ext_big_max_q_range(const swb_ctx *ctx, const swb_ext_task *tasks, size_t lo, size_t hi, const DevScoring &sc) {
     const bool pair_ok = sc.o_del + sc.e_del <= 32767 && sc.o_ins + sc.e_ins <= 32767;
+    const int top = ctx->ext_bins.q[ctx->ext_bins.n - 1];
     int m = 0;
     for (size_t i = lo; i < hi; ++i) {
         const swb_ext_task &t = tasks[i];
         if (t.qlen <= 0 || t.tlen <= 0) continue;
-        if (!pair_ok || t.qlen > kExtSmemMaxQ || !fits16(t.qlen, t.h0, sc.max_mat)) m = t.qlen > m ? t.qlen : m;
+        if (!pair_ok || t.qlen > top || !fits16(t.qlen, t.h0, sc.max_mat)) m = t.qlen > m ? t.qlen : m;
     }
     return m;
 }

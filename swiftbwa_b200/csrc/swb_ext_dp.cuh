@@ -16,17 +16,10 @@ struct ExtArgs {
     const swb_ext_task *tasks;
     swb_ext_result *out;
     const uint32_t *order;      // sorted task indices
-    const uint32_t *bin_start;  // kNumBins + 1 entries
+    const uint32_t *bin_start;  // bins + 1 entries
     unsigned long long *cells;
     uint32_t *claim = nullptr;  // per-bin claim counters (zeroed per pass)
 };
-
-// True when every H/E of the task fits int16: H <= h0 + qlen*maxMat
-// (each row adds at most the best match score) and E, F <= H.
-__device__ __host__ __forceinline__ bool fits16(int qlen, int h0, int max_mat) {
-    long long hi = (long long)h0 + (long long)qlen * (max_mat > 0 ? max_mat : 0);
-    return h0 >= 0 && hi <= 32000;
-}
 
 // ---------------------------------------------------------------- row stores
 // 16-bit store: one word per column, H low half, E high half, in shared memory.

@@ -40,16 +40,34 @@ inline DevScoring make_dev_scoring(const swb_scoring &s) {
     return d;
 }
 
+// True when every H/E of an extension task fits int16: H <= h0 + qlen*maxMat
+// (each row adds at most the best match score) and E, F <= H.
+__device__ __host__ __forceinline__ bool fits16(int qlen, int h0, int max_mat) {
+    long long hi = (long long)h0 + (long long)qlen * (max_mat > 0 ? max_mat : 0);
+    return h0 >= 0 && hi <= 32000;
+}
+
 // Cell counters: one per kernel family (indices below) in ctx->d_counters.
 enum CounterIdx {
-    kCntExtBin0 = 0,      // extension bins 0..20 -> 0..20
-    kCntGlobal = 24,
-    kCntLocalStriped = 25,
-    kCntLocalScalar = 26,
-    kNumCounters = 32
+    kCntExtBin0 = 0,      // extension bins 0..30 -> 0..30
+    kCntGlobal = 32,
+    kCntLocalStriped = 33,
+    kCntLocalScalar = 34,
+    kNumCounters = 40
 };
 
-constexpr int kSideStreams = 24;   // concurrent bin launches per context
+// Extension length classes: query-length upper bounds of the shared-memory
+// bins, ascending; each class has an int8-row and an int16-row bin, and one
+// more bin takes everything else (int32 rows).  The bin index sits in 5 bits
+// of the sort key, so 2 * 15 + 1 = 31 bins at most.
+constexpr int kMaxLenClasses = 15;
+constexpr int kMaxExtBins = 2 * kMaxLenClasses + 1;
+struct ExtBins {
+    int n = 10;
+    int q[kMaxLenClasses] = {32, 48, 64, 80, 96, 112, 128, 160, 192, 256};
+};
+
+constexpr int kSideStreams = 32;   // concurrent bin launches per context
 constexpr int kMaxChunks = 16;     // pipelined chunks of one synchronous batch call
 
 // ------------------------------------------------------------ a device arena
@@ -96,6 +114,7 @@ struct swb_ctx {
     unsigned long long last_cells = 0;
     // per-kernel profiling
     unsigned long long *d_counters = nullptr;   // swb::kNumCounters cells counters
+    swb::ExtBins ext_bins;   // extension length classes (swb_set_ext_bins / swb_tune_ext_bins)
     bool prof_on = false;
     struct ProfRec {
         const char *name;

@@ -19,7 +19,7 @@
 
 namespace swb {
 
-int ext_big_max_q_range(const swb_ext_task *tasks, size_t lo, size_t hi, const DevScoring &sc);
+int ext_big_max_q_range(const swb_ctx *ctx, const swb_ext_task *tasks, size_t lo, size_t hi, const DevScoring &sc);
 
 static thread_local std::string g_last_error;
 
@@ -245,6 +245,69 @@ ProfScope::~ProfScope() {
 
 using namespace swb;
 
+namespace {
+
+// Candidate length-class sets for a batch: the defaults, uniform steps, and
+// quantiles of the shared-memory bins' query lengths by task count and by
+// estimated cells (qlen * min(tlen, 2w+1)), 6 to 15 classes, bounds rounded
+// up to multiples of 8 and the last one covering the longest such query.
+std::vector<ExtBins> ext_bin_candidates(const swb_ext_task *tasks, size_t n, const DevScoring &sc) {
+    std::vector<ExtBins> out;
+    auto add = [&](std::vector<int> q) {
+        std::sort(q.begin(), q.end());
+        q.erase(std::unique(q.begin(), q.end()), q.end());
+        if (q.empty() || (int)q.size() > kMaxLenClasses) return;
+        ExtBins b;
+        b.n = (int)q.size();
+        for (int k = 0; k < b.n; ++k) b.q[k] = q[k];
+        for (const ExtBins &o : out)
+            if (o.n == b.n && std::equal(o.q, o.q + o.n, b.q)) return;
+        out.push_back(b);
+    };
+    const ExtBins dflt;
+    add(std::vector<int>(dflt.q, dflt.q + dflt.n));
+    std::vector<int> s16, s32;
+    for (int q = 32; q <= kExtSmemMaxQ; q += 16) s16.push_back(q);
+    for (int q = 32; q <= kExtSmemMaxQ; q += 32) s32.push_back(q);
+    add(s16);
+    add(s32);
+    const bool pair_ok = sc.o_del + sc.e_del <= 32767 && sc.o_ins + sc.e_ins <= 32767;
+    std::vector<std::pair<int, uint64_t>> ql;   // (qlen, estimated cells) of the shared-memory bins' tasks
+    const size_t step = std::max<size_t>(1, n / 200000);
+    for (size_t i = 0; i < n; i += step) {
+        const swb_ext_task &t = tasks[i];
+        if (t.qlen <= 0 || t.tlen <= 0 || !pair_ok || t.qlen > kExtSmemMaxQ || !fits16(t.qlen, t.h0, sc.max_mat)) continue;
+        const uint64_t band = 2 * (uint64_t)std::max(t.w, 0) + 1;
+        ql.push_back({t.qlen, (uint64_t)t.qlen * std::min<uint64_t>((uint64_t)t.tlen, band)});
+    }
+    if (ql.empty()) return out;
+    std::sort(ql.begin(), ql.end());
+    auto up8 = [](int q) { return std::min(kExtSmemMaxQ, std::max(16, (q + 7) / 8 * 8)); };
+    const int top = up8(ql.back().first);
+    uint64_t total = 0;
+    for (auto &x : ql) total += x.second;
+    for (int k : {6, 10, 15}) {
+        std::vector<int> by_n, by_c;
+        for (int j = 1; j < k; ++j) by_n.push_back(up8(ql[ql.size() * j / k].first));
+        uint64_t acc = 0;
+        int j = 1;
+        for (auto &x : ql) {
+            acc += x.second;
+            while (j < k && acc * (uint64_t)k >= total * (uint64_t)j) {
+                by_c.push_back(up8(x.first));
+                ++j;
+            }
+        }
+        by_n.push_back(top);
+        by_c.push_back(top);
+        add(by_n);
+        add(by_c);
+    }
+    return out;
+}
+
+}  // namespace
+
 extern "C" {
 
 void swb_scoring_default(swb_scoring *s) {
@@ -409,7 +472,7 @@ int swb_ext_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, siz
             if (a >= b) return;
             int mq, mt;
             if ((pt.code = validate_range(ctx, tasks, a, b, n_bases, &mq, &mt, &pt.err, &pt.code))) return;
-            pt.big_q = ext_big_max_q_range(tasks, a, b, dsc);
+            pt.big_q = ext_big_max_q_range(ctx, tasks, a, b, dsc);
             size_t m = 0;
             for (size_t i = a; i < b; ++i) {
                 const swb_ext_task &tk = tasks[i];
@@ -484,6 +547,97 @@ int swb_ext_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, siz
     SWB_CUDA(cudaStreamSynchronize(ctx->d2h));
     SWB_CUDA(cudaStreamSynchronize(ctx->stream));
     tm.collect();
+    return SWB_OK;
+}
+
+int swb_set_ext_bins(swb_ctx *ctx, const int32_t *qmax, int n) {
+    if (!ctx || !qmax) return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
+    if (n < 1 || n > kMaxLenClasses)
+        return set_error(SWB_ERR_INVALID_ARG, "between 1 and " + std::to_string(kMaxLenClasses) + " length classes");
+    ExtBins b;
+    b.n = n;
+    for (int k = 0; k < n; ++k) {
+        if (qmax[k] < 8 || qmax[k] > kExtSmemMaxQ || (k > 0 && qmax[k] <= qmax[k - 1]))
+            return set_error(SWB_ERR_INVALID_ARG, "length classes must ascend strictly within [8, 256]");
+        b.q[k] = qmax[k];
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->ext_bins = b;
+    return SWB_OK;
+}
+
+int swb_get_ext_bins(swb_ctx *ctx, int32_t *qmax, int cap, int *n) {
+    if (!ctx || !n || (!qmax && cap > 0)) return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    *n = ctx->ext_bins.n;
+    for (int k = 0; k < std::min(cap, ctx->ext_bins.n); ++k) qmax[k] = ctx->ext_bins.q[k];
+    return SWB_OK;
+}
+
+int swb_tune_ext_bins(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, size_t n_bases,
+                      const swb_ext_task *tasks, size_t n_tasks, int32_t *qmax_out, int cap, int *n_out,
+                      float *best_ms, float *default_ms) {
+    if (!ctx || !sc || (!tasks && n_tasks) || (!bases && n_bases)) return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
+    int rc;
+    if ((rc = validate_scoring(sc))) return rc;
+    {
+        int mq = 0, mt = 0, code = 0;
+        std::string err;
+        if ((rc = validate_range(ctx, tasks, 0, n_tasks, n_bases, &mq, &mt, &err, &code))) return set_error(rc, err);
+    }
+    const DevScoring dsc = make_dev_scoring(*sc);
+    const std::vector<ExtBins> cand = ext_bin_candidates(tasks, n_tasks, dsc);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    SWB_CUDA(cudaSetDevice(ctx->device));
+    const ExtBins keep = ctx->ext_bins;
+    float t_best = 0.f, t_default = 0.f;
+    ExtBins best = keep;
+    if (n_tasks > 0) {
+        const size_t bases_bytes = align256(std::max<size_t>(n_bases, 1));
+        if ((rc = ensure_dev(ctx, ctx->d_bases, bases_bytes + align256(n_tasks * sizeof(swb_ext_task)) + 256)) ||
+            (rc = ensure_dev(ctx, ctx->d_out, n_tasks * sizeof(swb_ext_result))))
+            return rc;
+        uint8_t *d_b = (uint8_t *)ctx->d_bases.p;
+        swb_ext_task *d_t = (swb_ext_task *)((char *)ctx->d_bases.p + bases_bytes);
+        if (n_bases) SWB_CUDA(cudaMemcpyAsync(d_b, bases, n_bases, cudaMemcpyHostToDevice, ctx->stream));
+        SWB_CUDA(cudaMemcpyAsync(d_t, tasks, n_tasks * sizeof(swb_ext_task), cudaMemcpyHostToDevice, ctx->stream));
+        t_best = 1e30f;
+        for (size_t c = 0; c < cand.size(); ++c) {
+            ctx->ext_bins = cand[c];
+            const int hint = ext_big_max_q_range(ctx, tasks, 0, n_tasks, dsc);
+            float ms = 1e30f;
+            for (int rep = 0; rep < 3; ++rep) {   // a warm-up run, then the better of two
+                float t = 0.f;
+                SWB_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
+                rc = launch_ext(ctx, dsc, d_b, d_t, n_tasks, (swb_ext_result *)ctx->d_out.p, ctx->d_counters, ctx->stream,
+                                hint);
+                if (rc) {
+                    ctx->ext_bins = keep;
+                    return rc;
+                }
+                SWB_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
+                SWB_CUDA(cudaEventSynchronize(ctx->ev_stop));
+                SWB_CUDA(cudaEventElapsedTime(&t, ctx->ev_start, ctx->ev_stop));
+                if (rep > 0 && t < ms) ms = t;
+            }
+            if (c == 0) t_default = ms;
+            if (ms < t_best) {
+                t_best = ms;
+                best = cand[c];
+            }
+        }
+        // Another set replaces the defaults only for a gain above the
+        // run-to-run spread (2 %).
+        if (!(t_best < 0.98f * t_default)) {
+            best = cand.front();
+            t_best = t_default;
+        }
+    }
+    ctx->ext_bins = best;
+    if (n_out) *n_out = best.n;
+    for (int k = 0; k < std::min(cap, best.n) && qmax_out; ++k) qmax_out[k] = best.q[k];
+    if (best_ms) *best_ms = t_best;
+    if (default_ms) *default_ms = t_default;
     return SWB_OK;
 }
 

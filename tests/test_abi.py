@@ -69,6 +69,10 @@ def test_null_arguments_are_rejected_without_crash(lib):
     v = C.c_double()
     assert lib.swb_int_alu_peak(None, C.byref(v)) == abi.SWB_ERR_INVALID_ARG
     assert lib.swb_int16x2_alu_peak(None, C.byref(v)) == abi.SWB_ERR_INVALID_ARG
+    q = (C.c_int32 * 2)(32, 64)
+    assert lib.swb_set_ext_bins(None, q, 2) == abi.SWB_ERR_INVALID_ARG
+    assert lib.swb_get_ext_bins(None, q, 2, C.byref(C.c_int())) == abi.SWB_ERR_INVALID_ARG
+    assert lib.swb_tune_ext_bins(None, C.byref(sc), None, 0, None, 0, None, 0, None, None, None) == abi.SWB_ERR_INVALID_ARG
     lib.swb_destroy(None)
 
 

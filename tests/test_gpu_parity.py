@@ -104,6 +104,53 @@ def test_ext_fuzz_int32_path(engine, oracle_mod):
     assert bad.size == 0, f"{bad.size} mismatches: {got[bad[:3]]} vs {exp[bad[:3]]}"
 
 
+@pytest.mark.parametrize("bins", [[64, 256], list(range(32, 257, 16)), [256], [8, 40, 100], [24, 200, 232]])
+def test_ext_length_classes(engine, oracle_mod, bins):
+    """Any set of length classes gives the oracle's results: coarse, fine,
+    one class, and low bounds that send long queries to the int32 bin."""
+    sc = Scoring.default()
+    d = gen.ext_tasks(2024, 3000, qmax=300, ref_len=5000)
+    engine.upload_reference(d["pac"], d["ref_bases"])
+    exp, cells = oracle_mod.ext_batch(sc, d["bases"], d["tasks"], pac=d["pac"], ref_bases=d["ref_bases"], n_threads=8)
+    default = engine.ext_bins()
+    try:
+        engine.set_ext_bins(bins)
+        assert engine.ext_bins() == bins
+        got = engine.ext_batch(sc, d["bases"], d["tasks"])
+        bad = _cmp_struct(got, exp, got.dtype.names)
+        assert bad.size == 0, f"{bins}: {bad.size} mismatches, first {bad[:5]}"
+        assert engine.last_batch_stats()[1] == cells
+    finally:
+        engine.set_ext_bins(default)
+
+
+def test_ext_bins_autotuner(engine, oracle_mod):
+    """The tuner keeps the fastest candidate, never slower than the defaults
+    on its sample, and results stay equal to the oracle under it."""
+    from swiftbwa_b200 import workloads as W
+    sc = Scoring.default()
+    wl = W.config2(n=200_000, ref_len=10_000_000)
+    engine.upload_reference(wl.ref.pac, wl.ref.n)
+    default = engine.ext_bins()
+    try:
+        assert default == [32, 48, 64, 80, 96, 112, 128, 160, 192, 256]
+        rep = engine.tune_ext_bins(sc, wl.bases, wl.tasks)
+        assert 1 <= len(rep["bins"]) <= 15 and rep["bins"] == sorted(set(rep["bins"]))
+        assert min(rep["bins"]) >= 8 and max(rep["bins"]) <= 256
+        assert engine.ext_bins() == rep["bins"]
+        assert 0 < rep["ms"] <= rep["default_ms"]
+        sub = slice(0, 20_000)
+        got = engine.ext_batch(sc, wl.bases, wl.tasks[sub])
+        exp, _ = oracle_mod.ext_batch(sc, wl.bases, wl.tasks[sub], pac=wl.ref.pac, ref_bases=wl.ref.n, n_threads=8)
+        assert np.array_equal(got, exp)
+        with pytest.raises(Exception):
+            engine.set_ext_bins([64, 32])          # not ascending
+        with pytest.raises(Exception):
+            engine.set_ext_bins([512])             # above the shared-memory rows' 256
+    finally:
+        engine.set_ext_bins(default)
+
+
 # Gap and mismatch costs high enough that long tasks leave the int16 rows.
 BIG_PENALTIES = dict(a=1, b=60, o_ins=50, e_ins=30, o_del=45, e_del=35)
 
