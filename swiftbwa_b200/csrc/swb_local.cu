@@ -58,8 +58,6 @@ __device__ __forceinline__ RowTable prof_table(const DevScoring &sc, uint32_t t,
     return r;
 }
 
-__device__ __forceinline__ int satsub(int a, int b) { return (a > b ? a : b) - b; }   // pmax(a,b) &- b
-
 __device__ __forceinline__ int seg_max16(int v) {
     v = max(v, __shfl_xor_sync(kFull, v, 8));
     v = max(v, __shfl_xor_sync(kFull, v, 4));
@@ -82,15 +80,17 @@ __device__ PassOut striped_pass(const LocalArgs &a, const swb_local_task &tk, bo
     const DevScoring &sc = a.sc;
     const int bias = sc.b & 0xFF;                        // UInt8(mismatchPenalty)
     const int gOE = (sc.o_ins + sc.e_ins) & 0xFF, gE = sc.e_ins & 0xFF;
+    // subs(max(subs(x, gOE), y), gE) over u8 values is max(x - gOE - gE, y - gE, 0).
+    const int gOEE = gOE + gE;
     const int sn = act ? (qLen + 15) / 16 : 0;
-    int qc[SN], H[SN], E[SN];
+    int qc[SN], H[SN], E[SN];   // qc: prmt selector of the query code (byte 5 = 0 fills the upper bytes)
 #pragma unroll
     for (int s = 0; s < SN; ++s) {
         const int j = s + lane * sn;
         uint32_t code = 5;
         if (act && s < sn && j < qLen)
             code = span_base(a.bases, a.pac, tk.q_off, rev ? (qLen - 1 - j) : j, tk.qlen, tk.flags, false);
-        qc[s] = (int)code;
+        qc[s] = (int)(code | 0x5550u);
         H[s] = 0;
         E[s] = 0;
     }
@@ -121,19 +121,15 @@ __device__ PassOut striped_pass(const LocalArgs &a, const swb_local_task &tk, bo
 #pragma unroll
         for (int s = 0; s < SN; ++s) {                   // :209-231
             if (s < sn) {
-                const int prof = (int)prmt(rt.lo, rt.hi, (uint32_t)qc[s] | 0x5550u) & 0xFF;
-                int hNew = (vH + prof) & 0xFF;
-                hNew = satsub(hNew, bias);
+                const int prof = (int)prmt(rt.lo, rt.hi, (uint32_t)qc[s]);     // score + bias, one byte
+                const int hRaw = (vH + prof) & 0xFF;
                 const int hPrev = H[s];
                 vH = hPrev;
-                const int eOpen = satsub(hPrev, gOE);
-                int eVal = max(eOpen, E[s]);
-                eVal = satsub(eVal, gE);
+                const int eVal = __viaddmax_s32_relu(hPrev, -gOEE, E[s] - gE);   // subs(max(subs(H, gOE), E), gE)
                 E[s] = eVal;
-                hNew = max(max(hNew, eVal), f);
+                const int hNew = __vimax3_s32(__viaddmax_s32(hRaw, -bias, 0), eVal, f);   // max(subs(h, bias), E, F)
                 H[s] = hNew;
-                const int fOpen = satsub(hNew, gOE);
-                f = satsub(max(fOpen, f), gE);
+                f = __viaddmax_s32_relu(hNew, -gOEE, f - gE);                   // subs(max(subs(H, gOE), F), gE)
             }
         }
         int corrF = __shfl_up_sync(kFull, f, 1, 16);     // lazy-F (:234-242)
@@ -149,8 +145,7 @@ __device__ PassOut striped_pass(const LocalArgs &a, const swb_local_task &tk, bo
             if (going && changed == 0) going = false;
             if (going) {
                 H[s] = newH;
-                const int fOpen = satsub(newH, gOE);
-                corrF = satsub(max(fOpen, corrF), gE);
+                corrF = __viaddmax_s32_relu(newH, -gOEE, corrF - gE);
             }
         }
         int m = 0;                                       // column max (:245-263)
