@@ -74,7 +74,10 @@ struct PassOut {
 // simdSWPass (:133-306) for one task per half-warp.  `act` is uniform per
 // half; the loop trip counts are uniform per warp so every shuffle/vote sees
 // all 32 lanes.  rev: read query/target reversed over their given lengths.
-template <int SN>
+// FULL: every active task of the warp has exactly SN stripes (the forward
+// pass always: tasks are binned by stripe count), so the stripe loops run
+// with a constant trip count; inactive half-warps stay at zero.
+template <int SN, bool FULL>
 __device__ PassOut striped_pass(const LocalArgs &a, const swb_local_task &tk, bool act, int qLen, int tLen,
                                 bool rev, int minSub, uint32_t *peaks, int lane, unsigned half_mask) {
     const DevScoring &sc = a.sc;
@@ -82,7 +85,7 @@ __device__ PassOut striped_pass(const LocalArgs &a, const swb_local_task &tk, bo
     const int gOE = (sc.o_ins + sc.e_ins) & 0xFF, gE = sc.e_ins & 0xFF;
     // subs(max(subs(x, gOE), y), gE) over u8 values is max(x - gOE - gE, y - gE, 0).
     const int gOEE = gOE + gE;
-    const int sn = act ? (qLen + 15) / 16 : 0;
+    const int sn = FULL ? SN : (act ? (qLen + 15) / 16 : 0);
     int qc[SN], H[SN], E[SN];   // qc: prmt selector of the query code (byte 5 = 0 fills the upper bytes)
 #pragma unroll
     for (int s = 0; s < SN; ++s) {
@@ -134,7 +137,7 @@ __device__ PassOut striped_pass(const LocalArgs &a, const swb_local_task &tk, bo
         }
         int corrF = __shfl_up_sync(kFull, f, 1, 16);     // lazy-F (:234-242)
         if (lane == 0) corrF = 0;
-        bool going = sn > 0;
+        bool going = act && sn > 0;
 #pragma unroll
         for (int s = 0; s < SN; ++s) {
             if (!__any_sync(kFull, going)) break;
@@ -220,12 +223,14 @@ __global__ void __launch_bounds__(kLT) local_striped_kernel(LocalArgs a, int bin
         swb_local_task tk{};
         if (act) tk = a.tasks[ti];
         const int minSub = clamp_min_sub(tk.min_sub_score);
-        PassOut fwd = striped_pass<SN>(a, tk, act, tk.qlen, tk.tlen, false, minSub, peaks, lane, half_mask);
+        PassOut fwd = striped_pass<SN, true>(a, tk, act, tk.qlen, tk.tlen, false, minSub, peaks, lane, half_mask);
         if (act && lane == 0) cells += (unsigned long long)tk.qlen * tk.tlen;
         const bool fwd_ok = act && !fwd.nil && fwd.score > 0;
         const int revQ = fwd.qEnd + 1, revT = fwd.tEnd + 1;
         const bool do_rev = fwd_ok && revQ > 0 && revT > 0;
-        PassOut rv = striped_pass<SN>(a, tk, do_rev, revQ, revT, true, 0, peaks, lane, half_mask);
+        const bool rev_full = __all_sync(kFull, !do_rev || (revQ + 15) / 16 == SN);
+        PassOut rv = rev_full ? striped_pass<SN, true>(a, tk, do_rev, revQ, revT, true, 0, peaks, lane, half_mask)
+                              : striped_pass<SN, false>(a, tk, do_rev, revQ, revT, true, 0, peaks, lane, half_mask);
         if (do_rev && lane == 0) cells += (unsigned long long)revQ * revT;
         if (act && lane == 0) {
             if (do_rev && !rv.nil) {
