@@ -58,6 +58,14 @@ __device__ __forceinline__ RowTable prof_table(const DevScoring &sc, uint32_t t,
     return r;
 }
 
+__device__ __forceinline__ int seg_min16(int v) {
+    v = min(v, __shfl_xor_sync(kFull, v, 8));
+    v = min(v, __shfl_xor_sync(kFull, v, 4));
+    v = min(v, __shfl_xor_sync(kFull, v, 2));
+    v = min(v, __shfl_xor_sync(kFull, v, 1));
+    return v;
+}
+
 __device__ __forceinline__ int seg_max16(int v) {
     v = max(v, __shfl_xor_sync(kFull, v, 8));
     v = max(v, __shfl_xor_sync(kFull, v, 4));
@@ -158,13 +166,43 @@ __device__ PassOut striped_pass(const LocalArgs &a, const swb_local_task &tk, bo
         const int colMax = seg_max16(m);
         if (live && colMax > 250) nil = true;
         const bool need = live && !nil && colMax > maxScore;
+        // The stripe walk below takes, among the stripes whose lane maximum
+        // sets a new running maximum, the last one where a real (non-padding)
+        // lane holds that maximum.  The last new maximum is colMax itself, at
+        // the first stripe fs whose lane maximum equals it; when a real lane
+        // holds colMax there, that is the answer (first such lane), found with
+        // one segment minimum and one ballot.  Otherwise (colMax only in
+        // padding lanes at fs) the walk runs.
+        bool walk = false;
         if (__any_sync(kFull, need)) {
+            int fs = SN;                                   // this lane's first stripe holding colMax
+#pragma unroll
+            for (int s = SN - 1; s >= 0; --s)
+                if (s < sn && H[s] == colMax) fs = s;
+            const int fsAll = seg_min16(fs);
+            int hAt = -1;
+#pragma unroll
+            for (int s = 0; s < SN; ++s)
+                if (s == fsAll) hAt = H[s];
+            const unsigned hit = __ballot_sync(kFull, need && hAt == colMax && fsAll + lane * sn < qLen) & half_mask;
+            if (need) {
+                if (hit) {
+                    maxScore = colMax;
+                    maxI = i;
+                    const int l = __ffs(hit) - 1 - ((half_mask & 1u) ? 0 : 16);
+                    maxJ = fsAll + l * sn;
+                } else {
+                    walk = true;
+                }
+            }
+        }
+        if (__any_sync(kFull, walk)) {
 #pragma unroll
             for (int s = 0; s < SN; ++s) {
                 const int lm = seg_max16(s < sn ? H[s] : 0);
                 const int j = s + lane * sn;
-                const unsigned hit = __ballot_sync(kFull, need && s < sn && H[s] == lm && j < qLen) & half_mask;
-                if (need && s < sn && lm > maxScore) {
+                const unsigned hit = __ballot_sync(kFull, walk && s < sn && H[s] == lm && j < qLen) & half_mask;
+                if (walk && s < sn && lm > maxScore) {
                     maxScore = lm;
                     maxI = i;
                     if (hit) {
