@@ -285,35 +285,38 @@ __device__ int global_dp_smem(const DevScoring &sc, const Row &row, const uint8_
         if (end > beg) cells += (unsigned long long)(end - beg);
         int hLeft = hBeg;
         uint32_t *zrow = zp.z + (size_t)i * rstride;
-        uint32_t word = 0;
-        int col = 0;
-        for (int j = beg; j < end; ++j, ++col) {
+        // One cell: H, E, F and its 4-bit backpointer code (bit 0: E extends,
+        // 1: F extends, 2: H from E, 3: H from F; ties as the reference).
+        // __vibmax_s32(a, b, &p) gives max(a, b) and p = (a >= b).
+        auto cell = [&](int j) -> uint32_t {
             int vh, ve;
             row.load(j + 1, vh, ve);
             int hCur = hDiag + row_score(rt, qs[j * T]);
             hDiag = vh;
-            const int eOpen = vh - oeDel;
-            const int eExtend = ve - eDel;
-            const uint32_t eFlag = eOpen > eExtend ? 0u : 1u;
-            const int eVal = eOpen > eExtend ? eOpen : eExtend;
-            const int fOpen = hLeft - oeIns;
-            const int fExtend = f - eIns;
-            const uint32_t fFlag = fOpen > fExtend ? 0u : 2u;
-            const int fVal = fOpen > fExtend ? fOpen : fExtend;
+            bool eExt, fExt, hKeepE, hKeepF;
+            const int eVal = __vibmax_s32(ve - eDel, vh - oeDel, &eExt);          // extend unless open > extend
+            const int fVal = __vibmax_s32(f - eIns, hLeft - oeIns, &fExt);
             f = fVal;
-            const uint32_t fromE = eVal > hCur ? 4u : 0u;
-            hCur = eVal > hCur ? eVal : hCur;
-            const uint32_t fromF = fVal > hCur ? 8u : 0u;
-            hCur = fVal > hCur ? fVal : hCur;
+            hCur = __vibmax_s32(hCur, eVal, &hKeepE);                              // from E when E > H
+            hCur = __vibmax_s32(hCur, fVal, &hKeepF);                              // from F when F > H
             row.store(j + 1, hCur, eVal);
             hLeft = hCur;
-            word |= (eFlag | fFlag | fromE | fromF) << ((col & 7) << 2);
-            if ((col & 7) == 7) {
-                zrow[(size_t)(col >> 3) * zp.nslots] = word;
-                word = 0;
-            }
+            return (eExt ? 1u : 0u) | (fExt ? 2u : 0u) | (hKeepE ? 0u : 4u) | (hKeepF ? 0u : 8u);
+        };
+        // Eight columns per backpointer word, with constant shifts.
+        int j = beg;
+        size_t zo = 0;
+        for (; j + 8 <= end; j += 8, zo += zp.nslots) {
+            uint32_t word = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) word |= cell(j + k) << (4 * k);
+            zrow[zo] = word;
         }
-        if (col & 7) zrow[(size_t)(col >> 3) * zp.nslots] = word;
+        if (j < end) {
+            uint32_t word = 0;
+            for (int k = 0; j < end; ++j, ++k) word |= cell(j) << (4 * k);
+            zrow[zo] = word;
+        }
     }
     const int thr = -(qlen + tlen + 2) * step_cost(sc) - 1;
     return row.final_score(row.getH(qlen), thr);                                 // :144
