@@ -448,13 +448,29 @@ int swb_ext_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, siz
     SWB_CUDA(cudaSetDevice(ctx->device));
     const DevScoring dsc = make_dev_scoring(*sc);
 
-    // Up to kMaxChunks chunks of at least 512K tasks.  The host checks chunk k
-    // (spans, the bases prefix it needs, the longest query of the int32 bin)
-    // while the GPU works on the chunks before it; chunk k starts once the
-    // prefix of `bases` its tasks reference is on the device.
+    // Chunks of at least 512K tasks: a short first one (1/16 of the batch, so
+    // the GPU starts after a short copy), then seven equal ones; smaller
+    // batches are up to eight equal chunks.  The host checks chunk k (spans,
+    // the bases prefix it needs, the longest query of the int32 bin) while the
+    // GPU works on the chunks before it; chunk k starts once the prefix of
+    // `bases` its tasks reference is on the device.
     const size_t kMinChunk = 1u << 19;
-    const size_t nchunks = std::min<size_t>(kMaxChunks, std::max<size_t>(1, n_tasks / kMinChunk));
-    const size_t per = (n_tasks + nchunks - 1) / nchunks;
+    std::vector<size_t> cb{0};   // chunk k is tasks[cb[k], cb[k + 1])
+    {
+        const size_t n16 = n_tasks / 16;
+        if (n16 >= kMinChunk) {
+            cb.push_back(n16);
+            const size_t per7 = (n_tasks - n16 + 6) / 7;
+            for (size_t k = 1; k <= 7; ++k) cb.push_back(std::min(n_tasks, n16 + k * per7));
+        } else {
+            const size_t m = std::min<size_t>(8, std::max<size_t>(1, n_tasks / kMinChunk)), p = (n_tasks + m - 1) / m;
+            for (size_t k = 1; k <= m; ++k) cb.push_back(std::min(n_tasks, k * p));
+        }
+    }
+    static_assert(kMaxChunks >= 8, "chunk events");
+    const size_t nchunks = cb.size() - 1;
+    size_t per = 0;   // the largest chunk (sizes the scratch sets)
+    for (size_t k = 0; k < nchunks; ++k) per = std::max(per, cb[k + 1] - cb[k]);
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     struct Part {
         int code = 0, big_q = 0;
@@ -512,7 +528,7 @@ int swb_ext_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, siz
     SWB_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->fork_ev, 0));
     size_t copied = 0, need = 0, last = 0;
     for (size_t k = 0; k < nchunks; ++k) {
-        const size_t lo = k * per, hi = std::min(n_tasks, lo + per);
+        const size_t lo = cb[k], hi = cb[k + 1];
         if (lo >= hi) break;
         int big_q = 0;
         if ((rc = scan_chunk(lo, hi, need, big_q))) {

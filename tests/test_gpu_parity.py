@@ -199,6 +199,21 @@ def test_ext_config_workloads_chunked(engine, oracle_mod):
         assert engine.last_batch_stats()[1] == cells
 
 
+def test_ext_large_batch_chunk_schedules(engine):
+    """A batch large enough for the host entry point's ramped chunks (a
+    short first chunk, then seven equal ones) gives the same results as its
+    two halves, each cut into equal chunks."""
+    from swiftbwa_b200 import workloads as W
+    sc = Scoring.default()
+    wl = W.config1(n_reads=4_300_000, ref_len=10_000_000)
+    assert len(wl.tasks) >= 16 * (1 << 19)
+    engine.upload_reference(wl.ref.pac, wl.ref.n)
+    whole = engine.ext_batch(sc, wl.bases, wl.tasks)
+    h = len(wl.tasks) // 2
+    parts = np.concatenate([engine.ext_batch(sc, wl.bases, wl.tasks[:h]), engine.ext_batch(sc, wl.bases, wl.tasks[h:])])
+    assert np.array_equal(whole, parts)
+
+
 @pytest.mark.parametrize("si", [0, 3])
 def test_cigar_generate_fuzz(engine, oracle_mod, si):
     """CIGARGenerator.generate: fast path, device DP with retries, squeeze,
