@@ -606,6 +606,15 @@ int swb_tune_ext_bins(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases,
     std::lock_guard<std::mutex> lk(ctx->mu);
     SWB_CUDA(cudaSetDevice(ctx->device));
     const ExtBins keep = ctx->ext_bins;
+    // Any early return (a failed CUDA call) puts the caller's classes back.
+    struct Restore {
+        swb_ctx *c;
+        ExtBins b;
+        bool on = true;
+        ~Restore() {
+            if (on) c->ext_bins = b;
+        }
+    } restore{ctx, keep};
     float t_best = 0.f, t_default = 0.f;
     ExtBins best = keep;
     if (n_tasks > 0) {
@@ -627,10 +636,7 @@ int swb_tune_ext_bins(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases,
                 SWB_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
                 rc = launch_ext(ctx, dsc, d_b, d_t, n_tasks, (swb_ext_result *)ctx->d_out.p, ctx->d_counters, ctx->stream,
                                 hint);
-                if (rc) {
-                    ctx->ext_bins = keep;
-                    return rc;
-                }
+                if (rc) return rc;
                 SWB_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
                 SWB_CUDA(cudaEventSynchronize(ctx->ev_stop));
                 SWB_CUDA(cudaEventElapsedTime(&t, ctx->ev_start, ctx->ev_stop));
@@ -649,6 +655,7 @@ int swb_tune_ext_bins(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases,
             t_best = t_default;
         }
     }
+    restore.on = false;
     ctx->ext_bins = best;
     if (n_out) *n_out = best.n;
     for (int k = 0; k < std::min(cap, best.n) && qmax_out; ++k) qmax_out[k] = best.q[k];
