@@ -465,10 +465,9 @@ extern "C" int swb_extend_chains(swb_ctx *ctx, const swb_scoring *sc, const uint
     region_counts_kernel<<<(unsigned)((nc + tb - 1) / tb), tb, 0, st>>>(d_state, (uint32_t)nc, d_counts);
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
-    if (n_seeds) SWB_CUDA(cudaMemcpyAsync(out, d_reg, n_seeds * sizeof(swb_region), cudaMemcpyDeviceToHost, st));
-    SWB_CUDA(cudaMemcpyAsync(n_regions, d_counts, nc * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    SWB_CUDA(cudaEventRecord(ctx->ev_stop, st));
-    SWB_CUDA(cudaStreamSynchronize(st));
+    if ((rc = d2h_staged(ctx, st, {DevSpan{d_reg, out, n_seeds * sizeof(swb_region)},
+                                   DevSpan{d_counts, n_regions, nc * sizeof(uint32_t)}}, ctx->ev_stop)))
+        return rc;
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) ctx->last_ms = ms;
     unsigned long long c[kNumCounters] = {0};

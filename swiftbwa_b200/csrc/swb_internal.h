@@ -2,6 +2,8 @@
 // libswb_cuda.so.  Not part of the public C ABI (include/swb_cuda.h).
 #pragma once
 
+#include <initializer_list>
+
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -147,6 +149,18 @@ struct ProfScope {
     ProfScope(swb_ctx *c, cudaStream_t st, const char *name, int counter);
     ~ProfScope();
 };
+
+// Downloads of a call's results into (pageable) caller arrays through the
+// context's pinned staging buffer: one async copy each into pinned memory,
+// then host threads unpack.  Synchronises `st` (recording after_copies, when
+// given, once the copies are queued).  Pageable downloads are much slower.
+struct DevSpan {
+    const void *dev;
+    void *dst;
+    size_t bytes;
+};
+void par_copy(void *dst, const void *src, size_t bytes);
+int d2h_staged(swb_ctx *ctx, cudaStream_t st, std::initializer_list<DevSpan> parts, cudaEvent_t after_copies = nullptr);
 
 // Grow-only allocation against the context budget.
 int ensure_dev(swb_ctx *ctx, DevBuf &b, size_t bytes);

@@ -179,6 +179,50 @@ struct Part {
     void **dev;
 };
 
+}  // namespace swb
+
+// Host memcpy on several host threads for large copies.
+void swb::par_copy(void *dst, const void *src, size_t bytes) {
+    const size_t kPart = 8u << 20;
+    const size_t nth = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), bytes / kPart);
+    if (nth <= 1) {
+        if (bytes) std::memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t per = (bytes + nth - 1) / nth;
+    std::vector<std::thread> th;
+    for (size_t t = 0; t < nth; ++t)
+        th.emplace_back([=] {
+            const size_t a = std::min(bytes, t * per), b = std::min(bytes, a + per);
+            if (b > a) std::memcpy((char *)dst + a, (const char *)src + a, b - a);
+        });
+    for (auto &x : th) x.join();
+}
+
+int swb::d2h_staged(swb_ctx *ctx, cudaStream_t st, std::initializer_list<DevSpan> parts, cudaEvent_t after_copies) {
+    size_t total = 0;
+    for (const DevSpan &p : parts) total += align256(p.bytes);
+    int rc;
+    if ((rc = ensure_host(ctx, ctx->h_out, std::max<size_t>(total, 256)))) return rc;
+    char *stage = (char *)ctx->h_out.p;
+    size_t off = 0;
+    for (const DevSpan &p : parts) {
+        if (p.bytes) SWB_CUDA(cudaMemcpyAsync(stage + off, p.dev, p.bytes, cudaMemcpyDeviceToHost, st));
+        off += align256(p.bytes);
+    }
+    if (after_copies) SWB_CUDA(cudaEventRecord(after_copies, st));
+    SWB_CUDA(cudaStreamSynchronize(st));
+    off = 0;
+    for (const DevSpan &p : parts) {
+        par_copy(p.dst, stage + off, p.bytes);
+        off += align256(p.bytes);
+    }
+    return SWB_OK;
+}
+
+namespace swb {
+
+// Inputs of one call into the context's device buffer.
 static int stage_in(swb_ctx *ctx, std::initializer_list<Part> parts) {
     size_t total = 0;
     for (const Part &p : parts) total += align256(p.bytes);
