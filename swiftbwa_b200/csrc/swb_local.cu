@@ -242,8 +242,9 @@ __device__ PassOut striped_pass(const LocalArgs &a, const swb_local_task &tk, bo
     return o;
 }
 
+// Five 128-thread blocks per SM (96 registers, no spills; six spill).
 template <int SN>
-__global__ void __launch_bounds__(kLT) local_striped_kernel(LocalArgs a, int bin, uint32_t *peaks_base,
+__global__ void __launch_bounds__(kLT, 5) local_striped_kernel(LocalArgs a, int bin, uint32_t *peaks_base,
                                                             int peak_stride) {
     const int lane = threadIdx.x & 15;
     const unsigned half_mask = (threadIdx.x & 16) ? 0xFFFF0000u : 0x0000FFFFu;
