@@ -2,40 +2,31 @@
 // BandedSWScalar.align (Sources/Alignment/BandedSWScalar.swift:21-191).
 //
 // Layout and schedule
-//   * One thread owns one extension and walks the Swift row loop literally,
-//     so the reference's storage semantics hold as written: cells outside
-//     the current band keep their stale values, h[end] receives the last H
-//     of the row, e[end] = 0, and band narrowing scans the words the Swift
-//     loop scans.
-//   * The DP row lives in shared memory as one 32-bit word per query column
-//     (H in the low half, E in the high half; both are >= 0 and below 32768
-//     for the tasks routed here), interleaved [column][thread] so that every
-//     access is bank-conflict free.  Beside it each column keeps the 16-bit
-//     prmt selector of its query base, so the score of a cell is one byte
-//     permute of the row's 8-byte score table with sign replication.
-//   * Per cell the recurrence is five fused integer ops:
-//         d   = relu(min(M + s, M << 7))   -- M ? M + s : 0, clamped at 0 (*)
-//         H   = max3(d, E, F)
-//         E'  = relu(max(E - eDel, d - oeDel))
-//         F'  = relu(max(F - eIns, d - oeIns))
-//         key = max(key, H << 16 | j)      -- row max, last j on ties
-//     (*) Clamping the diagonal at 0 changes no output: E and F are >= 0, so
-//     H = max(diag, E, F) is unchanged, and E', F' clamp at 0 anyway.
-//     M << 7 >= M + s for every M >= 1 because s <= a <= 127.
-//   * Tasks whose score bound h0 + qlen*maxScore is at most 255 (all
-//     short-read extensions with the default scoring) use int8 rows instead:
-//     one word per column holding the selector (low half), H and E (one
-//     byte each), so a cell needs one shared load and the row takes 4 bytes
-//     per column.  The bound is static, so the int8 rows never saturate and
-//     nothing is re-run.
-//   * Tasks are binned on the device by row width (int8 / int16) and query
-//     length (10 classes from 32 to 256 columns) and radix-sorted by
-//     (bin, qlen, tlen) so a warp's threads walk rows of similar shape; each
-//     bin's kernel is instantiated for its row size and launched on its own
-//     stream, so the bins overlap on the GPU.
-//   * Tasks whose scores could leave int16 (h0 + qlen*maxScore > 32000) or
-//     whose query exceeds 256 run the generic device function over int32
-//     rows in global scratch (swb_ext_dp.cuh).
+//   * Tasks are binned on the device by row width and query-length class:
+//     int8 rows when the score bound h0 + qlen*maxScore is at most 255,
+//     int16 rows when it is at most 32000, each in the context's length
+//     classes (ExtBins: up to 15 bounds, defaults 32..256, chosen by
+//     swb_tune_ext_bins); everything else (queries above the last bound,
+//     larger scores, gap costs beyond a 16-bit lane) goes to the int32 bin.
+//     The bounds are static, so no row ever saturates and nothing is re-run.
+//     A CUB radix sort orders the tasks by (bin, longest query, longest
+//     target).
+//   * Every shared-memory bin is one launch of a persistent grid of one-warp
+//     blocks; lane 0 claims the next 32 sorted tasks of the bin from a device
+//     counter, so long tasks start first and no block holds a bin up.  The
+//     bins run on their own streams and overlap.
+//   * One thread owns one extension and computes two target rows per pass in
+//     the 16-bit lanes of DPX s16x2 operations (swb_ext_pair.cuh), keeping the
+//     reference's row storage semantics (stale cells outside the band,
+//     h[end], the last-j row-max tie, z-drop, band narrowing).  The row lives
+//     in shared memory, [column][thread]: a 16-bit (int8 scores) or 32-bit
+//     (int16) H|E word and a query byte per column.  A class bound sizes only
+//     these rows; bounds that are multiples of 16 get a kernel instance with
+//     the bound as a constant.
+//   * The int32 bin runs one warp per extension for queries up to 4096
+//     (swb_ext_warp.cuh) and one thread per extension over int32 rows in
+//     global scratch above that (swb_ext_dp.cuh).
+
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>

@@ -32,8 +32,8 @@ __global__ void __launch_bounds__(256) alu_probe_kernel(int iters, int seed, int
 }
 
 // The same chains on packed 16-bit lanes: one DPX add+max per statement,
-// two lanes per instruction (the form the int8-bounded extension kernel
-// computes its two target rows in).
+// two lanes per instruction (the form the shared-memory extension kernels
+// compute their two target rows in).
 __global__ void __launch_bounds__(256) alu16x2_probe_kernel(int iters, int seed, int *sink) {
     uint32_t x[8], y[8];
 #pragma unroll
