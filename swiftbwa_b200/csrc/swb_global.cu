@@ -3,12 +3,16 @@
 // and, per task flag, CIGARGenerator.generate's band-doubling retry
 // (Sources/Alignment/CIGARGenerator.swift:88-96).
 //
-// One thread owns one alignment.  Its H/E rows (int32), staged query and
-// target, and the 4-bit backpointer matrix live in global scratch laid out
-// [index][slot] so the threads of a warp touch adjacent words/bytes.  The
-// backpointer matrix of the last attempt is walked by the same thread; ops
-// are written in traceback order into the task's CIGAR window, merged into
-// runs on the fly, and reversed in place at the end (CIGARBuilder.swift).
+// One thread owns one alignment.  Alignments are sorted by row width, then
+// largest shape first; queries up to 256 run global_smem_kernel (H/E rows in
+// shared memory, int16 where every value provably fits, else int32), whose
+// warps claim 32 sorted alignments at a time; longer queries run
+// global_kernel over rows in global scratch.  The 4-bit backpointers go to
+// global memory [row][word][slot], eight columns per word, so a warp's
+// threads touch adjacent words.  The backpointer matrix of the last attempt
+// is walked by the same thread; ops are written in traceback order into the
+// task's CIGAR window, merged into runs on the fly, and reversed in place at
+// the end (CIGARBuilder.swift).
 #include <type_traits>
 
 #include "swb_device.cuh"

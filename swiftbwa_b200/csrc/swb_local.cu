@@ -8,9 +8,11 @@
 // wavefront kernel would not match it.  Here a 16-thread half-warp plays
 // the 16 SIMD lanes: thread l keeps lane l of every stripe's H and E in
 // registers (the stripe count is a template parameter, one instantiation
-// per sn), the lane shifts are __shfl_up_sync within the half, per-stripe
-// lane maxima are butterfly reductions, and the lazy-F early break is a
-// ballot.  All arithmetic is the reference's u8 wrap/saturate arithmetic.
+// per sn, tasks binned by it), the lane shifts are __shfl_up_sync within the
+// half, the position of a new column maximum is a segment minimum and a
+// ballot, and the lazy-F early break is a ballot.  All arithmetic is the
+// reference's u8 wrap/saturate arithmetic, its saturating steps folded into
+// DPX add-max forms where that is exact.
 // Tasks the reference sends to its scalar int32 fallback (qLen*A > 250,
 // u8 overflow, a zero forward score, or a failed reverse pass) are
 // appended to a device list and finished by a one-thread-per-task kernel
