@@ -1,13 +1,16 @@
 """Builds libswb_cuda.so in-tree with nvcc for sm_100a.
 
-    python -m swiftbwa_b200.build [--debug]
+    python -m swiftbwa_b200.build [--debug] [--ptxas-v]
 
 The library is a plain C-ABI shared object (include/swb_cuda.h): no torch,
 no Python.  cudart is linked statically so the .so only needs the driver.
+Each .cu file compiles to its own object (in parallel, rebuilt when the file
+or any header is newer than the object) and one nvcc call links them.
 """
 from __future__ import annotations
 
 import argparse
+import concurrent.futures as cf
 import os
 import shutil
 import subprocess
@@ -15,9 +18,12 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "libswb_cuda.so")
-SOURCES = ["swb_runtime.cu", "swb_ext.cu", "swb_global.cu", "swb_local.cu", "swb_probe.cu", "swb_noalloc.cu", "swb_cigar.cu", "swb_serve.cu", "swb_extend.cu", "swb_rescue.cu"]
+SOURCES = ["swb_runtime.cu", "swb_ext.cu", "swb_global.cu", "swb_local.cu", "swb_probe.cu", "swb_noalloc.cu",
+           "swb_cigar.cu", "swb_serve.cu", "swb_extend.cu", "swb_rescue.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3"]
 
 
 def nvcc() -> str:
@@ -43,25 +49,46 @@ def build_workload() -> str:
     return WORKLOAD_OUT
 
 
+def _stale(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
 def build(debug: bool = False, verbose: bool = False, ptxas_v: bool = False) -> str:
     build_workload()
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
-    deps = srcs + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-    deps.append(os.path.join(HERE, "..", "include", "swb_cuda.h"))
-    if os.path.exists(OUT) and not debug and not ptxas_v:
-        t = os.path.getmtime(OUT)
-        if all(os.path.getmtime(d) <= t for d in deps):
-            return OUT
-    cmd = [nvcc(), *ARCH, "-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3",
-           "-shared", "-o", OUT + ".tmp", *srcs]
-    if debug:
-        cmd += ["-DSWB_DEBUG=1"]
-    if ptxas_v:
-        cmd += ["-Xptxas", "-v"]
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    subprocess.run(cmd, check=True)
-    os.replace(OUT + ".tmp", OUT)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    headers.append(os.path.join(HERE, "..", "include", "swb_cuda.h"))
+    force = debug or ptxas_v
+    if not force and not _stale(OUT, srcs + headers):
+        return OUT
+    os.makedirs(OBJ, exist_ok=True)
+    extra = (["-DSWB_DEBUG=1"] if debug else []) + (["-Xptxas", "-v"] if ptxas_v else [])
+    objs, jobs = [], []
+    for s in srcs:
+        o = os.path.join(OBJ, os.path.basename(s)[:-3] + ".o")
+        objs.append(o)
+        if force or _stale(o, [s, *headers]):
+            jobs.append([nvcc(), *ARCH, *FLAGS, *extra, "-c", "-o", o + ".tmp", s])
+
+    def run(cmd):
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        os.replace(cmd[cmd.index("-o") + 1], cmd[cmd.index("-o") + 1][:-4])
+
+    if jobs:
+        with cf.ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
+            for f in [ex.submit(run, j) for j in jobs]:
+                f.result()
+    if jobs or _stale(OUT, objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", OUT + ".tmp", *objs]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        os.replace(OUT + ".tmp", OUT)
     return OUT
 
 
