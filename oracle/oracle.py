@@ -13,7 +13,7 @@ import subprocess
 
 import numpy as np
 
-from swiftbwa_b200.abi import (ExtResult, LocalResult, Scoring, ptr, EXT_RESULT_DTYPE,
+from swiftbwa_b200.abi import (ExtResult, LocalResult, Scoring, ptr, CIGAR_RESULT_DTYPE, EXT_RESULT_DTYPE,
                                GLOBAL_RESULT_DTYPE, LOCAL_RESULT_DTYPE)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -89,6 +89,9 @@ def lib() -> C.CDLL:
                                        C.c_void_p, P(C.c_uint32), C.c_size_t, C.c_int,
                                        P(C.c_uint64)]
         L.orc_local_batch.argtypes = L.orc_ext_batch.argtypes
+        L.orc_cigar_batch.argtypes = [P(Scoring), u8p, u8p, C.c_void_p, C.c_size_t, C.c_void_p, P(C.c_uint32),
+                                      C.c_size_t, C.c_char_p, C.c_size_t, C.c_int, P(C.c_uint64)]
+        L.orc_cigar_batch.restype = C.c_int
         L.orc_extend_batch.argtypes = [P(Scoring), u8p, u8p, C.c_int64, C.c_void_p, C.c_void_p, C.c_size_t,
                                        C.c_void_p, P(C.c_uint32), C.c_int, P(C.c_uint64)]
         L.orc_extend_batch.restype = C.c_int
@@ -245,6 +248,24 @@ def global_batch(sc: Scoring, bases: np.ndarray, tasks: np.ndarray, pac=None, re
     if rc != 0:
         raise ValueError("global_batch failed")
     return res, cig, cells.value
+
+
+def cigar_batch(sc: Scoring, bases: np.ndarray, tasks: np.ndarray, pac=None, n_threads: int = 1):
+    """CIGARGenerator.generate over CIGAR_TASK_DTYPE tasks, host threads ->
+    (CIGAR_RESULT_DTYPE results, CIGAR words, MD bytes, cells); task k's CIGAR
+    is words[cigar_off : cigar_off + n_cigar], its MD md[md_off : md_off + md_len]."""
+    qr = tasks["qlen"].astype(np.int64).clip(0) + tasks["rlen"].astype(np.int64).clip(0)
+    ccap = int((qr + 2).sum()) + 1
+    mcap = int((6 * qr + 8).sum()) + 1
+    res = np.zeros(len(tasks), CIGAR_RESULT_DTYPE)
+    cig = np.zeros(ccap, np.uint32)
+    md = C.create_string_buffer(mcap)
+    cells = C.c_uint64()
+    rc = lib().orc_cigar_batch(C.byref(sc), ptr(bases), ptr(pac), tasks.ctypes.data, len(tasks), res.ctypes.data,
+                               ptr(cig, C.c_uint32), ccap, md, mcap, n_threads, C.byref(cells))
+    if rc != 0:
+        raise ValueError("cigar_batch failed")
+    return res, cig, np.frombuffer(md.raw, np.uint8), cells.value
 
 
 def local_batch(sc: Scoring, bases: np.ndarray, tasks: np.ndarray, pac=None, ref_bases=0,

@@ -1291,6 +1291,62 @@ int orc_global_batch(const swb_scoring *sc, const uint8_t *bases, const uint8_t 
     return 0;
 }
 
+// CIGARGenerator.generate (CIGARGenerator.swift:30-111) over a batch of
+// swb_cigar_task, host threads over static task ranges.  Task k writes its
+// CIGAR at cigar_out + sum_{j<k}(qlen_j + rlen_j + 2) and its MD string
+// (NUL-terminated) at md_out + sum_{j<k}(6*(qlen_j + rlen_j) + 8), the
+// fixed-capacity layout of swb_cigar_batch's header.
+int orc_cigar_batch(const swb_scoring *sc, const uint8_t *bases, const uint8_t *pac,
+                    const swb_cigar_task *tasks, size_t n, swb_cigar_result *results,
+                    uint32_t *cigar_out, size_t cigar_cap, char *md_out, size_t md_cap,
+                    int n_threads, uint64_t *cells) {
+    std::vector<uint64_t> coff(n + 1, 0), moff(n + 1, 0);
+    for (size_t k = 0; k < n; ++k) {
+        const uint64_t qr = (uint64_t)std::max(tasks[k].qlen, 0) + (uint64_t)std::max(tasks[k].rlen, 0);
+        coff[k + 1] = coff[k] + qr + 2;
+        moff[k + 1] = moff[k] + 6 * qr + 8;
+    }
+    if (coff[n] > cigar_cap || moff[n] > md_cap) return -1;
+    std::vector<uint64_t> per(std::max(n_threads, 1), 0);
+    std::vector<int> bad(std::max(n_threads, 1), 0);
+    parallel_for(n, n_threads, [&](size_t lo, size_t hi, int tid) {
+        std::vector<uint8_t> q, r;
+        uint64_t acc = 0;
+        for (size_t k = lo; k < hi; ++k) {
+            const swb_cigar_task &tk = tasks[k];
+            q.resize(std::max(tk.qlen, 1));
+            r.resize(std::max(tk.rlen, 1));
+            load_span(bases, pac, tk.q_off, tk.qlen, tk.flags, false, q.data());
+            load_span(bases, pac, tk.t_off, tk.rlen, tk.flags, true, r.data());
+            swb_cigar_result &res = results[k];
+            int32_t ncig = (int32_t)(coff[k + 1] - coff[k]), nm = 0, score = 0, used = 0;
+            int64_t pos = 0;
+            uint64_t c = 0;
+            if (orc_cigar_generate(q.data(), tk.qlen, r.data(), tk.rlen, tk.qb, tk.qe, tk.read_len, tk.is_reverse,
+                                   tk.true_score, tk.initial_w, sc, tk.ref_pos, cigar_out + coff[k], &ncig, &nm,
+                                   md_out + moff[k], (int32_t)(moff[k + 1] - moff[k]), &score, &pos, &c,
+                                   &used) != 0) {
+                bad[tid] = 1;
+                continue;
+            }
+            acc += c;
+            res.score = score;
+            res.nm = nm;
+            res.n_cigar = ncig;
+            res.md_len = (int32_t)std::strlen(md_out + moff[k]);
+            res.pos = pos;
+            res.cigar_off = coff[k];
+            res.md_off = moff[k];
+            res.used_dp = used;
+            res.reserved = 0;
+        }
+        per[tid] += acc;
+    });
+    if (cells) { *cells = 0; for (auto v : per) *cells += v; }
+    for (int b : bad) if (b) return -1;
+    return 0;
+}
+
 int orc_local_batch(const swb_scoring *sc, const uint8_t *bases, const uint8_t *pac,
                     uint64_t ref_bases, const swb_local_task *tasks, size_t n,
                     swb_local_result *out, int n_threads, uint64_t *cells) {

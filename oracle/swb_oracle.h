@@ -111,6 +111,10 @@ int orc_global_batch(const swb_scoring *sc, const uint8_t *bases, const uint8_t 
                      uint64_t ref_bases, const swb_global_task *tasks, size_t n,
                      swb_global_result *results, uint32_t *cigar_out, size_t cigar_cap,
                      int n_threads, uint64_t *cells);
+int orc_cigar_batch(const swb_scoring *sc, const uint8_t *bases, const uint8_t *pac,
+                    const swb_cigar_task *tasks, size_t n, swb_cigar_result *results,
+                    uint32_t *cigar_out, size_t cigar_cap, char *md_out, size_t md_cap,
+                    int n_threads, uint64_t *cells);
 int orc_local_batch(const swb_scoring *sc, const uint8_t *bases, const uint8_t *pac,
                     uint64_t ref_bases, const swb_local_task *tasks, size_t n,
                     swb_local_result *out, int n_threads, uint64_t *cells);
