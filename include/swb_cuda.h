@@ -241,6 +241,21 @@ int swb_ext_batch_device(swb_ctx *ctx, const swb_scoring *sc,
                          const uint8_t *d_bases, const swb_ext_task *d_tasks,
                          size_t n_tasks, swb_ext_result *d_out, void *stream);
 
+/* The plain one-launch-per-batch form of swb_ext_batch_device, the dispatch
+ * shape of BandedSWDispatcher.dispatchBatch8/16 (BandedSWDispatcher.swift:48,107):
+ * one launch over the batch in input order, one task per thread, with the
+ * same two-row kernel code as the binned pass and rows sized for the
+ * batch's longest query (int8 rows when every task's scores fit a byte,
+ * else int16) -- no sort, no length bins, no claiming.  Tasks that code
+ * cannot take (queries above 256 bases, scores beyond int16) run the
+ * binned pass's int32 kernels afterwards.  Same results as
+ * swb_ext_batch_device; it exists as the baseline that batching is
+ * measured against.  Reads the batch's shape back from the device, so it
+ * synchronises `stream` once before its main launch. */
+int swb_ext_batch_plain_device(swb_ctx *ctx, const swb_scoring *sc,
+                               const uint8_t *d_bases, const swb_ext_task *d_tasks,
+                               size_t n_tasks, swb_ext_result *d_out, void *stream);
+
 /* Length classes of the extension bins: ascending query-length bounds
  * (1..15 values within [8, 256]); each class has an int8-row and an
  * int16-row bin (two target rows per pass, one task per thread), and
@@ -271,15 +286,19 @@ int swb_tune_ext_bins(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases,
  * pointer is a device pointer the caller owns (d_pac: the .pac reference
  * for SWB_T_FROM_REF spans, may be NULL otherwise; spans are trusted, as in
  * swb_ext_batch_device).  Its only working memory is one static device
- * array of 18.9 MB that every GPU loading the library holds until the
- * process exits.  Limit: a task that needs the int32 path (query above 256
- * bases, or h0 + qlen*maxScore above 32000) may have at most 1024 query
- * bases; a longer one gets an all-zero result and the call returns
+ * array of 18.9 MB.  A GPU holds it from the first call on that GPU (which
+ * loads this code there under CUDA's default lazy module loading; a call
+ * with n_tasks = 0 is enough) until the process exits, so a caller that is
+ * about to hand the free HBM to its own arena makes that first call before.
+ * Limit: a task that needs the int32 path (query above 256 bases, or
+ * h0 + qlen*maxScore above 32000) may have at most 1024 query bases; a
+ * longer one gets an all-zero result and the call returns
  * SWB_ERR_TOO_LARGE naming the first such task.  The first call on a device
  * does a one-time set-up (looks up the array's address, sizes a kernel);
  * make that first call before any stream capture.  The call waits for its
- * stream to finish.  Calls share the array, so calls that overlap on the
- * GPU (other threads or streams) race; serialise them. */
+ * stream to finish.  Calls share the array: calls from threads of one
+ * process take turns (a per-device lock held until the stream is done);
+ * calls from different processes on one GPU that overlap there race. */
 int swb_ext_batch_static(const swb_scoring *sc, const uint8_t *d_bases, const uint8_t *d_pac,
                          const swb_ext_task *d_tasks, size_t n_tasks, swb_ext_result *d_out,
                          void *stream);
@@ -391,7 +410,7 @@ int swb_mate_rescue(swb_ctx *ctx, const swb_scoring *sc,
  * tasks, large requests split across waves so small ones do not wait behind
  * them), stages each request's bases once into a device arena admitted
  * against arena_bytes, sorts/bins every wave's tasks together, and
- * alternates waves between two internal lanes so that one wave's copies
+ * rotates waves over three internal lanes so that one wave's copies
  * overlap the other's kernels.  plain = 1 disables all of that: one
  * request at a time, one launch sequence each (the baseline).  The caller
  * keeps each request's buffers alive until its ticket completes; each
@@ -403,7 +422,8 @@ typedef struct swb_server_opts {
     int32_t  plain;            /* 0 = served (waves, three lanes); 1 = one request
                                   at a time through the binned launch sequence;
                                   2 = one request at a time through the plain
-                                  single-launch kernel (swb_ext_batch_static)  */
+                                  one-launch-per-batch kernel
+                                  (swb_ext_batch_plain_device)                 */
     int32_t  start_paused;     /* 1 = admit nothing until swb_server_resume    */
     uint32_t latency_cells;    /* served mode: tasks with more DP cells than this
                                   (qlen * tlen) run one warp per extension, so no

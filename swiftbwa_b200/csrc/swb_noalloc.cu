@@ -7,8 +7,11 @@
 // cudaMalloc/cudaFree, which may synchronise the device and stall the other
 // requests' streams.  swb_ext_batch_static serves them: the caller passes
 // device inputs and outputs, and the only working memory is the
-// file-scope array below, which the driver places on every GPU that loads
-// the library and keeps until the process exits.
+// file-scope array below.  The driver places it on a GPU when this file's
+// device code is loaded there -- with CUDA's default lazy module loading,
+// at the first call on that GPU (a call with zero tasks is enough) -- and
+// keeps it until the process exits.  A caller that is about to give the
+// free HBM to its own arena makes that first call before.
 //
 // It runs the same device code as swb_ext_batch_device (swb_ext_dp.cuh),
 // without the sort/binning pass: tasks are taken in input order by the
@@ -81,6 +84,7 @@ struct DeviceState {
     unsigned char *scratch = nullptr;   // device address of g_ext_static_scratch
     int sm_count = 0;
     int smem_blocks = 1;
+    std::mutex call_mu;                 // one call at a time per device in this process
 };
 
 std::mutex g_state_mu;
@@ -131,13 +135,16 @@ extern "C" int swb_ext_batch_static(const swb_scoring *sc, const uint8_t *d_base
     if (sc->e_ins <= 0 || sc->e_del <= 0 || sc->o_ins < 0 || sc->o_del < 0 || sc->a < 0 || sc->b < 0 ||
         sc->a > 127 || sc->b > 128)
         return set_error(SWB_ERR_INVALID_ARG, "scoring: need e_ins, e_del > 0, o_* >= 0 and 0 <= a <= 127, 0 <= b <= 128");
-    if (n_tasks == 0) return SWB_OK;
     int dev = 0;
     SWB_CUDA(cudaGetDevice(&dev));
     DeviceState *st = nullptr;
-    int rc = device_state(dev, &st);
+    int rc = device_state(dev, &st);   // also for n_tasks == 0: loads the array on this device
     if (rc) return rc;
+    if (n_tasks == 0) return SWB_OK;
     cudaStream_t s = (cudaStream_t)stream;
+    // Calls from this process's threads share the array; hold it from the
+    // status reset until the stream has finished with it.
+    std::lock_guard<std::mutex> call_lock(st->call_mu);
     // Every call shares the array: reset the status words (code 0, index ~0).
     SWB_CUDA(cudaMemsetAsync(st->scratch, 0, sizeof(int), s));
     SWB_CUDA(cudaMemsetAsync(st->scratch + sizeof(int), 0xFF, sizeof(int), s));
