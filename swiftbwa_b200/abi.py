@@ -130,7 +130,7 @@ assert LOCAL_RESULT_DTYPE.itemsize == C.sizeof(LocalResult) == 24
 EXPORTED_SYMBOLS = (
     "swb_scoring_default", "swb_init", "swb_destroy", "swb_strerror",
     "swb_last_error_message", "swb_upload_reference", "swb_ext_batch",
-    "swb_global_batch", "swb_local_batch", "swb_ext_batch_device",
+    "swb_global_batch", "swb_local_batch", "swb_ext_batch_device", "swb_ext_batch_plain_device",
     "swb_banded_sw_align", "swb_global_align", "swb_local_align",
     "swb_kernel_launches", "swb_last_batch_stats", "swb_profile", "swb_profile_reset",
     "swb_profile_read", "swb_int_alu_peak", "swb_int16x2_alu_peak", "swb_set_ext_bins", "swb_get_ext_bins", "swb_tune_ext_bins", "swb_ext_batch_static", "swb_cigar_batch",
@@ -199,6 +199,8 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.swb_local_batch.restype = C.c_int
     lib.swb_ext_batch_device.argtypes = [vp, P(Scoring), vp, vp, C.c_size_t, vp, vp]
     lib.swb_ext_batch_device.restype = C.c_int
+    lib.swb_ext_batch_plain_device.argtypes = [vp, P(Scoring), vp, vp, C.c_size_t, vp, vp]
+    lib.swb_ext_batch_plain_device.restype = C.c_int
     lib.swb_banded_sw_align.argtypes = [vp, u8p, C.c_int32, u8p, C.c_int32, P(Scoring),
                                         C.c_int32, C.c_int32, C.c_int32, P(ExtResult)]
     lib.swb_banded_sw_align.restype = C.c_int

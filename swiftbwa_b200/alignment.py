@@ -296,6 +296,13 @@ class Engine:
         _check(self.lib.swb_ext_batch_device(self.h, C.byref(sc), C.c_void_p(d_bases), C.c_void_p(d_tasks), n,
                                              C.c_void_p(d_out), C.c_void_p(stream)), "swb_ext_batch_device")
 
+    def ext_batch_plain_device(self, sc: Scoring, d_bases: int, d_tasks: int, n: int, d_out: int, stream: int = 0):
+        """swb_ext_batch_plain_device: the plain one-launch-per-batch kernel (the
+        dispatch shape of BandedSWDispatcher.dispatchBatch16), same results."""
+        _check(self.lib.swb_ext_batch_plain_device(self.h, C.byref(sc), C.c_void_p(d_bases), C.c_void_p(d_tasks), n,
+                                                   C.c_void_p(d_out), C.c_void_p(stream)),
+               "swb_ext_batch_plain_device")
+
     # --------------------------------------------------- single-call forms
     def banded_sw_align(self, query, target, scoring: Scoring, w: int, h0: int,
                         end_bonus: int = 0) -> SWResult:

@@ -200,6 +200,84 @@ __global__ void __launch_bounds__(kBigT) ext_global_kernel(ExtArgs a, int bin, i
     add_cells(a.cells + kCntExtBin0 + bin, cells);
 }
 
+// ------------------------------------------------------ plain comparator
+// The batch as the reference's GPU dispatcher shapes it
+// (BandedSWDispatcher.dispatchBatch16, Sources/MetalSW/BandedSWDispatcher.swift:107-160):
+// one launch, one task per thread in input order -- no sort, no length bins,
+// no claiming -- running the same two-row code (ext_pair_one) with rows sized
+// for the batch's longest query: int8 rows when every task's score bound fits
+// a byte, else int16 rows.  It differs from the binned pass only in the
+// batching, which makes it the baseline the batching is measured against.
+// Tasks the two-row code cannot take (queries above kExtSmemMaxQ, scores
+// beyond int16, gap costs beyond a 16-bit lane) are collected, unordered,
+// into one list that the int32 kernels of the binned pass run.
+
+// True when the two-row code takes the task in the plain launch.
+__device__ __forceinline__ bool plain_pair_task(const swb_ext_task &t, int max_mat, bool pair_ok) {
+    return t.qlen <= 0 || t.tlen <= 0 || (pair_ok && t.qlen <= kExtSmemMaxQ && fits16(t.qlen, t.h0, max_mat));
+}
+
+// Shape of a plain batch (device words in the pass's misc block).
+struct PlainShape {
+    int pair_max_q;   // longest query the plain launch takes (at least 1 when it takes any task; 0: none)
+    int need16;       // 1 when one of them needs int16 rows
+    int big_max_q;    // longest query of the int32 list
+};
+constexpr size_t kPlainShapeOff = 64;
+
+// Classifies every task: the plain launch's row shape, and the int32 list
+// (order[0 .. bin_start[1]) with bin_start[0] = 0).
+__global__ void ext_plain_scan_kernel(const swb_ext_task *__restrict__ tasks, size_t n, int max_mat, int pair_ok,
+                                      uint32_t *__restrict__ bin_start, uint32_t *__restrict__ order,
+                                      PlainShape *__restrict__ shape) {
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    int pq = 0, n16 = 0, bq = 0;
+    if (i < n) {
+        const swb_ext_task t = tasks[i];
+        if (plain_pair_task(t, max_mat, pair_ok != 0)) {
+            pq = t.qlen > 0 && t.tlen > 0 ? t.qlen : 1;   // an empty task still needs its zero result
+            n16 = t.qlen > 0 && t.tlen > 0 && !fits8(t.qlen, t.h0, max_mat);
+        } else {
+            bq = t.qlen;
+            order[atomicAdd(&bin_start[1], 1u)] = (uint32_t)i;
+        }
+    }
+    pq = (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)pq);
+    n16 = (int)__reduce_or_sync(0xFFFFFFFFu, (unsigned)n16);
+    bq = (int)__reduce_max_sync(0xFFFFFFFFu, (unsigned)bq);
+    if ((threadIdx.x & 31) == 0) {
+        if (pq) atomicMax(&shape->pair_max_q, pq);
+        if (n16) atomicOr(&shape->need16, 1);
+        if (bq) atomicMax(&shape->big_max_q, bq);
+    }
+}
+
+template <int T, bool U8>
+__global__ void __launch_bounds__(T) ext_plain_kernel(ExtArgs a, size_t n, int qcap, int pair_ok) {
+    extern __shared__ uint32_t sm[];
+    uint16_t *he16 = reinterpret_cast<uint16_t *>(sm) + threadIdx.x;
+    uint32_t *he32 = sm + threadIdx.x;
+    uint8_t *qc = reinterpret_cast<uint8_t *>(sm) + (size_t)(qcap + 1) * T * (U8 ? 2 : 4) + threadIdx.x;
+    unsigned long long cells = 0;
+    const size_t pos = blockIdx.x * (size_t)T + threadIdx.x;
+    if (pos < n) {
+        const swb_ext_task tk = a.tasks[pos];
+        if (plain_pair_task(tk, a.sc.max_mat, pair_ok != 0)) {
+            swb_ext_result r;
+            const bool sym = a.sc.o_del + a.sc.e_del == a.sc.o_ins + a.sc.e_ins;
+            if constexpr (U8) {
+                if (sym) ext_pair_one<T, true, false>(a, tk, he16, qc, r, cells);
+                else ext_pair_one<T, false, false>(a, tk, he16, qc, r, cells);
+            } else {
+                if (sym) ext_pair_one<T, true, true>(a, tk, he32, qc, r, cells);
+                else ext_pair_one<T, false, true>(a, tk, he32, qc, r, cells);
+            }
+            a.out[pos] = r;
+        }
+    }
+    add_cells(a.cells + kCntExtBin0, cells);
+}
+
 // A 16-bit (int8 scores) or 32-bit (int16) word and a query byte per column.
 size_t fast_smem_bytes(int qcap, bool u8) {
     return ((size_t)(qcap + 1) * kFastT * (u8 ? sizeof(uint16_t) : sizeof(uint32_t)) + (size_t)qcap * kFastT + 15) &
@@ -400,6 +478,80 @@ int ext_big_max_q_range(const swb_ctx *ctx, const swb_ext_task *tasks, size_t lo
         if (!pair_ok || t.qlen > top || !fits16(t.qlen, t.h0, sc.max_mat)) m = t.qlen > m ? t.qlen : m;
     }
     return m;
+}
+
+// The plain comparator (see ext_plain_kernel): one launch of the two-row code
+// over the batch in input order, then the int32 kernels over the tasks it
+// cannot take.  The batch's shape (row length and width) is read back from
+// the device, which synchronises `s` once.
+int launch_ext_plain(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases, const swb_ext_task *d_tasks,
+                     size_t n, swb_ext_result *d_out, unsigned long long *d_cells, cudaStream_t s) {
+    if (n == 0) return SWB_OK;
+    if (n > 0x7FFFFFF0ull) return set_error(SWB_ERR_TOO_LARGE, "more than 2^31-16 tasks in one batch");
+    int rc;
+    if ((rc = ensure_dev(ctx, ctx->d_idx2, n * 4)) || (rc = ensure_dev(ctx, ctx->d_misc, kMiscBytes))) return rc;
+    char *misc = (char *)ctx->d_misc.p;
+    uint32_t *bin_start = (uint32_t *)misc;                 // {0, int32-list length}
+    PlainShape *shape = (PlainShape *)(misc + kPlainShapeOff);
+    uint32_t *claim = (uint32_t *)(misc + 320);
+    uint32_t *order = (uint32_t *)ctx->d_idx2.p;
+    SWB_CUDA(cudaMemsetAsync(misc, 0, kMiscBytes, s));
+    const int pair_ok = sc.o_del + sc.e_del <= 32767 && sc.o_ins + sc.e_ins <= 32767;
+    const unsigned tb = 256;
+    {
+        ProfScope ps(ctx, s, "ext_plain_scan", -1);
+        ext_plain_scan_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(d_tasks, n, sc.max_mat, pair_ok, bin_start,
+                                                                            order, shape);
+    }
+    ctx->launches++;
+    SWB_CUDA(cudaGetLastError());
+    PlainShape sh{};
+    SWB_CUDA(cudaMemcpyAsync(&sh, shape, sizeof(sh), cudaMemcpyDeviceToHost, s));
+    SWB_CUDA(cudaStreamSynchronize(s));
+    if (sh.big_max_q > kMaxLen) return set_error(SWB_ERR_TOO_LARGE, "query longer than 65535 bases");
+    ExtArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_out, order, bin_start, d_cells, claim};
+    if (sh.pair_max_q > 0) {
+        // Rows for the longest query, in the kernel's word width; one
+        // 32-thread block per 32 consecutive tasks.
+        const int qcap = imin(sh.pair_max_q, kExtSmemMaxQ);
+        const bool u8 = sh.need16 == 0;
+        const size_t smem = fast_smem_bytes(qcap, u8);
+        ProfScope ps(ctx, s, "ext_plain", kCntExtBin0);
+        const unsigned grid = (unsigned)((n + kFastT - 1) / kFastT);
+        if (u8) ext_plain_kernel<kFastT, true><<<grid, kFastT, smem, s>>>(a, n, qcap, pair_ok);
+        else ext_plain_kernel<kFastT, false><<<grid, kFastT, smem, s>>>(a, n, qcap, pair_ok);
+        ctx->launches++;
+        SWB_CUDA(cudaGetLastError());
+    }
+    if (sh.big_max_q > 0) {
+        const int wq = imin(sh.big_max_q, kWarpMaxQ);
+        const size_t wstride = ((size_t)(wq + 1) * 8 + (size_t)wq + 15) & ~(size_t)15;
+        const int wwarps = (int)std::max<size_t>(1, std::min<size_t>(8, (size_t)(200 * 1024) / wstride));
+        int wblocks = 0;
+        SWB_CUDA(cudaFuncSetAttribute(ext_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(wwarps * wstride)));
+        SWB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wblocks, ext_warp_kernel, wwarps * 32,
+                                                               wwarps * wstride));
+        wblocks = imax(wblocks, 1) * ctx->sm_count;
+        {
+            ProfScope ps(ctx, s, "ext_plain_i32", kCntExtBin0 + 1);
+            ext_warp_kernel<<<(unsigned)wblocks, wwarps * 32, wwarps * wstride, s>>>(a, 0, wq);
+        }
+        ctx->launches++;
+        SWB_CUDA(cudaGetLastError());
+        if (sh.big_max_q > kWarpMaxQ) {
+            const size_t nslots = (size_t)ctx->sm_count * 4 * kBigT;
+            const size_t cols = (size_t)sh.big_max_q + 1;
+            if ((rc = ensure_dev(ctx, ctx->d_scratch, cols * nslots * (2 * sizeof(int) + 1) + 256))) return rc;
+            int *hbuf = (int *)ctx->d_scratch.p;
+            int *ebuf = hbuf + cols * nslots;
+            uint8_t *qbuf = (uint8_t *)(ebuf + cols * nslots);
+            ext_global_kernel<<<(unsigned)(nslots / kBigT), kBigT, 0, s>>>(a, 0, hbuf, ebuf, qbuf, nslots, wq);
+            ctx->launches++;
+            SWB_CUDA(cudaGetLastError());
+        }
+    }
+    return SWB_OK;
 }
 
 }  // namespace swb

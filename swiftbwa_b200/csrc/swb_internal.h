@@ -188,6 +188,12 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
                unsigned long long *d_cells, cudaStream_t stream, int max_q_hint,
                uint32_t warp_cells = 0, const ExtPipe *pipe = nullptr);
 
+// The plain one-launch-per-batch comparator of the extension pass (the same
+// two-row kernel over the batch in input order; no sort, bins or claiming).
+// Reads the batch's shape back from the device: synchronises `stream` once.
+int launch_ext_plain(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases, const swb_ext_task *d_tasks,
+                     size_t n, swb_ext_result *d_out, unsigned long long *d_cells, cudaStream_t stream);
+
 // Banded global + traceback (kernel 2).  Tasks with qlen <= kGlobalSmemMaxQ
 // run in the shared-memory kernel, longer ones in the global-scratch kernel;
 // the shape gives each group's count and largest query / target.

@@ -721,6 +721,18 @@ int swb_ext_batch_device(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *d_b
     return launch_ext(ctx, make_dev_scoring(*sc), d_bases, d_tasks, n_tasks, d_out, ctx->d_counters, s, -1);
 }
 
+int swb_ext_batch_plain_device(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *d_bases,
+                               const swb_ext_task *d_tasks, size_t n_tasks, swb_ext_result *d_out, void *stream) {
+    if (!ctx || (!d_tasks && n_tasks) || (!d_out && n_tasks)) return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
+    int rc;
+    if ((rc = validate_scoring(sc))) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (n_tasks == 0) return SWB_OK;
+    SWB_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    return launch_ext_plain(ctx, make_dev_scoring(*sc), d_bases, d_tasks, n_tasks, d_out, ctx->d_counters, s);
+}
+
 int swb_global_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, size_t n_bases,
                      const swb_global_task *tasks, size_t n_tasks, swb_global_result *results,
                      uint32_t *cigar_out, size_t cigar_cap) {

@@ -23,7 +23,8 @@
 //     request when its last slice has landed.
 // plain = 1 is the baseline of the same kernels: one request at a time, copy
 // in, compute, copy out, synchronise.  plain = 2 also swaps the binned pass
-// for the plain single-launch kernel of swb_ext_batch_static.
+// for the plain one-launch-per-batch kernel (launch_ext_plain: the same
+// two-row code over the request in input order, no sort or bins).
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -35,9 +36,6 @@
 #include <vector>
 
 #include "swb_internal.h"
-
-extern "C" int swb_ext_batch_static(const swb_scoring *sc, const uint8_t *d_bases, const uint8_t *d_pac,
-                                    const swb_ext_task *d_tasks, size_t n_tasks, swb_ext_result *d_out, void *stream);
 
 using namespace swb;
 
@@ -296,7 +294,13 @@ bool launch_wave(swb_server *s, Lane &L) {
     if (!rc) cudaEventRecord(L.ev_t0, st);
     if (!rc) {
         if (s->plain == 2) {
-            rc = swb_ext_batch_static(&s->sc, s->d_arena, c->d_pac, d_tasks, wn, d_out, st);
+            // The plain launch reads the request's shape back (a stream
+            // synchronisation): submitters and waiters need not wait for it.
+            // Only this worker thread touches the lanes and the dispatched
+            // requests meanwhile.
+            s->mu.unlock();
+            rc = launch_ext_plain(c, s->dsc, s->d_arena, d_tasks, wn, d_out, c->d_counters, st);
+            s->mu.lock();
         } else {
             // The int32 bin's scratch is sized from the longest query of the
             // wave's requests (an upper bound of the bin's), known since submit.
