@@ -1,6 +1,7 @@
 """The continuous-batching request loop (swb_server_*): every request's
-results are the same alone and in the mix, in served and plain mode; waits
-are bounded; admission waits for arena space; oversized requests are
+results equal the oracle's (the C++ restatement of BandedSWScalar.align)
+and are the same alone and in the mix, in served and both plain modes;
+waits are bounded; admission waits for arena space; oversized requests are
 rejected at submit."""
 import numpy as np
 import pytest
@@ -22,9 +23,11 @@ def engine():
     e.close()
 
 
-def _pool(engine, seed=31, n=6000):
+def _pool(engine, seed=31, n=6000, with_ref=False):
     d = gen.ext_tasks(seed, n, qmax=280, ref_len=8000)
     engine.upload_reference(d["pac"], d["ref_bases"])
+    if with_ref:
+        return d["bases"], d["tasks"], d["pac"], d["ref_bases"]
     return d["bases"], d["tasks"]
 
 
@@ -38,13 +41,16 @@ def _requests(n_pool, seed=7, k=40):
     return out
 
 
-@pytest.mark.parametrize("plain", [False, True])
-def test_same_alone_and_in_mix(engine, plain):
+@pytest.mark.parametrize("plain", [0, 1, 2])
+def test_same_alone_and_in_mix(engine, oracle_mod, plain):
     from swiftbwa_b200.serving import Server, slice_request
     sc = Scoring.default()
-    bases, tasks = _pool(engine)
+    bases, tasks, pac, ref_bases = _pool(engine, with_ref=True)
     reqs = [slice_request(bases, tasks, lo, hi) for lo, hi in _requests(len(tasks))]
     alone = [engine.ext_batch(sc, b, t) for b, t in reqs]
+    for k, (b, t) in enumerate(reqs):
+        exp, _ = oracle_mod.ext_batch(sc, b, t, pac=pac, ref_bases=ref_bases)
+        assert np.array_equal(alone[k], exp), f"request {k} alone differs from the oracle"
     # Small waves force large requests across several waves and both lanes.
     srv = Server(engine, sc, arena_bytes=1 << 24, max_wave_tasks=700, plain=plain)
     try:
@@ -104,9 +110,10 @@ def test_admission_waits_for_arena_space(engine):
 
 
 @pytest.mark.parametrize("plain", [0, 2])
-def test_pinned_zero_copy_pool(engine, plain):
+def test_pinned_zero_copy_pool(engine, oracle_mod, plain):
     """Requests as views of a pinned pool (span_origin, device-side rebase),
-    served and through the plain single-launch kernel: same as alone."""
+    served and through the plain single-launch kernel: same as alone and as
+    the oracle."""
     torch = pytest.importorskip("torch")
     from swiftbwa_b200 import workloads as W
     from swiftbwa_b200.abi import EXT_RESULT_DTYPE
@@ -119,6 +126,8 @@ def test_pinned_zero_copy_pool(engine, plain):
     pt = torch.from_numpy(pool.tasks.view(np.uint8)).pin_memory().numpy().view(pool.tasks.dtype)
     po = torch.zeros(len(pool.tasks) * EXT_RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy().view(EXT_RESULT_DTYPE)
     expected = engine.ext_batch(sc, pool.bases, pool.tasks)
+    oracle_out, _ = oracle_mod.ext_batch(sc, pool.bases, pool.tasks, pac=ref.pac, ref_bases=ref.n, n_threads=8)
+    assert np.array_equal(expected, oracle_out)
     rng = np.random.default_rng(3)
     cuts = np.sort(rng.choice(np.arange(1, len(pool.tasks)), 30, replace=False))
     bounds = list(zip([0, *cuts], [*cuts, len(pool.tasks)]))     # disjoint requests covering the pool
@@ -133,15 +142,17 @@ def test_pinned_zero_copy_pool(engine, plain):
     finally:
         srv.stop()
     assert np.array_equal(po, expected)
+    assert np.array_equal(po, oracle_out)
 
 
-def test_multiserver_on_one_gpu(engine):
+def test_multiserver_on_one_gpu(engine, oracle_mod):
     """The multi-GPU router over this GPU's server (one device here): results
-    equal the direct batch call, whole and split into slices."""
+    equal the oracle and the direct batch call, whole and split into slices."""
     from swiftbwa_b200.serving import MultiServer, Server
     sc = Scoring.default()
     d = gen.ext_tasks(404, 4000, qmax=200)
     expected = engine.ext_batch(sc, d["bases"], d["tasks"])
+    assert np.array_equal(expected, oracle_mod.ext_batch(sc, d["bases"], d["tasks"])[0])
     srv = Server(engine, sc)
     try:
         ms = MultiServer([srv], split_tasks=1000)

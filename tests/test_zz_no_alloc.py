@@ -4,10 +4,12 @@ It exists for callers that cannot let the library call cudaMalloc -- a
 server whose own arena already holds the free HBM, or a batching loop that
 cannot afford cudaMalloc/cudaFree stalling its other streams -- and works
 from one static device array instead.  These tests call it through the C
-ABI on device buffers the test owns and hold it to the allocating entry
-point (swb_ext_batch) bit for bit, on two calls in a row (the second call
-sees the array the first one left behind), and check that a task beyond
-its stated limit is rejected with a clear error.
+ABI on device buffers the test owns and hold it to the oracle (the C++
+restatement of BandedSWScalar.align) and to the allocating entry point
+(swb_ext_batch) bit for bit, on two calls in a row (the second call sees
+the array the first one left behind), check that the second call leaves the
+device's free memory unchanged, and check that a task beyond its stated
+limit is rejected with a clear error.
 
 This file is named to be collected last.
 """
@@ -50,7 +52,7 @@ def _call_static(lib, torch, sc, d_bases, d_pac, d_tasks, n, d_out):
                                     C.c_void_p(torch.cuda.current_stream().cuda_stream))
 
 
-def test_static_entry_matches_allocating_entry_twice():
+def test_static_entry_matches_allocating_entry_twice(oracle_mod):
     torch = pytest.importorskip("torch")
     from swiftbwa_b200.alignment import Engine
     from swiftbwa_b200.build import build
@@ -64,14 +66,23 @@ def test_static_entry_matches_allocating_entry_twice():
             expected = eng.ext_batch(scoring, bases, tasks)
         finally:
             eng.close()
+        oracle_out, _ = oracle_mod.ext_batch(scoring, bases, tasks, pac=pac, ref_bases=ref_bases, n_threads=8)
+        assert np.array_equal(expected, oracle_out)
         d_bases, d_pac, d_tasks = _dev(torch, bases), _dev(torch, pac), _dev(torch, tasks)
+        outs = [torch.full((len(tasks) * EXT_RESULT_DTYPE.itemsize,), 0xA5, dtype=torch.uint8, device="cuda:0")
+                for _ in range(2)]
         for call in range(2):
-            d_out = torch.full((len(tasks) * EXT_RESULT_DTYPE.itemsize,), 0xA5, dtype=torch.uint8, device="cuda:0")
-            rc = _call_static(lib, torch, scoring, d_bases, d_pac, d_tasks, len(tasks), d_out)
+            torch.cuda.synchronize()
+            free_before = torch.cuda.mem_get_info(0)[0]
+            rc = _call_static(lib, torch, scoring, d_bases, d_pac, d_tasks, len(tasks), outs[call])
             assert rc == abi.SWB_OK, (rc, lib.swb_last_error_message())
-            got = d_out.cpu().numpy().view(EXT_RESULT_DTYPE)
-            bad = np.nonzero(got != expected)[0]
-            assert bad.size == 0, f"call {call}: {bad.size} tasks differ, first {bad[:5]}"
+            torch.cuda.synchronize()
+            if call == 1:   # the set-up of the first call may load the library's device code
+                assert torch.cuda.mem_get_info(0)[0] == free_before, "the second call changed free device memory"
+            got = outs[call].cpu().numpy().view(EXT_RESULT_DTYPE)
+            bad = np.nonzero(got != oracle_out)[0]
+            assert bad.size == 0, f"call {call}: {bad.size} tasks differ from the oracle, first {bad[:5]}"
+            assert np.array_equal(got, expected)
 
 
 def test_static_entry_rejects_query_beyond_limit():
