@@ -211,8 +211,11 @@ struct ZPacked {
     uint32_t *z;      // this slot's first word
     size_t nslots;
     int ncw;          // words per row for this attempt
+    int w = 0;        // band of this attempt (absolute layout)
+    bool absolute = false;   // nibble of absolute column j (not of band column j - beg)
     __device__ __forceinline__ uint32_t operator()(int i, int col) const {
-        return (z[((size_t)i * ncw + (col >> 3)) * nslots] >> ((col & 7) << 2)) & 0xFu;
+        const int j = absolute ? col + imax(0, i - w) : col;
+        return (z[((size_t)i * ncw + (j >> 3)) * nslots] >> ((j & 7) << 2)) & 0xFu;
     }
 };
 
@@ -240,20 +243,11 @@ struct RowI32 {
     __device__ __forceinline__ int final_score(int s, int) const { return s; }
 };
 
+//   The int16 rows are computed two target rows at a time (global_dp_pair16).
 struct RowI16 {
     uint32_t *he;
     int T;
     static constexpr int kNeg = -16384;
-    __device__ __forceinline__ void load(int j, int &h, int &e) const {
-        const uint32_t w = he[j * T];
-        h = (int)(int16_t)(w & 0xFFFFu);
-        e = (int)w >> 16;
-    }
-    __device__ __forceinline__ void store(int j, int h, int e) const {
-        he[j * T] = ((uint32_t)h & 0xFFFFu) | ((uint32_t)e << 16);
-    }
-    __device__ __forceinline__ int getH(int j) const { return (int)(int16_t)(he[j * T] & 0xFFFFu); }
-    __device__ __forceinline__ void setH(int j, int h) const { reinterpret_cast<int16_t *>(he + j * T)[0] = (int16_t)h; }
     // thr: every real value is above it, every sentinel-derived one at or below.
     __device__ __forceinline__ int final_score(int s, int thr) const { return s <= thr ? kNegInf + (s - kNeg) : s; }
 };
@@ -326,6 +320,156 @@ __device__ int global_dp_smem(const DevScoring &sc, const Row &row, const uint8_
     return row.final_score(row.getH(qlen), thr);                                 // :144
 }
 
+// ------------------------------------------------------------------------
+// int16-row instance, two target rows per pass.  Row i's cell at column c
+// and row i+1's at column c-1 are the low and high 16-bit lanes of one
+// register and go through the DPX s16x2 forms together: vibmax_s16x2 gives
+// each lane's max and its comparison, so the reference's tie rules and
+// backpointer bits come out of the same operation.  Row i+1 takes row i's H
+// and E of column c-1 from registers (one step old) and its diagonal, H of
+// row i at column c-2, from two steps back; only row i+1's words reach
+// shared memory, so a row pair costs one word load and one word store per
+// column.  Row i's band [beg0, end0) and row i+1's [beg1, end1) differ by at
+// most one column at each end (GlobalAligner.swift:90-91), so a pair runs
+// row i alone for one or two columns, both rows together, then row i+1
+// alone for one or two columns.  Backpointer codes are addressed by absolute
+// column (word j/8 of the row, nibble j%8).  Values are those of RowI16.
+__device__ __forceinline__ uint32_t rep16(int v) { return (uint32_t)(uint16_t)(int16_t)v * 0x10001u; }
+// Lane-wise a + b (no lane leaves int16 here: see RowI16).
+__device__ __forceinline__ uint32_t padd16(uint32_t a, uint32_t b) { return __viaddmax_s16x2(a, b, 0x80008000u); }
+// prmt selector (q, q|8, 5, 5) of query code q: score as one 16-bit lane.
+__device__ __forceinline__ uint32_t nw_sel(uint32_t q) { return q * 0x11u + 0x5580u; }
+
+struct NwPairConsts {
+    uint32_t negOeDel, negEDel, negOeIns, negEIns;
+};
+
+// One step of both lanes: DG/UH/UE are the diagonal H, the H and E above,
+// S the scores; h, f are the previous step's H and F (the left neighbours),
+// e receives E.  code0/code1: the 4-bit backpointers of lanes 0/1
+// (GlobalAligner.swift:112-140: bit 0 E extends, 1 F extends, 2 H from E, 3 H from F).
+__device__ __forceinline__ void nw_pair_step(const NwPairConsts &k, uint32_t DG, uint32_t UH, uint32_t UE, uint32_t S,
+                                             uint32_t &h, uint32_t &e, uint32_t &f, uint32_t &code0,
+                                             uint32_t &code1) {
+    bool eh, el, fh, fl, keh, kel, kfh, kfl;
+    uint32_t hc = padd16(DG, S);
+    const uint32_t ev = __vibmax_s16x2(padd16(UE, k.negEDel), padd16(UH, k.negOeDel), &eh, &el);
+    const uint32_t fv = __vibmax_s16x2(padd16(f, k.negEIns), padd16(h, k.negOeIns), &fh, &fl);
+    hc = __vibmax_s16x2(hc, ev, &keh, &kel);
+    hc = __vibmax_s16x2(hc, fv, &kfh, &kfl);
+    code0 = (el ? 1u : 0u) | (fl ? 2u : 0u) | (kel ? 0u : 4u) | (kfl ? 0u : 8u);
+    code1 = (eh ? 1u : 0u) | (fh ? 2u : 0u) | (keh ? 0u : 4u) | (kfh ? 0u : 8u);
+    f = fv;
+    h = hc;
+    e = ev;
+}
+
+// Backpointer word of one row: codes are or-ed in at nibble j%8 and the
+// word is stored when its last column is done.
+struct ZRow {
+    uint32_t *z;      // word 0 of this row and slot
+    size_t nslots;
+    uint32_t acc = 0;
+    __device__ __forceinline__ void put(int j, uint32_t code, int last) {
+        acc |= code << ((j & 7) << 2);
+        if ((j & 7) == 7 || j == last) {
+            z[(size_t)(j >> 3) * nslots] = acc;
+            acc = 0;
+        }
+    }
+};
+
+__device__ int global_dp_pair16(const DevScoring &sc, uint32_t *__restrict__ he, const uint8_t *__restrict__ qs,
+                                int T, const GlobalArgs &a, const swb_global_task &tk, int w, const ZPacked &zp,
+                                unsigned long long &cells) {
+    constexpr int kNeg = RowI16::kNeg;
+    const int qlen = tk.qlen, tlen = tk.tlen;
+    const int oDel = sc.o_del, eDel = sc.e_del, oIns = sc.o_ins, eIns = sc.e_ins;
+    const int oeDel = oDel + eDel, oeIns = oIns + eIns;
+    const NwPairConsts k{rep16(-oeDel), rep16(-eDel), rep16(-oeIns), rep16(-eIns)};
+    const uint32_t negHi = (uint32_t)(uint16_t)kNeg << 16;
+    // First row (GlobalAligner.swift:75-84): h[0] = 0, h[j] = -(oIns + eIns*j) up to w, E = -inf.
+    const int initEnd = imin(w, qlen);
+    for (int j = 0; j <= qlen; ++j) {
+        const int hv = j == 0 ? 0 : (j <= initEnd ? 0 - (oIns + eIns * j) : kNeg);
+        he[j * T] = ((uint32_t)hv & 0xFFFFu) | negHi;
+    }
+    const size_t rstride = (size_t)zp.ncw * zp.nslots;
+    for (int i = 0; i < tlen; i += 2) {                                          // :89-142, two rows at a time
+        const bool pair = i + 1 < tlen;
+        const int beg0 = imax(0, i - w), end0 = imin(qlen, i + w + 1);
+        const int beg1 = imax(0, i + 1 - w), end1 = pair ? imin(qlen, i + w + 2) : beg1;
+        const RowTable rt0 = row_table(sc, span_base(a.bases, a.pac, tk.t_off, i, tlen, tk.flags, true));
+        const RowTable rt1 = pair ? row_table(sc, span_base(a.bases, a.pac, tk.t_off, i + 1, tlen, tk.flags, true)) : rt0;
+        const int hBeg0 = beg0 == 0 ? 0 - (oeDel + eDel * i) : kNeg;
+        const int hBeg1 = beg1 == 0 ? 0 - (oeDel + eDel * (i + 1)) : kNeg;
+        cells += (unsigned long long)(end0 - beg0) + (unsigned long long)(end1 - beg1);
+        ZRow z0{zp.z + (size_t)i * rstride, zp.nslots}, z1{zp.z + (size_t)(i + 1) * rstride, zp.nslots};
+        // Lane 0 state: H of row i at column beg0-1 is hBeg0 (the reference's h[beg0]); F starts at -inf.
+        uint32_t h = (uint32_t)hBeg0 & 0xFFFFu, hp2 = h, e = 0u, f = (uint32_t)(uint16_t)kNeg;
+        uint32_t wdp = he[beg0 * T];                 // word beg0: its H is row i's first diagonal
+        uint32_t selp = 0u;                          // query selector of the previous column
+        bool started = false;                        // lane 1 running
+        int c = beg0;
+        // Lane 1 begins at column beg1 (step beg1 + 1): H at beg1-1 is hBeg1,
+        // F is -inf, and the reference's h[beg1] = hBeg1 is stored.
+        auto start1 = [&]() {
+            h = (h & 0xFFFFu) | ((uint32_t)hBeg1 << 16);
+            f = (f & 0xFFFFu) | negHi;
+            reinterpret_cast<int16_t *>(he + beg1 * T)[0] = (int16_t)hBeg1;
+            started = true;
+        };
+        for (; c < end0; ++c) {
+            const uint32_t wd = he[(c + 1) * T];     // [H(i-1,c) | E(i-1,c)]
+            const uint32_t sel = nw_sel(qs[c * T]);
+            const bool two = pair && c >= beg1 + 1;
+            if (two && !started) start1();
+            const uint32_t DG = __byte_perm(wdp, hp2, 0x5410);    // [H(i-1,c-1), H(i,c-2)]
+            const uint32_t UH = __byte_perm(wd, h, 0x5410);       // [H(i-1,c),   H(i,c-1)]
+            const uint32_t UE = __byte_perm(wd, e, 0x5432);       // [E(i-1,c),   E(i,c-1)]
+            const uint32_t S = prmt(rt1.lo, rt1.hi, selp) * 65536u + prmt(rt0.lo, rt0.hi, sel);
+            hp2 = h;
+            uint32_t code0, code1;
+            nw_pair_step(k, DG, UH, UE, S, h, e, f, code0, code1);
+            z0.put(c, code0, end0 - 1);
+            if (two) {
+                he[c * T] = __byte_perm(h, e, 0x7632);             // row i+1's word c: H, E of column c-1
+                z1.put(c - 1, code1, end1 - 1);
+            } else if (!pair) {
+                he[(c + 1) * T] = __byte_perm(h, e, 0x5410);       // last row alone: its own words
+            }
+            wdp = wd;
+            selp = sel;
+        }
+        if (!pair) continue;
+        // Row i+1 alone for its columns past row i's band (c = end0 .. end1).
+        // Row i's H at end0-1 (or hBeg0) is its diagonal at column end0.
+        uint32_t hLast0 = h & 0xFFFFu, eLast0 = e & 0xFFFFu, hLast0p = hp2 & 0xFFFFu;
+        for (c = imax(end0, beg1 + 1); c <= end1; ++c) {
+            if (!started) start1();
+            const uint32_t sel = nw_sel(qs[(c - 1) * T]);
+            uint32_t DG, UH, UE;
+            if (c - 1 < end0) {             // column end0-1: row i's values from registers
+                DG = hLast0p << 16;
+                UH = hLast0 << 16;
+                UE = eLast0 << 16;
+            } else {                        // column end0: diagonal H(i, end0-1), stale word above
+                const uint32_t wd = he[c * T];
+                DG = hLast0 << 16;
+                UH = wd << 16;
+                UE = wd & 0xFFFF0000u;
+            }
+            const uint32_t S = prmt(rt1.lo, rt1.hi, sel) * 65536u;
+            uint32_t code0, code1;
+            nw_pair_step(k, DG, UH, UE, S, h, e, f, code0, code1);
+            he[c * T] = __byte_perm(h, e, 0x7632);
+            z1.put(c - 1, code1, end1 - 1);
+        }
+    }
+    const int thr = -(qlen + tlen + 2) * step_cost(sc) - 1;
+    return RowI16{he, T}.final_score((int)(int16_t)(he[qlen * T] & 0xFFFFu), thr);     // :144
+}
+
 // Sort key: shared-memory tasks first, then by query length, target length
 // and band, so the threads of a warp align tasks of the same shape.
 // Sort key: the shared-memory kernels' int16-row alignments first, then
@@ -379,8 +523,13 @@ __global__ void __launch_bounds__(256) global_smem_kernel(GlobalArgs a, const ui
             int w0 = tk.w;
             int w = imax(w0, abs(qlen - tlen));                          // :47
             int nCol = (int)min((long long)qlen, 2ll * w + 1);           // :48
-            ZPacked zp{z + slot, nslots, (nCol + 7) >> 3};
-            int score = global_dp_smem(a.sc, row, qs, T, a, tk, w, zp, cells);
+            // int16 rows: backpointers by absolute column, qlen/8 words per row.
+            ZPacked zp{z + slot, nslots, I16 ? (qlen + 7) >> 3 : (nCol + 7) >> 3, w, I16};
+            auto dp = [&]() -> int {
+                if constexpr (I16) return global_dp_pair16(a.sc, row.he, qs, T, a, tk, w, zp, cells);
+                else return global_dp_smem(a.sc, row, qs, T, a, tk, w, zp, cells);
+            };
+            int score = dp();
             if (tk.flags & SWB_GLB_RETRY) {                              // CIGARGenerator.swift:88-96
                 int retries = 0;
                 while (score < tk.true_score && retries < 3) {
@@ -389,8 +538,9 @@ __global__ void __launch_bounds__(256) global_smem_kernel(GlobalArgs a, const ui
                     r.attempts++;
                     w = imax(w0, abs(qlen - tlen));
                     nCol = (int)min((long long)qlen, 2ll * w + 1);
-                    zp.ncw = (nCol + 7) >> 3;
-                    score = global_dp_smem(a.sc, row, qs, T, a, tk, w, zp, cells);
+                    if (!I16) zp.ncw = (nCol + 7) >> 3;
+                    zp.w = w;
+                    score = dp();
                 }
             }
             r.score = score;
