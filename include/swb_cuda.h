@@ -401,6 +401,44 @@ int swb_mate_rescue(swb_ctx *ctx, const swb_scoring *sc,
                     const int64_t *contig_offsets, const int32_t *contig_lengths, size_t n_contigs,
                     uint64_t genome_len, swb_rescued *out, uint32_t *n_out, uint32_t *n_cand);
 
+/* ------------------------------------------------ SMEM seeding (FM index) */
+/* CheckpointOCC (Sources/FMIndex/CheckpointOCC.swift:6-13): the cumulative
+ * A, C, G, T counts before a block of 64 BWT characters and one bitstring
+ * per base with bit 63-y set when position y of the block holds it. */
+typedef struct swb_bwt_checkpoint {
+    int64_t  counts[4];
+    uint64_t bits[4];
+} swb_bwt_checkpoint;        /* 64 bytes */
+
+/* SMEM (Sources/BWACore/SMEM.swift:5-29): SA interval [k, l], inclusive,
+ * and the query span [qb, qe). */
+typedef struct swb_smem {
+    int64_t k, l;
+    int32_t qb, qe;
+} swb_smem;                  /* 24 bytes */
+
+/* Keeps the BWT resident in HBM (the fields of BWT, Sources/FMIndex/BWT.swift:5-20):
+ * n_cp = (length >> 6) + 1 checkpoints, count[5] = the cumulative base
+ * counts each +1 for the sentinel (count[4] = length), sentinel = the BWT
+ * position of '$'.  Replaces the Metal engine's bwtCheckpointBuffer /
+ * bwtCountsBuffer / bwtSentinelBuffer (MetalSWEngine.swift:88-120). */
+int swb_upload_bwt(swb_ctx *ctx, const swb_bwt_checkpoint *cp, uint64_t n_cp, const int64_t count[5],
+                   int64_t length, int64_t sentinel);
+
+/* SMEMFinder.findAllSMEMs(query:bwt:minSeedLen:minIntv:) (SMEMFinder.swift:28-63)
+ * for many reads on the resident BWT: read r is bases[read_off[r] ..+ read_len[r])
+ * (codes 0-4, N = 4).  Its SMEMs, sorted by query begin then longest first,
+ * go to out[r * cap_per_read ..+ n_out[r]].  When a read has more than
+ * cap_per_read SMEMs, n_out[r] still counts them all, its window holds the
+ * first cap_per_read in the order found, and the call returns
+ * SWB_ERR_TOO_LARGE naming the first such read, so the caller can retry
+ * with a larger window (every other read's results are complete).  Replaces
+ * the CPU loop of BWAMemAligner.alignReadPhase1to3 (BWAMemAligner.swift:133-139)
+ * and the Metal forward kernel (Kernels/smem_forward.metal:117) for a batch. */
+int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uint64_t *read_off,
+                   const int32_t *read_len, size_t n_reads, int32_t min_seed_len, int64_t min_intv,
+                   uint32_t cap_per_read, swb_smem *out, uint32_t *n_out);
+
 /* ------------------------------------------------ serving (continuous batching) */
 /* A request loop over one context's GPU for extension batches of differing
  * sizes that arrive concurrently (the actor loop of BWAMemAligner's

@@ -13,8 +13,8 @@ import subprocess
 
 import numpy as np
 
-from swiftbwa_b200.abi import (ExtResult, LocalResult, Scoring, ptr, CIGAR_RESULT_DTYPE, EXT_RESULT_DTYPE,
-                               GLOBAL_RESULT_DTYPE, LOCAL_RESULT_DTYPE)
+from swiftbwa_b200.abi import (ExtResult, LocalResult, Scoring, ptr, BWT_CHECKPOINT_DTYPE, CIGAR_RESULT_DTYPE,
+                               EXT_RESULT_DTYPE, GLOBAL_RESULT_DTYPE, LOCAL_RESULT_DTYPE, SMEM_DTYPE)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "build", "libswb_oracle.so")
@@ -92,6 +92,12 @@ def lib() -> C.CDLL:
         L.orc_cigar_batch.argtypes = [P(Scoring), u8p, u8p, C.c_void_p, C.c_size_t, C.c_void_p, P(C.c_uint32),
                                       C.c_size_t, C.c_char_p, C.c_size_t, C.c_int, P(C.c_uint64)]
         L.orc_cigar_batch.restype = C.c_int
+        L.orc_bwt_build.argtypes = [u8p, C.c_int64, C.c_void_p, C.c_int64, P(C.c_int64), P(C.c_int64),
+                                    P(C.c_int64), C.c_int]
+        L.orc_bwt_build.restype = C.c_int
+        L.orc_smem_batch.argtypes = [C.c_void_p, P(C.c_int64), C.c_int64, C.c_int64, u8p, C.c_void_p, C.c_void_p,
+                                     C.c_size_t, C.c_int32, C.c_int64, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int]
+        L.orc_smem_batch.restype = C.c_int64
         L.orc_extend_batch.argtypes = [P(Scoring), u8p, u8p, C.c_int64, C.c_void_p, C.c_void_p, C.c_size_t,
                                        C.c_void_p, P(C.c_uint32), C.c_int, P(C.c_uint64)]
         L.orc_extend_batch.restype = C.c_int
@@ -266,6 +272,43 @@ def cigar_batch(sc: Scoring, bases: np.ndarray, tasks: np.ndarray, pac=None, n_t
     if rc != 0:
         raise ValueError("cigar_batch failed")
     return res, cig, np.frombuffer(md.raw, np.uint8), cells.value
+
+
+class FMIndex:
+    """The FM index of a forward strand as the reference loads it (BWT.swift):
+    checkpoints, count[5], length, sentinel."""
+
+    def __init__(self, cp, count, length, sentinel):
+        self.cp, self.count, self.length, self.sentinel = cp, count, int(length), int(sentinel)
+
+
+def bwt_build(codes: np.ndarray) -> FMIndex:
+    """FM index of `codes` (0-3) and its reverse complement, with '$' (test infrastructure)."""
+    codes = np.ascontiguousarray(codes, dtype=np.uint8)
+    n = codes.size
+    n_cp = ((2 * n + 1) >> 6) + 1
+    cp = np.zeros(n_cp, BWT_CHECKPOINT_DTYPE)
+    count = np.zeros(5, np.int64)
+    length, sentinel = C.c_int64(), C.c_int64()
+    rc = lib().orc_bwt_build(ptr(codes), n, cp.ctypes.data, n_cp, count.ctypes.data_as(C.POINTER(C.c_int64)),
+                             C.byref(length), C.byref(sentinel), 1)
+    if rc != 0:
+        raise ValueError(f"bwt_build failed ({rc})")
+    return FMIndex(cp, count, length.value, sentinel.value)
+
+
+def smem_batch(idx: FMIndex, bases: np.ndarray, read_off: np.ndarray, read_len: np.ndarray, min_seed_len: int,
+               min_intv: int = 1, cap: int = 64, n_threads: int = 1):
+    """SMEMFinder.findAllSMEMs per read -> (SMEM_DTYPE [n_reads * cap], n_out, reads over cap)."""
+    read_off = np.ascontiguousarray(read_off, dtype=np.uint64)
+    read_len = np.ascontiguousarray(read_len, dtype=np.int32)
+    n = read_off.size
+    out = np.zeros(max(n * cap, 1), SMEM_DTYPE)
+    n_out = np.zeros(n, np.uint32)
+    over = lib().orc_smem_batch(idx.cp.ctypes.data, idx.count.ctypes.data_as(C.POINTER(C.c_int64)), idx.length,
+                                idx.sentinel, ptr(bases), read_off.ctypes.data, read_len.ctypes.data, n,
+                                min_seed_len, min_intv, cap, out.ctypes.data, n_out.ctypes.data, n_threads)
+    return out, n_out, int(over)
 
 
 def local_batch(sc: Scoring, bases: np.ndarray, tasks: np.ndarray, pac=None, ref_bases=0,

@@ -1549,3 +1549,222 @@ int orc_mate_rescue_batch(const swb_scoring *sc, const uint8_t *bases, const uin
     if (cells) { *cells = 0; for (auto v : per) *cells += v; }
     return 0;
 }
+
+// --------------------------------------------------------------------------
+// FM index and SMEM finding -- Sources/FMIndex/BWT.swift, BackwardSearch.swift,
+// SMEMFinder.swift (bwa-mem2 FMI_search.cpp's backwardExt and
+// getSMEMsOnePosOneThread / getSMEMsAllPosOneThread).
+// --------------------------------------------------------------------------
+namespace {
+
+struct OrcBwt {
+    const swb_bwt_checkpoint *cp;
+    int64_t count[5];
+    int64_t length, sentinel;
+    // BWT.occ (BWT.swift:68-84): checkpoint count plus the set bits of the
+    // block before position y (oneHotMaskArray[y] = the top y bits).
+    int64_t occ(int64_t pos, int c) const {
+        const swb_bwt_checkpoint &k = cp[pos >> 6];
+        const int y = (int)(pos & 63);
+        const uint64_t mask = y == 0 ? 0ull : ~(~0ull >> y);
+        return k.counts[c] + (int64_t)__builtin_popcountll(k.bits[c] & mask);
+    }
+};
+
+struct Intv {
+    int64_t k, l, s;
+};
+
+// BackwardSearch.backwardExt (BackwardSearch.swift:21-77).
+Intv backward_ext(const OrcBwt &b, int64_t k, int64_t l, int64_t s, int a) {
+    if (a >= 4) return {0, 0, 0};
+    const int64_t sp = k, ep = k + s;
+    int64_t kAll[4], sAll[4], lAll[4];
+    for (int c = 0; c < 4; ++c) {
+        const int64_t occSP = b.occ(sp, c), occEP = b.occ(ep, c);
+        kAll[c] = b.count[c] + occSP;
+        sAll[c] = occEP - occSP;
+    }
+    const int64_t sentinelOffset = (sp <= b.sentinel && ep > b.sentinel) ? 1 : 0;
+    lAll[3] = l + sentinelOffset;
+    lAll[2] = lAll[3] + sAll[3];
+    lAll[1] = lAll[2] + sAll[2];
+    lAll[0] = lAll[1] + sAll[1];
+    return {kAll[a], lAll[a], sAll[a]};
+}
+
+// SMEMFinder.BidiInterval (SMEMFinder.swift:67-73).
+struct Bidi {
+    int64_t k, l, s;
+    int32_t m, n;
+};
+
+// SMEMFinder.findSMEMsAtPosition (SMEMFinder.swift:89-268); returns nextPos.
+int find_smems_at(const OrcBwt &b, const uint8_t *query, int readLength, int startPos, int32_t minSeedLen,
+                  int64_t minIntv, std::vector<swb_smem> &smems, std::vector<Bidi> &prev) {
+    int nextPos = startPos + 1;
+    const int a = query[startPos];
+    if (a >= 4) return nextPos;                                              // :104-107
+    Bidi smem{b.count[a], b.count[3 - a], b.count[a + 1] - b.count[a], startPos, startPos};   // :111-117
+    prev.clear();
+    int numPrev = 0;
+    int j = startPos + 1;                                                    // :124-157
+    while (j < readLength) {
+        const int base = query[j];
+        nextPos = j + 1;
+        if (base >= 4) break;
+        const Intv ext = backward_ext(b, smem.l, smem.k, smem.s, 3 - base);   // swapped k/l, complement base
+        const Bidi newSmem{ext.l, ext.k, ext.s, smem.m, (int32_t)j};
+        if (newSmem.s != smem.s) {
+            prev.push_back(smem);
+            numPrev += 1;
+        }
+        if (newSmem.s < minIntv) {
+            nextPos = j;
+            break;
+        }
+        smem = newSmem;
+        j += 1;
+    }
+    if (smem.s >= minIntv) {                                                 // :160-163
+        prev.push_back(smem);
+        numPrev += 1;
+    }
+    std::reverse(prev.begin(), prev.end());                                  // :166
+    for (int bj = startPos - 1; bj >= 0; --bj) {                             // :169-250
+        const int base = query[bj];
+        if (base >= 4) break;
+        int numCurr = 0;
+        int64_t currS = -1;
+        int p = 0;
+        while (p < numPrev) {
+            const Bidi iv = prev[p];
+            const Intv ext = backward_ext(b, iv.k, iv.l, iv.s, base);
+            const Bidi ni{ext.k, ext.l, ext.s, (int32_t)bj, iv.n};
+            if (ni.s < minIntv && (iv.n - iv.m + 1) >= minSeedLen) {          // condition 1
+                smems.push_back(swb_smem{iv.k, iv.k + iv.s - 1, iv.m, iv.n + 1});
+                break;
+            }
+            if (ni.s >= minIntv && ni.s != currS) {                          // condition 2
+                currS = ni.s;
+                if (numCurr < (int)prev.size()) prev[numCurr] = ni;
+                else prev.push_back(ni);
+                numCurr += 1;
+                break;
+            }
+            p += 1;
+        }
+        p += 1;
+        while (p < numPrev) {
+            const Bidi iv = prev[p];
+            const Intv ext = backward_ext(b, iv.k, iv.l, iv.s, base);
+            const Bidi ni{ext.k, ext.l, ext.s, (int32_t)bj, iv.n};
+            if (ni.s >= minIntv && ni.s != currS) {
+                currS = ni.s;
+                if (numCurr < (int)prev.size()) prev[numCurr] = ni;
+                else prev.push_back(ni);
+                numCurr += 1;
+            }
+            p += 1;
+        }
+        numPrev = numCurr;
+        if (numCurr == 0) break;
+    }
+    if (numPrev != 0) {                                                      // :253-265
+        const Bidi iv = prev[0];
+        if ((iv.n - iv.m + 1) >= minSeedLen) smems.push_back(swb_smem{iv.k, iv.k + iv.s - 1, iv.m, iv.n + 1});
+    }
+    return nextPos;
+}
+
+// SMEMFinder.findAllSMEMs (SMEMFinder.swift:28-63): every start position in
+// turn, then sorted by query begin, longer first.
+void find_all_smems(const OrcBwt &b, const uint8_t *query, int readLength, int32_t minSeedLen, int64_t minIntv,
+                    std::vector<swb_smem> &out) {
+    out.clear();
+    std::vector<Bidi> prev;
+    int pos = 0;
+    while (pos < readLength) pos = find_smems_at(b, query, readLength, pos, minSeedLen, minIntv, out, prev);
+    std::stable_sort(out.begin(), out.end(), [](const swb_smem &x, const swb_smem &y) {
+        if (x.qb != y.qb) return x.qb < y.qb;
+        return (x.qe - x.qb) > (y.qe - y.qb);
+    });
+}
+
+}  // namespace
+
+// FM index of a forward strand (codes 0-3) in the layout the reference
+// loads (BWT.swift, CheckpointOCC.swift): the text is the strand followed by
+// its reverse complement, then '$'; SA by prefix doubling; BWT[i] =
+// text[SA[i]-1] ('$' where SA[i] = 0: the sentinel position); count[c] =
+// 1 + the characters below c; a checkpoint per 64 BWT positions.  Test
+// infrastructure: builds the indexes of the synthetic references.
+int orc_bwt_build(const uint8_t *codes, int64_t n, swb_bwt_checkpoint *cp, int64_t n_cp, int64_t count_out[5],
+                  int64_t *length_out, int64_t *sentinel_out, int n_threads) {
+    (void)n_threads;
+    const int64_t N = 2 * n + 1;
+    if (n_cp < (N >> 6) + 1) return -1;
+    std::vector<uint8_t> T((size_t)N);
+    for (int64_t i = 0; i < n; ++i) {
+        if (codes[i] > 3) return -2;
+        T[(size_t)i] = (uint8_t)(codes[i] + 1);
+        T[(size_t)(n + i)] = (uint8_t)(3 - codes[n - 1 - i] + 1);
+    }
+    T[(size_t)(2 * n)] = 0;                                   // '$', smallest
+    // Prefix doubling: rank by the first h characters, h = 1, 2, 4, ...
+    std::vector<int32_t> sa((size_t)N), rank((size_t)N), tmp((size_t)N);
+    for (int64_t i = 0; i < N; ++i) { sa[(size_t)i] = (int32_t)i; rank[(size_t)i] = T[(size_t)i]; }
+    for (int64_t h = 1;; h <<= 1) {
+        auto key = [&](int32_t i) -> std::pair<int32_t, int32_t> {
+            return {rank[(size_t)i], i + h < N ? rank[(size_t)(i + h)] : -1};
+        };
+        std::sort(sa.begin(), sa.end(), [&](int32_t x, int32_t y) { return key(x) < key(y); });
+        tmp[(size_t)sa[0]] = 0;
+        for (int64_t r = 1; r < N; ++r)
+            tmp[(size_t)sa[(size_t)r]] = tmp[(size_t)sa[(size_t)(r - 1)]] + (key(sa[(size_t)(r - 1)]) < key(sa[(size_t)r]) ? 1 : 0);
+        rank.swap(tmp);
+        if (rank[(size_t)sa[(size_t)(N - 1)]] == N - 1) break;
+    }
+    int64_t cnt[5] = {0, 0, 0, 0, 0};
+    for (int64_t i = 0; i < 2 * n; ++i) cnt[T[(size_t)i]] += 1;        // cnt[c+1] = occurrences of base c
+    count_out[0] = 1;
+    for (int c = 1; c <= 4; ++c) count_out[c] = count_out[c - 1] + cnt[c];
+    int64_t run[4] = {0, 0, 0, 0};
+    int64_t sentinel = -1;
+    for (int64_t b = 0; b < n_cp; ++b) {
+        for (int c = 0; c < 4; ++c) { cp[b].counts[c] = run[c]; cp[b].bits[c] = 0; }
+        for (int y = 0; y < 64; ++y) {
+            const int64_t i = b * 64 + y;
+            if (i >= N) break;
+            const int32_t s = sa[(size_t)i];
+            if (s == 0) { sentinel = i; continue; }
+            const int c = T[(size_t)(s - 1)] - 1;
+            cp[b].bits[c] |= 1ull << (63 - y);
+            run[c] += 1;
+        }
+    }
+    *length_out = N;
+    *sentinel_out = sentinel;
+    return 0;
+}
+
+// findAllSMEMs over a batch of reads (host threads); the output layout of
+// swb_smem_batch: read r's SMEMs at out[r * cap ..+ n_out[r]] (the first cap
+// kept when there are more).  Returns the number of reads with more than cap.
+int64_t orc_smem_batch(const swb_bwt_checkpoint *cp, const int64_t count[5], int64_t length, int64_t sentinel,
+                       const uint8_t *bases, const uint64_t *read_off, const int32_t *read_len, size_t n_reads,
+                       int32_t min_seed_len, int64_t min_intv, uint32_t cap, swb_smem *out, uint32_t *n_out,
+                       int n_threads) {
+    OrcBwt b{cp, {count[0], count[1], count[2], count[3], count[4]}, length, sentinel};
+    std::atomic<int64_t> over{0};
+    parallel_for(n_reads, n_threads, [&](size_t lo, size_t hi, int) {
+        std::vector<swb_smem> v;
+        for (size_t r = lo; r < hi; ++r) {
+            find_all_smems(b, bases + read_off[r], read_len[r], min_seed_len, min_intv, v);
+            n_out[r] = (uint32_t)v.size();
+            if (v.size() > cap) over += 1;
+            std::copy(v.begin(), v.begin() + std::min<size_t>(v.size(), cap), out + r * (size_t)cap);
+        }
+    });
+    return over.load();
+}

@@ -133,6 +133,13 @@ int orc_mate_rescue_batch(const swb_scoring *sc, const uint8_t *bases, const uin
                           const int64_t *contig_offsets, const int32_t *contig_lengths, size_t n_contigs,
                           swb_rescued *out, uint32_t *n_out, uint32_t *n_cand, int n_threads, uint64_t *cells);
 
+int orc_bwt_build(const uint8_t *codes, int64_t n, swb_bwt_checkpoint *cp, int64_t n_cp, int64_t count_out[5],
+                  int64_t *length_out, int64_t *sentinel_out, int n_threads);
+int64_t orc_smem_batch(const swb_bwt_checkpoint *cp, const int64_t count[5], int64_t length, int64_t sentinel,
+                       const uint8_t *bases, const uint64_t *read_off, const int32_t *read_len, size_t n_reads,
+                       int32_t min_seed_len, int64_t min_intv, uint32_t cap, swb_smem *out, uint32_t *n_out,
+                       int n_threads);
+
 #ifdef __cplusplus
 }
 #endif

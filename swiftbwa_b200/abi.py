@@ -122,6 +122,10 @@ assert SEED_DTYPE.itemsize == 24 and CHAIN_DTYPE.itemsize == 24 and REGION_DTYPE
 assert EXT_TASK_DTYPE.itemsize == C.sizeof(ExtTask) == 40
 assert GLOBAL_TASK_DTYPE.itemsize == C.sizeof(GlobalTask) == 40
 assert LOCAL_TASK_DTYPE.itemsize == C.sizeof(LocalTask) == 32
+# CheckpointOCC and SMEM (swb_bwt_checkpoint, swb_smem).
+BWT_CHECKPOINT_DTYPE = np.dtype([("counts", "<i8", (4,)), ("bits", "<u8", (4,))])
+SMEM_DTYPE = np.dtype([("k", "<i8"), ("l", "<i8"), ("qb", "<i4"), ("qe", "<i4")])
+assert BWT_CHECKPOINT_DTYPE.itemsize == 64 and SMEM_DTYPE.itemsize == 24
 assert GLOBAL_RESULT_DTYPE.itemsize == C.sizeof(GlobalResult) == 24
 assert EXT_RESULT_DTYPE.itemsize == C.sizeof(ExtResult) == 24
 assert LOCAL_RESULT_DTYPE.itemsize == C.sizeof(LocalResult) == 24
@@ -136,6 +140,7 @@ EXPORTED_SYMBOLS = (
     "swb_profile_read", "swb_int_alu_peak", "swb_int16x2_alu_peak", "swb_set_ext_bins", "swb_get_ext_bins", "swb_tune_ext_bins", "swb_ext_batch_static", "swb_cigar_batch",
     "swb_server_start", "swb_server_submit", "swb_server_poll", "swb_server_wait", "swb_server_resume",
     "swb_server_stats_get", "swb_server_stop", "swb_extend_chains", "swb_mate_rescue",
+    "swb_upload_bwt", "swb_smem_batch",
 )
 
 
@@ -201,6 +206,10 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.swb_ext_batch_device.restype = C.c_int
     lib.swb_ext_batch_plain_device.argtypes = [vp, P(Scoring), vp, vp, C.c_size_t, vp, vp]
     lib.swb_ext_batch_plain_device.restype = C.c_int
+    lib.swb_upload_bwt.argtypes = [vp, vp, C.c_uint64, P(C.c_int64), C.c_int64, C.c_int64]
+    lib.swb_upload_bwt.restype = C.c_int
+    lib.swb_smem_batch.argtypes = [vp, vp, C.c_size_t, vp, vp, C.c_size_t, C.c_int32, C.c_int64, C.c_uint32, vp, vp]
+    lib.swb_smem_batch.restype = C.c_int
     lib.swb_banded_sw_align.argtypes = [vp, u8p, C.c_int32, u8p, C.c_int32, P(Scoring),
                                         C.c_int32, C.c_int32, C.c_int32, P(ExtResult)]
     lib.swb_banded_sw_align.restype = C.c_int

@@ -26,8 +26,8 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import abi
-from .abi import (EXT_RESULT_DTYPE, EXT_TASK_DTYPE, GLOBAL_RESULT_DTYPE, GLOBAL_TASK_DTYPE,
-                  LOCAL_RESULT_DTYPE, LOCAL_TASK_DTYPE, ExtResult, LocalResult, Scoring, ptr)
+from .abi import (BWT_CHECKPOINT_DTYPE, EXT_RESULT_DTYPE, EXT_TASK_DTYPE, GLOBAL_RESULT_DTYPE, GLOBAL_TASK_DTYPE,
+                  LOCAL_RESULT_DTYPE, LOCAL_TASK_DTYPE, SMEM_DTYPE, ExtResult, LocalResult, Scoring, ptr)
 
 
 class SWBError(RuntimeError):
@@ -295,6 +295,32 @@ class Engine:
         """swb_ext_batch_device on device pointers (HBM-resident inputs)."""
         _check(self.lib.swb_ext_batch_device(self.h, C.byref(sc), C.c_void_p(d_bases), C.c_void_p(d_tasks), n,
                                              C.c_void_p(d_out), C.c_void_p(stream)), "swb_ext_batch_device")
+
+    # ------------------------------------------------------- SMEM seeding
+    def upload_bwt(self, cp: np.ndarray, count: np.ndarray, length: int, sentinel: int):
+        """Keeps an FM index resident (BWT.swift's fields): checkpoints
+        (BWT_CHECKPOINT_DTYPE), count[5], length, sentinel."""
+        assert cp.dtype == BWT_CHECKPOINT_DTYPE
+        cp = np.ascontiguousarray(cp)
+        cnt = np.ascontiguousarray(count, dtype=np.int64)
+        _check(self.lib.swb_upload_bwt(self.h, cp.ctypes.data, cp.size, cnt.ctypes.data_as(C.POINTER(C.c_int64)),
+                                       int(length), int(sentinel)), "swb_upload_bwt")
+
+    def smem_batch(self, bases: np.ndarray, read_off: np.ndarray, read_len: np.ndarray, min_seed_len: int,
+                   min_intv: int = 1, cap_per_read: int = 64):
+        """SMEMFinder.findAllSMEMs per read on the resident FM index ->
+        (SMEM_DTYPE [n_reads * cap_per_read], n_out); read r's SMEMs are
+        out[r * cap : r * cap + n_out[r]]."""
+        bases = np.ascontiguousarray(bases, dtype=np.uint8)
+        read_off = np.ascontiguousarray(read_off, dtype=np.uint64)
+        read_len = np.ascontiguousarray(read_len, dtype=np.int32)
+        n = read_off.size
+        out = np.zeros(max(n * cap_per_read, 1), SMEM_DTYPE)
+        n_out = np.zeros(max(n, 1), np.uint32)
+        _check(self.lib.swb_smem_batch(self.h, ptr(bases), bases.size, read_off.ctypes.data, read_len.ctypes.data, n,
+                                       int(min_seed_len), int(min_intv), int(cap_per_read), out.ctypes.data,
+                                       n_out.ctypes.data), "swb_smem_batch")
+        return out, n_out[:n]
 
     def ext_batch_plain_device(self, sc: Scoring, d_bases: int, d_tasks: int, n: int, d_out: int, stream: int = 0):
         """swb_ext_batch_plain_device: the plain one-launch-per-batch kernel (the

@@ -21,7 +21,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "libswb_cuda.so")
 SOURCES = ["swb_runtime.cu", "swb_ext.cu", "swb_global.cu", "swb_local.cu", "swb_probe.cu", "swb_noalloc.cu",
-           "swb_cigar.cu", "swb_serve.cu", "swb_extend.cu", "swb_rescue.cu"]
+           "swb_cigar.cu", "swb_serve.cu", "swb_extend.cu", "swb_rescue.cu", "swb_seed.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3"]
 

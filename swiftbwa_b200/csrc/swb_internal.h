@@ -55,6 +55,7 @@ enum CounterIdx {
     kCntGlobal = 32,
     kCntLocalStriped = 33,
     kCntLocalScalar = 34,
+    kCntSeed = 35,        // backward extensions of the SMEM search
     kNumCounters = 40
 };
 
@@ -111,6 +112,11 @@ struct swb_ctx {
     swb::DevBuf d_bases, d_tasks, d_out, d_keys, d_keys2, d_idx, d_idx2, d_sort_tmp, d_misc,
         d_scratch, d_cigar, d_aux, d_chain;
     swb::HostBuf h_in, h_out;
+    // resident FM index (swb_upload_bwt): checkpoints, counts, length, sentinel
+    swb::DevBuf d_bwt, d_seed;
+    int64_t bwt_count[5] = {0, 0, 0, 0, 0};
+    int64_t bwt_length = 0, bwt_sentinel = -1;
+    uint64_t bwt_ncp = 0;
     unsigned long long launches = 0;
     double last_ms = 0.0;
     unsigned long long last_cells = 0;

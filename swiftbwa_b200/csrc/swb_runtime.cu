@@ -426,7 +426,8 @@ void swb_destroy(swb_ctx *ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     DevBuf *bufs[] = {&ctx->d_bases, &ctx->d_tasks, &ctx->d_out, &ctx->d_keys, &ctx->d_keys2, &ctx->d_idx,
-                      &ctx->d_idx2, &ctx->d_sort_tmp, &ctx->d_misc, &ctx->d_scratch, &ctx->d_cigar, &ctx->d_aux, &ctx->d_chain};
+                      &ctx->d_idx2, &ctx->d_sort_tmp, &ctx->d_misc, &ctx->d_scratch, &ctx->d_cigar, &ctx->d_aux, &ctx->d_chain,
+                      &ctx->d_bwt, &ctx->d_seed};
     for (DevBuf *b : bufs) free_buf(ctx, *b);
     if (ctx->d_pac && ctx->pac_owned) cudaFree(ctx->d_pac);
     if (ctx->d_counters) cudaFree(ctx->d_counters);

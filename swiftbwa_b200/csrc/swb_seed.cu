@@ -1,0 +1,361 @@
+// swb_seed.cu -- SMEM seeding on the resident FM index, bit-exact with
+// SMEMFinder.findAllSMEMs (Sources/FMIndex/SMEMFinder.swift:28-268) over
+// BWT.occ (Sources/FMIndex/BWT.swift:68-84) and BackwardSearch.backwardExt
+// (Sources/FMIndex/BackwardSearch.swift:21-77).
+//
+// One thread owns one read and walks its start positions in the reference's
+// order (each start's forward phase decides the next start), so the SMEMs,
+// their order and their SA intervals are the reference's.  The work is a
+// chain of rank queries into the checkpoint array (64 bytes per 64 BWT
+// positions, at most 2 checkpoints per backward extension): random reads
+// over the resident index, so the kernel is bound by memory latency and
+// keeps as many reads in flight as the SMs hold threads.  Warps claim 32
+// reads at a time from a counter.  Each thread's list of candidate
+// intervals (at most one per query base) lives in a column of global
+// scratch laid out [entry][thread], so a warp's threads touch adjacent
+// words when they are at the same entry.  A read's SMEMs go to its own
+// output window in the order found and are then sorted there (query begin,
+// longer first), as the reference sorts its array.
+#include <algorithm>
+
+#include "swb_internal.h"
+
+namespace swb {
+namespace {
+
+constexpr int kSeedT = 128;   // threads per block
+
+struct SeedArgs {
+    const swb_bwt_checkpoint *cp;
+    int64_t count[5];
+    int64_t sentinel;
+    const uint8_t *bases;
+    const uint64_t *read_off;
+    const int32_t *read_len;
+    uint32_t n_reads;
+    int32_t min_seed_len;
+    int64_t min_intv;
+    uint32_t cap;
+    swb_smem *out;
+    uint32_t *n_out;
+    uint32_t *claim;            // next unclaimed read
+    uint32_t *first_over;       // lowest read index with more SMEMs than cap (~0 = none)
+    unsigned long long *exts;   // backward extensions (work counter)
+    // candidate intervals, [entry][slot]
+    int64_t *pk, *pl, *ps;
+    int2 *pmn;
+    size_t nslots;
+};
+
+struct Intv {
+    int64_t k, l, s;
+};
+
+// Ranks of the four bases before BWT position pos (BWT.occ for c = 0..3):
+// the checkpoint's counts plus the set bits of the block before pos.
+__device__ __forceinline__ void occ4(const swb_bwt_checkpoint *__restrict__ cp, int64_t pos, int64_t o[4]) {
+    const longlong2 *p = reinterpret_cast<const longlong2 *>(cp + (pos >> 6));
+    const longlong2 c01 = __ldg(p), c23 = __ldg(p + 1), b01 = __ldg(p + 2), b23 = __ldg(p + 3);
+    const int y = (int)(pos & 63);
+    const unsigned long long mask = y == 0 ? 0ull : ~(~0ull >> y);   // oneHotMaskArray[y]: the top y bits
+    o[0] = c01.x + __popcll((unsigned long long)b01.x & mask);
+    o[1] = c01.y + __popcll((unsigned long long)b01.y & mask);
+    o[2] = c23.x + __popcll((unsigned long long)b23.x & mask);
+    o[3] = c23.y + __popcll((unsigned long long)b23.y & mask);
+}
+
+// BackwardSearch.backwardExt: the interval of base a prepended (a < 4).
+__device__ __forceinline__ Intv backward_ext(const SeedArgs &g, int64_t k, int64_t l, int64_t s, int a) {
+    const int64_t sp = k, ep = k + s;
+    int64_t osp[4], oep[4];
+    occ4(g.cp, sp, osp);
+    if ((sp >> 6) == (ep >> 6)) {
+        // Same block: the ranks at ep add the bits between sp and ep.
+        const swb_bwt_checkpoint *c = g.cp + (sp >> 6);
+        const int ys = (int)(sp & 63), ye = (int)(ep & 63);
+        const unsigned long long m = (ye == 0 ? 0ull : ~(~0ull >> ye)) & ~(ys == 0 ? 0ull : ~(~0ull >> ys));
+        const longlong2 *p = reinterpret_cast<const longlong2 *>(c);
+        const longlong2 b01 = __ldg(p + 2), b23 = __ldg(p + 3);
+        oep[0] = osp[0] + __popcll((unsigned long long)b01.x & m);
+        oep[1] = osp[1] + __popcll((unsigned long long)b01.y & m);
+        oep[2] = osp[2] + __popcll((unsigned long long)b23.x & m);
+        oep[3] = osp[3] + __popcll((unsigned long long)b23.y & m);
+    } else {
+        occ4(g.cp, ep, oep);
+    }
+    const int64_t s0 = oep[0] - osp[0], s1 = oep[1] - osp[1], s2 = oep[2] - osp[2], s3 = oep[3] - osp[3];
+    const int64_t sentinelOffset = (sp <= g.sentinel && ep > g.sentinel) ? 1 : 0;
+    const int64_t l3 = l + sentinelOffset, l2 = l3 + s3, l1 = l2 + s2, l0 = l1 + s1;
+    switch (a) {
+        case 0: return {g.count[0] + osp[0], l0, s0};
+        case 1: return {g.count[1] + osp[1], l1, s1};
+        case 2: return {g.count[2] + osp[2], l2, s2};
+        default: return {g.count[3] + osp[3], l3, s3};
+    }
+}
+
+struct Cand {   // SMEMFinder.BidiInterval
+    int64_t k, l, s;
+    int32_t m, n;
+};
+
+struct Prev {
+    const SeedArgs &g;
+    size_t slot;
+    __device__ __forceinline__ Cand get(int e) const {
+        const size_t i = (size_t)e * g.nslots + slot;
+        const int2 mn = g.pmn[i];
+        return {g.pk[i], g.pl[i], g.ps[i], mn.x, mn.y};
+    }
+    __device__ __forceinline__ void put(int e, const Cand &c) const {
+        const size_t i = (size_t)e * g.nslots + slot;
+        g.pk[i] = c.k;
+        g.pl[i] = c.l;
+        g.ps[i] = c.s;
+        g.pmn[i] = make_int2(c.m, c.n);
+    }
+};
+
+struct Emit {
+    swb_smem *w;      // the read's window
+    uint32_t cap, n = 0;
+    __device__ __forceinline__ void add(const Cand &c) {
+        if (n < cap) w[n] = swb_smem{c.k, c.k + c.s - 1, c.m, c.n + 1};
+        ++n;
+    }
+};
+
+// SMEMFinder.findSMEMsAtPosition (SMEMFinder.swift:89-268); returns nextPos.
+__device__ int smems_at(const SeedArgs &g, const uint8_t *__restrict__ q, int readLength, int startPos,
+                        const Prev &prev, Emit &emit, unsigned long long &exts) {
+    int nextPos = startPos + 1;
+    const int a = q[startPos];
+    if (a >= 4) return nextPos;                                              // :104-107
+    Cand smem{g.count[a], g.count[3 - a], g.count[a + 1] - g.count[a], startPos, startPos};
+    int numPrev = 0;
+    for (int j = startPos + 1; j < readLength; ++j) {                        // :124-157
+        const int base = q[j];
+        nextPos = j + 1;
+        if (base >= 4) break;
+        // Forward extension: backward extension with k/l swapped and the complement base.
+        const Intv ext = backward_ext(g, smem.l, smem.k, smem.s, 3 - base);
+        ++exts;
+        if (ext.s != smem.s) prev.put(numPrev++, smem);
+        if (ext.s < g.min_intv) {
+            nextPos = j;
+            break;
+        }
+        smem = Cand{ext.l, ext.k, ext.s, smem.m, j};
+    }
+    if (smem.s >= g.min_intv) prev.put(numPrev++, smem);                     // :160-163
+    for (int x = 0, y = numPrev - 1; x < y; ++x, --y) {                      // :166 (longest first)
+        const Cand cx = prev.get(x), cy = prev.get(y);
+        prev.put(x, cy);
+        prev.put(y, cx);
+    }
+    for (int bj = startPos - 1; bj >= 0; --bj) {                             // :169-250
+        const int base = q[bj];
+        if (base >= 4) break;
+        int numCurr = 0;
+        int64_t currS = -1;
+        int p = 0;
+        for (; p < numPrev; ++p) {
+            const Cand iv = prev.get(p);
+            const Intv ext = backward_ext(g, iv.k, iv.l, iv.s, base);
+            ++exts;
+            if (ext.s < g.min_intv && (iv.n - iv.m + 1) >= g.min_seed_len) { // condition 1: emit, stop
+                emit.add(iv);
+                break;
+            }
+            if (ext.s >= g.min_intv && ext.s != currS) {                     // condition 2: keep, stop
+                currS = ext.s;
+                prev.put(numCurr++, Cand{ext.k, ext.l, ext.s, bj, iv.n});
+                break;
+            }
+        }
+        for (p += 1; p < numPrev; ++p) {                                     // :231-246
+            const Cand iv = prev.get(p);
+            const Intv ext = backward_ext(g, iv.k, iv.l, iv.s, base);
+            ++exts;
+            if (ext.s >= g.min_intv && ext.s != currS) {
+                currS = ext.s;
+                prev.put(numCurr++, Cand{ext.k, ext.l, ext.s, bj, iv.n});
+            }
+        }
+        numPrev = numCurr;
+        if (numCurr == 0) break;
+    }
+    if (numPrev != 0) {                                                      // :253-265
+        const Cand iv = prev.get(0);
+        if ((iv.n - iv.m + 1) >= g.min_seed_len) emit.add(iv);
+    }
+    return nextPos;
+}
+
+__global__ void __launch_bounds__(kSeedT) smem_kernel(SeedArgs g) {
+    const size_t slot = blockIdx.x * (size_t)kSeedT + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const Prev prev{g, slot};
+    unsigned long long exts = 0;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(g.claim, 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= g.n_reads) break;
+        const uint32_t r = base + lane;
+        if (r < g.n_reads) {
+            const uint8_t *q = g.bases + g.read_off[r];
+            const int len = g.read_len[r];
+            Emit emit{g.out + (size_t)r * g.cap, g.cap};
+            for (int pos = 0; pos < len;) pos = smems_at(g, q, len, pos, prev, emit, exts);   // :41-51
+            g.n_out[r] = emit.n;
+            if (emit.n > g.cap) {
+                atomicMin(g.first_over, r);
+            } else {
+                // Sort by query begin, longer first (:53-58); equal keys are equal SMEMs.
+                swb_smem *w = emit.w;
+                for (uint32_t i = 1; i < emit.n; ++i) {
+                    const swb_smem x = w[i];
+                    uint32_t j = i;
+                    while (j > 0 && (w[j - 1].qb > x.qb || (w[j - 1].qb == x.qb && w[j - 1].qe - w[j - 1].qb < x.qe - x.qb))) {
+                        w[j] = w[j - 1];
+                        --j;
+                    }
+                    w[j] = x;
+                }
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) exts += __shfl_down_sync(0xFFFFFFFFu, exts, o);
+    if (lane == 0 && exts) atomicAdd(g.exts, exts);
+}
+
+}  // namespace
+}  // namespace swb
+
+using namespace swb;
+
+extern "C" {
+
+int swb_upload_bwt(swb_ctx *ctx, const swb_bwt_checkpoint *cp, uint64_t n_cp, const int64_t count[5], int64_t length,
+                   int64_t sentinel) {
+    if (!ctx || !count || (!cp && n_cp)) return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
+    if (length < 1 || n_cp < (uint64_t)(length >> 6) + 1 || sentinel < 0 || sentinel >= length || count[4] != length)
+        return set_error(SWB_ERR_INVALID_ARG, "BWT: need length >= 1, (length >> 6) + 1 checkpoints, "
+                                              "0 <= sentinel < length and count[4] == length");
+    for (int c = 0; c < 4; ++c)
+        if (count[c] < 0 || count[c] > count[c + 1]) return set_error(SWB_ERR_INVALID_ARG, "BWT: counts must ascend");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    SWB_CUDA(cudaSetDevice(ctx->device));
+    int rc;
+    if ((rc = ensure_dev(ctx, ctx->d_bwt, n_cp * sizeof(swb_bwt_checkpoint)))) return rc;
+    SWB_CUDA(cudaMemcpy(ctx->d_bwt.p, cp, n_cp * sizeof(swb_bwt_checkpoint), cudaMemcpyHostToDevice));
+    for (int c = 0; c < 5; ++c) ctx->bwt_count[c] = count[c];
+    ctx->bwt_length = length;
+    ctx->bwt_sentinel = sentinel;
+    ctx->bwt_ncp = n_cp;
+    return SWB_OK;
+}
+
+int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uint64_t *read_off,
+                   const int32_t *read_len, size_t n_reads, int32_t min_seed_len, int64_t min_intv,
+                   uint32_t cap_per_read, swb_smem *out, uint32_t *n_out) {
+    if (!ctx || (n_reads && (!read_off || !read_len || !n_out || (!out && cap_per_read))) || (!bases && n_bases))
+        return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
+    if (n_reads > 0xFFFFFFF0ull) return set_error(SWB_ERR_TOO_LARGE, "more than 2^32-16 reads in one batch");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->last_ms = 0;
+    ctx->last_cells = 0;
+    if (n_reads == 0) return SWB_OK;
+    if (ctx->bwt_ncp == 0) return set_error(SWB_ERR_NO_REFERENCE, "no FM index uploaded (swb_upload_bwt)");
+    int max_len = 0;
+    for (size_t r = 0; r < n_reads; ++r) {
+        if (read_len[r] < 0 || read_len[r] > kMaxLen)
+            return set_error(SWB_ERR_TOO_LARGE, "read " + std::to_string(r) + ": length outside 0..65535");
+        if (read_off[r] + (uint64_t)read_len[r] > n_bases)
+            return set_error(SWB_ERR_INVALID_ARG, "read " + std::to_string(r) + ": span outside the bases buffer");
+        max_len = std::max(max_len, read_len[r]);
+    }
+    SWB_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t b_bytes = al(n_bases), o_bytes = al(n_reads * 8), l_bytes = al(n_reads * 4);
+    const size_t out_bytes = al(n_reads * (size_t)cap_per_read * sizeof(swb_smem)), n_bytes = al(n_reads * 4);
+    int rc;
+    if ((rc = ensure_dev(ctx, ctx->d_bases, b_bytes + o_bytes + l_bytes + 256)) ||
+        (rc = ensure_dev(ctx, ctx->d_out, out_bytes + n_bytes + 256)))
+        return rc;
+    char *in = (char *)ctx->d_bases.p;
+    uint8_t *d_b = (uint8_t *)in;
+    uint64_t *d_off = (uint64_t *)(in + b_bytes);
+    int32_t *d_len = (int32_t *)(in + b_bytes + o_bytes);
+    uint32_t *d_misc = (uint32_t *)(in + b_bytes + o_bytes + l_bytes);   // claim, first_over
+    swb_smem *d_out = (swb_smem *)ctx->d_out.p;
+    uint32_t *d_n = (uint32_t *)((char *)ctx->d_out.p + out_bytes);
+    // Persistent grid: resident blocks on every SM, each thread with a
+    // candidate column of max_len entries (32 bytes each).
+    int per_sm = 0;
+    SWB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, smem_kernel, kSeedT, 0));
+    per_sm = std::max(per_sm, 1);
+    size_t blocks = std::min<size_t>((size_t)ctx->sm_count * per_sm, (n_reads + kSeedT - 1) / kSeedT);
+    const size_t entries = (size_t)std::max(max_len, 1);
+    const size_t per_slot = entries * 32;
+    const size_t avail = ctx->budget > ctx->allocated ? (ctx->budget - ctx->allocated) / 2 : 0;
+    while (blocks > 1 && blocks * kSeedT * per_slot > avail) blocks /= 2;
+    const size_t nslots = blocks * kSeedT;
+    if ((rc = ensure_dev(ctx, ctx->d_seed, nslots * per_slot + 256))) return rc;
+    char *sp = (char *)ctx->d_seed.p;
+    SeedArgs g{};
+    g.cp = (const swb_bwt_checkpoint *)ctx->d_bwt.p;
+    for (int c = 0; c < 5; ++c) g.count[c] = ctx->bwt_count[c];
+    g.sentinel = ctx->bwt_sentinel;
+    g.bases = d_b;
+    g.read_off = d_off;
+    g.read_len = d_len;
+    g.n_reads = (uint32_t)n_reads;
+    g.min_seed_len = min_seed_len;
+    g.min_intv = min_intv;
+    g.cap = cap_per_read;
+    g.out = d_out;
+    g.n_out = d_n;
+    g.claim = d_misc;
+    g.first_over = d_misc + 1;
+    g.pk = (int64_t *)sp;
+    g.pl = g.pk + entries * nslots;
+    g.ps = g.pl + entries * nslots;
+    g.pmn = (int2 *)(g.ps + entries * nslots);
+    g.nslots = nslots;
+    if (n_bases) SWB_CUDA(cudaMemcpyAsync(d_b, bases, n_bases, cudaMemcpyHostToDevice, st));
+    SWB_CUDA(cudaMemcpyAsync(d_off, read_off, n_reads * 8, cudaMemcpyHostToDevice, st));
+    SWB_CUDA(cudaMemcpyAsync(d_len, read_len, n_reads * 4, cudaMemcpyHostToDevice, st));
+    SWB_CUDA(cudaMemsetAsync(d_misc, 0, 4, st));
+    SWB_CUDA(cudaMemsetAsync(d_misc + 1, 0xFF, 4, st));
+    SWB_CUDA(cudaMemsetAsync(ctx->d_counters, 0, sizeof(unsigned long long) * kNumCounters, st));
+    g.exts = ctx->d_counters + kCntSeed;
+    SWB_CUDA(cudaEventRecord(ctx->ev_start, st));
+    {
+        ProfScope ps(ctx, st, "smem_search", kCntSeed);
+        smem_kernel<<<(unsigned)blocks, kSeedT, 0, st>>>(g);
+    }
+    ctx->launches++;
+    SWB_CUDA(cudaGetLastError());
+    SWB_CUDA(cudaEventRecord(ctx->ev_stop, st));
+    uint32_t first_over = 0;
+    SWB_CUDA(cudaMemcpyAsync(n_out, d_n, n_reads * 4, cudaMemcpyDeviceToHost, st));
+    if (cap_per_read)
+        SWB_CUDA(cudaMemcpyAsync(out, d_out, n_reads * (size_t)cap_per_read * sizeof(swb_smem), cudaMemcpyDeviceToHost, st));
+    SWB_CUDA(cudaMemcpyAsync(&first_over, d_misc + 1, 4, cudaMemcpyDeviceToHost, st));
+    SWB_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) ctx->last_ms = ms;
+    unsigned long long exts = 0;
+    if (cudaMemcpy(&exts, ctx->d_counters + kCntSeed, sizeof(exts), cudaMemcpyDeviceToHost) == cudaSuccess)
+        ctx->last_cells = exts;
+    if (first_over != 0xFFFFFFFFu)
+        return set_error(SWB_ERR_TOO_LARGE, "read " + std::to_string(first_over) + ": " +
+                                                std::to_string(n_out[first_over]) + " SMEMs, more than cap_per_read (" +
+                                                std::to_string(cap_per_read) + ")");
+    return SWB_OK;
+}
+
+}  // extern "C"

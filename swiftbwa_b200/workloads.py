@@ -263,3 +263,86 @@ def config3_jobs(rank: int = 0, n: int = 1_000_000, ref_len: int = 100_000_000) 
     wl = rescue_jobs(ref, SEED_BASE + 3 + 1000 * rank + 7, n, 150, n_contigs=24)
     wl.name = f"config3 rescue driver: {n} mates, {len(wl.templates)} template regions, {ref_len // 10**6} Mbp reference, 24 contigs"
     return wl
+
+
+# ------------------------------------------------------------ FM index (seeding)
+@dataclass
+class FMIndexData:
+    """An FM index in the layout the reference loads (BWT.swift, CheckpointOCC.swift)."""
+    cp: np.ndarray             # BWT_CHECKPOINT_DTYPE, (length >> 6) + 1 entries
+    count: np.ndarray          # int64[5]: 1 + the characters below each base; count[4] = length
+    length: int
+    sentinel: int
+
+
+def fm_index(codes: np.ndarray, device: str = "cuda") -> FMIndexData:
+    """FM index of a synthetic forward strand (codes 0-3): the text is the
+    strand, its reverse complement and '$'; the suffix array comes from
+    prefix doubling with torch sorts on `device` (ranks of 27-base prefixes
+    packed in base 5, then doubled until every suffix has its own rank), the
+    BWT is text[SA-1], and one checkpoint per 64 BWT positions holds the
+    base counts before it and one bitstring per base (bit 63-y for position
+    y).  Workload generation for the seeding tests and benchmark, not part of
+    the seeding path: the same arrays as the oracle's builder, faster."""
+    import torch
+    from .abi import BWT_CHECKPOINT_DTYPE
+    codes = np.ascontiguousarray(codes, dtype=np.uint8)
+    n = int(codes.size)
+    N = 2 * n + 1
+    T = np.empty(N, np.int64)
+    T[:n] = codes.astype(np.int64) + 1
+    T[n:2 * n] = 4 - codes[::-1].astype(np.int64)          # complement c -> 3 - c, then + 1
+    T[2 * n] = 0                                            # '$'
+    dev = torch.device(device)
+    t = torch.from_numpy(T).to(dev)
+    K = 27                                                  # 5**27 < 2**63
+    key = torch.zeros(N, dtype=torch.int64, device=dev)
+    for j in range(K):
+        nxt = torch.zeros(N, dtype=torch.int64, device=dev)
+        if j < N:
+            nxt[: N - j] = t[j:]
+        key = key * 5 + nxt
+    del t
+
+    def ranks_of(sorted_keys, order):
+        r = torch.empty(N, dtype=torch.int64, device=dev)
+        new = torch.ones(N, dtype=torch.int64, device=dev)
+        new[0] = 0
+        new[1:] = (sorted_keys[1:] != sorted_keys[:-1]).to(torch.int64)
+        r[order] = torch.cumsum(new, 0)
+        return r
+
+    sk, sa = torch.sort(key)
+    rank = ranks_of(sk, sa)
+    h = K
+    while int(rank.max()) < N - 1:
+        second = torch.zeros(N, dtype=torch.int64, device=dev)
+        if h < N:
+            second[: N - h] = rank[h:] + 1
+        key = rank * (N + 1) + second
+        sk, sa = torch.sort(key)
+        rank = ranks_of(sk, sa)
+        h *= 2
+    del key, sk, rank
+    tt = torch.from_numpy(T).to(dev)
+    prev = torch.where(sa > 0, tt[(sa - 1).clamp(min=0)], torch.zeros_like(sa))   # 0 = '$' (the sentinel)
+    sentinel = int(torch.nonzero(sa == 0)[0, 0])
+    n_cp = (N >> 6) + 1
+    pad = torch.zeros(n_cp * 64, dtype=torch.int64, device=dev)
+    pad[:N] = prev
+    blk = pad.view(n_cp, 64)
+    cp = np.zeros(n_cp, BWT_CHECKPOINT_DTYPE)
+    shift = (63 - torch.arange(64, device=dev, dtype=torch.int64))
+    for c in range(4):
+        m = (blk == c + 1).to(torch.int64)
+        cnt = m.sum(1)
+        before = torch.cumsum(cnt, 0) - cnt
+        cp["counts"][:, c] = before.cpu().numpy()
+        hi = (m[:, :32] << (shift[:32] - 32)).sum(1).cpu().numpy().astype(np.uint64)   # bits 63..32
+        lo = (m[:, 32:] << shift[32:]).sum(1).cpu().numpy().astype(np.uint64)          # bits 31..0
+        cp["bits"][:, c] = (hi << np.uint64(32)) | lo
+    tot = np.array([int(np.sum(codes == c)) + int(np.sum(codes == 3 - c)) for c in range(4)], np.int64)
+    count = np.zeros(5, np.int64)
+    count[0] = 1
+    count[1:] = 1 + np.cumsum(tot)
+    return FMIndexData(cp, count, N, sentinel)
