@@ -66,9 +66,11 @@ def parse():
     ap.add_argument("--tune-sample", type=int, default=0,
                     help="tasks the length-class autotuner times (0: the whole workload)")
     ap.add_argument("--c3-jobs", type=int, default=1_000_000)
+    ap.add_argument("--seed-reads", type=int, default=1_000_000, help="seeding: config-1 reads per SMEM batch")
     ap.add_argument("--suite-only", default="",
                     help="comma list of secondary configs to run alone (config0, config2, config3, config3_rescue_driver, "
-                         "config1_nw_cigar, config5_extend_chains, config4); prints their JSON and skips the headline")
+                         "config1_nw_cigar, config5_extend_chains, seeding, config4); prints their JSON and skips "
+                         "the headline")
     return ap.parse_args()
 
 
@@ -398,6 +400,54 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
             c5["bitexact_sample"] = f"{same}/{int(mask.sum())} regions, counts equal: {bool(ok)}"
         out["config5_extend_chains"] = c5
         del wl5, g5
+
+    # ---- seeding: SMEMFinder.findAllSMEMs over the config-1 reads (swb_smem_batch)
+    if want("seeding"):
+        wl6 = W.config1(n_reads=args.seed_reads, ref_len=args.ref_len)
+        t0 = time.perf_counter()
+        fm = W.fm_index(wl6.ref.codes, device=f"cuda:{dev.index or 0}")
+        build_s = time.perf_counter() - t0
+        torch.cuda.empty_cache()
+        eng.upload_bwt(fm.cp, fm.count, fm.length, fm.sentinel)
+        nr = args.seed_reads
+        L = wl6.read_len
+        off6 = np.arange(nr, dtype=np.uint64) * L
+        len6 = np.full(nr, L, np.int32)
+        cap6 = 64
+        eng.smem_batch(wl6.bases[: 10_000 * L], off6[:10_000], len6[:10_000], 19, cap_per_read=cap6)
+        times = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            sm6, n6 = eng.smem_batch(wl6.bases, off6, len6, 19, cap_per_read=cap6)
+            times.append(time.perf_counter() - t0)
+        e2e6 = float(np.median(times))
+        ms6, exts6 = eng.last_batch_stats()
+        # Bytes the rank queries read: one or two 64-byte checkpoints per
+        # backward extension, counted as 96 bytes (1.5 checkpoints) each.
+        c6 = {"reads": nr, "read_len": L, "smems": int(n6.sum()), "kernel_ms": ms6,
+              "reads_per_s_kernel": nr / ms6 * 1e3, "reads_per_s_e2e": nr / e2e6,
+              "smems_per_s_kernel": float(n6.sum()) / ms6 * 1e3,
+              "backward_extensions": int(exts6), "backward_ext_per_s": exts6 / ms6 * 1e3,
+              "index": f"{wl6.ref.n // 10**6} Mbp forward strand + reverse complement, {fm.cp.size} checkpoints "
+                       f"({fm.cp.nbytes / 1e6:.0f} MB resident, larger than L2), built in {build_s:.1f} s",
+              "approx_checkpoint_gbs": exts6 * 96 / ms6 / 1e6}
+        if cpu_on:
+            s6 = min(nr, 100_000)
+            t0 = time.perf_counter()
+            e6, en6, _ = oracle.smem_batch(oracle.FMIndex(fm.cp, fm.count, fm.length, fm.sentinel), wl6.bases,
+                                           off6[:s6], len6[:s6], 19, cap=cap6, n_threads=threads)
+            dt6 = time.perf_counter() - t0
+            c6["cpu_baseline"] = {"value": s6 / dt6, "unit": "reads/s", "cores": threads, "kind": "port",
+                                  "sample": f"first {s6} reads, SMEMFinder.findAllSMEMs restated, {threads} threads, "
+                                            f"{dt6:.1f} s"}
+            same6 = bool(np.array_equal(n6[:s6], en6))
+            for r in range(s6):
+                if not np.array_equal(sm6[r * cap6: r * cap6 + n6[r]], e6[r * cap6: r * cap6 + en6[r]]):
+                    same6 = False
+                    break
+            c6["bitexact_sample"] = f"{s6} reads: {'all equal' if same6 else 'DIFFERENT'}"
+        out["seeding"] = c6
+        del wl6, fm
 
     # ---- config 4: serving, Poisson 200 req/s, 1 Gbp resident reference
     if want("config4"):
