@@ -414,11 +414,15 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
         off6 = np.arange(nr, dtype=np.uint64) * L
         len6 = np.full(nr, L, np.int32)
         cap6 = 64
-        eng.smem_batch(wl6.bases[: 10_000 * L], off6[:10_000], len6[:10_000], 19, cap_per_read=cap6)
+        # Phases 1 and 1.25 of alignReadPhase1to3: findAllSMEMs, then internal
+        # re-seeding (split length Int(Float(19) * 1.5 + 0.499) = 28, split width 10).
+        split6 = oracle.split_len_of(19, 1.5)
+        eng.smem_batch(wl6.bases[: 10_000 * L], off6[:10_000], len6[:10_000], 19, cap_per_read=cap6,
+                       split_len=split6)
         times = []
         for _ in range(3):
             t0 = time.perf_counter()
-            sm6, n6 = eng.smem_batch(wl6.bases, off6, len6, 19, cap_per_read=cap6)
+            sm6, n6 = eng.smem_batch(wl6.bases, off6, len6, 19, cap_per_read=cap6, split_len=split6)
             times.append(time.perf_counter() - t0)
         e2e6 = float(np.median(times))
         ms6, exts6 = eng.last_batch_stats()
@@ -435,10 +439,12 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
             s6 = min(nr, 100_000)
             t0 = time.perf_counter()
             e6, en6, _ = oracle.smem_batch(oracle.FMIndex(fm.cp, fm.count, fm.length, fm.sentinel), wl6.bases,
-                                           off6[:s6], len6[:s6], 19, cap=cap6, n_threads=threads)
+                                           off6[:s6], len6[:s6], 19, cap=cap6, n_threads=threads,
+                                           split_len=split6, split_width=10)
             dt6 = time.perf_counter() - t0
             c6["cpu_baseline"] = {"value": s6 / dt6, "unit": "reads/s", "cores": threads, "kind": "port",
-                                  "sample": f"first {s6} reads, SMEMFinder.findAllSMEMs restated, {threads} threads, "
+                                  "sample": f"first {s6} reads, SMEMFinder.findAllSMEMs + internalReseed restated, "
+                                            f"{threads} threads, "
                                             f"{dt6:.1f} s"}
             same6 = bool(np.array_equal(n6[:s6], en6))
             for r in range(s6):

@@ -426,7 +426,13 @@ int swb_upload_bwt(swb_ctx *ctx, const swb_bwt_checkpoint *cp, uint64_t n_cp, co
                    int64_t length, int64_t sentinel);
 
 /* SMEMFinder.findAllSMEMs(query:bwt:minSeedLen:minIntv:) (SMEMFinder.swift:28-63)
- * for many reads on the resident BWT: read r is bases[read_off[r] ..+ read_len[r])
+ * for many reads on the resident BWT, followed, when split_len > 0, by the
+ * internal re-seeding of BWAMemAligner.internalReseed (BWAMemAligner.swift:259-305):
+ * every SMEM at least split_len long with at most split_width occurrences is
+ * searched again from its midpoint with minIntv = its count + 1 and the new
+ * SMEMs join the list (split_len = Int(Float(minSeedLength) * seedSplitRatio
+ * + 0.499) as the reference computes it, 28 for the defaults; split_width =
+ * splitWidth, 10).  Read r is bases[read_off[r] ..+ read_len[r])
  * (codes 0-4, N = 4).  Its SMEMs, sorted by query begin then longest first,
  * go to out[r * cap_per_read ..+ n_out[r]].  When a read has more than
  * cap_per_read SMEMs, n_out[r] still counts them all, its window holds the
@@ -437,7 +443,7 @@ int swb_upload_bwt(swb_ctx *ctx, const swb_bwt_checkpoint *cp, uint64_t n_cp, co
  * and the Metal forward kernel (Kernels/smem_forward.metal:117) for a batch. */
 int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uint64_t *read_off,
                    const int32_t *read_len, size_t n_reads, int32_t min_seed_len, int64_t min_intv,
-                   uint32_t cap_per_read, swb_smem *out, uint32_t *n_out);
+                   int32_t split_len, int32_t split_width, uint32_t cap_per_read, swb_smem *out, uint32_t *n_out);
 
 /* ------------------------------------------------ serving (continuous batching) */
 /* A request loop over one context's GPU for extension batches of differing

@@ -96,7 +96,8 @@ def lib() -> C.CDLL:
                                     P(C.c_int64), C.c_int]
         L.orc_bwt_build.restype = C.c_int
         L.orc_smem_batch.argtypes = [C.c_void_p, P(C.c_int64), C.c_int64, C.c_int64, u8p, C.c_void_p, C.c_void_p,
-                                     C.c_size_t, C.c_int32, C.c_int64, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int]
+                                     C.c_size_t, C.c_int32, C.c_int64, C.c_int32, C.c_int32, C.c_uint32, C.c_void_p,
+                                     C.c_void_p, C.c_int]
         L.orc_smem_batch.restype = C.c_int64
         L.orc_extend_batch.argtypes = [P(Scoring), u8p, u8p, C.c_int64, C.c_void_p, C.c_void_p, C.c_size_t,
                                        C.c_void_p, P(C.c_uint32), C.c_int, P(C.c_uint64)]
@@ -297,9 +298,17 @@ def bwt_build(codes: np.ndarray) -> FMIndex:
     return FMIndex(cp, count, length.value, sentinel.value)
 
 
+def split_len_of(min_seed_len: int, seed_split_ratio: float = 1.5) -> int:
+    """Int(Float(minSeedLength) * seedSplitRatio + 0.499) in single precision
+    (BWAMemAligner.swift:265): 28 for the defaults 19 and 1.5."""
+    f = np.float32(min_seed_len) * np.float32(seed_split_ratio)
+    return int(np.float32(f + np.float32(0.499)))
+
+
 def smem_batch(idx: FMIndex, bases: np.ndarray, read_off: np.ndarray, read_len: np.ndarray, min_seed_len: int,
-               min_intv: int = 1, cap: int = 64, n_threads: int = 1):
-    """SMEMFinder.findAllSMEMs per read -> (SMEM_DTYPE [n_reads * cap], n_out, reads over cap)."""
+               min_intv: int = 1, cap: int = 64, n_threads: int = 1, split_len: int = 0, split_width: int = 10):
+    """SMEMFinder.findAllSMEMs per read, then (split_len > 0) internalReseed ->
+    (SMEM_DTYPE [n_reads * cap], n_out, reads over cap)."""
     read_off = np.ascontiguousarray(read_off, dtype=np.uint64)
     read_len = np.ascontiguousarray(read_len, dtype=np.int32)
     n = read_off.size
@@ -307,7 +316,8 @@ def smem_batch(idx: FMIndex, bases: np.ndarray, read_off: np.ndarray, read_len: 
     n_out = np.zeros(n, np.uint32)
     over = lib().orc_smem_batch(idx.cp.ctypes.data, idx.count.ctypes.data_as(C.POINTER(C.c_int64)), idx.length,
                                 idx.sentinel, ptr(bases), read_off.ctypes.data, read_len.ctypes.data, n,
-                                min_seed_len, min_intv, cap, out.ctypes.data, n_out.ctypes.data, n_threads)
+                                min_seed_len, min_intv, split_len, split_width, cap, out.ctypes.data,
+                                n_out.ctypes.data, n_threads)
     return out, n_out, int(over)
 
 

@@ -1748,19 +1748,47 @@ int orc_bwt_build(const uint8_t *codes, int64_t n, swb_bwt_checkpoint *cp, int64
     return 0;
 }
 
-// findAllSMEMs over a batch of reads (host threads); the output layout of
-// swb_smem_batch: read r's SMEMs at out[r * cap ..+ n_out[r]] (the first cap
-// kept when there are more).  Returns the number of reads with more than cap.
+// BWAMemAligner.internalReseed (BWAMemAligner.swift:259-305, the arena form
+// alignReadPhase1to3 calls): every SMEM of the first pass at least split_len
+// long with at most split_width occurrences is searched again from its
+// midpoint with minIntv = its count + 1; the new SMEMs are appended and the
+// list re-sorted.
+void internal_reseed(const OrcBwt &b, const uint8_t *query, int readLength, int32_t minSeedLen, int32_t splitLen,
+                     int32_t splitWidth, std::vector<swb_smem> &smems) {
+    const size_t originalCount = smems.size();
+    std::vector<swb_smem> added;
+    std::vector<Bidi> prev;
+    for (size_t i = 0; i < originalCount; ++i) {
+        const swb_smem sm = smems[i];
+        const int len = sm.qe - sm.qb;
+        const int64_t cnt = sm.l - sm.k + 1;
+        if (len < splitLen || cnt > (int64_t)splitWidth) continue;
+        const int midpoint = (sm.qb + sm.qe) / 2;
+        find_smems_at(b, query, readLength, midpoint, minSeedLen, cnt + 1, added, prev);
+    }
+    if (added.empty()) return;
+    smems.insert(smems.end(), added.begin(), added.end());
+    std::stable_sort(smems.begin(), smems.end(), [](const swb_smem &x, const swb_smem &y) {
+        if (x.qb != y.qb) return x.qb < y.qb;
+        return (x.qe - x.qb) > (y.qe - y.qb);
+    });
+}
+
+// findAllSMEMs (and, when split_len > 0, internalReseed) over a batch of
+// reads (host threads); the output layout of swb_smem_batch: read r's SMEMs
+// at out[r * cap ..+ n_out[r]] (the first cap kept when there are more).
+// Returns the number of reads with more than cap.
 int64_t orc_smem_batch(const swb_bwt_checkpoint *cp, const int64_t count[5], int64_t length, int64_t sentinel,
                        const uint8_t *bases, const uint64_t *read_off, const int32_t *read_len, size_t n_reads,
-                       int32_t min_seed_len, int64_t min_intv, uint32_t cap, swb_smem *out, uint32_t *n_out,
-                       int n_threads) {
+                       int32_t min_seed_len, int64_t min_intv, int32_t split_len, int32_t split_width, uint32_t cap,
+                       swb_smem *out, uint32_t *n_out, int n_threads) {
     OrcBwt b{cp, {count[0], count[1], count[2], count[3], count[4]}, length, sentinel};
     std::atomic<int64_t> over{0};
     parallel_for(n_reads, n_threads, [&](size_t lo, size_t hi, int) {
         std::vector<swb_smem> v;
         for (size_t r = lo; r < hi; ++r) {
             find_all_smems(b, bases + read_off[r], read_len[r], min_seed_len, min_intv, v);
+            if (split_len > 0) internal_reseed(b, bases + read_off[r], read_len[r], min_seed_len, split_len, split_width, v);
             n_out[r] = (uint32_t)v.size();
             if (v.size() > cap) over += 1;
             std::copy(v.begin(), v.begin() + std::min<size_t>(v.size(), cap), out + r * (size_t)cap);

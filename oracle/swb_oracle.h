@@ -137,8 +137,8 @@ int orc_bwt_build(const uint8_t *codes, int64_t n, swb_bwt_checkpoint *cp, int64
                   int64_t *length_out, int64_t *sentinel_out, int n_threads);
 int64_t orc_smem_batch(const swb_bwt_checkpoint *cp, const int64_t count[5], int64_t length, int64_t sentinel,
                        const uint8_t *bases, const uint64_t *read_off, const int32_t *read_len, size_t n_reads,
-                       int32_t min_seed_len, int64_t min_intv, uint32_t cap, swb_smem *out, uint32_t *n_out,
-                       int n_threads);
+                       int32_t min_seed_len, int64_t min_intv, int32_t split_len, int32_t split_width, uint32_t cap,
+                       swb_smem *out, uint32_t *n_out, int n_threads);
 
 #ifdef __cplusplus
 }

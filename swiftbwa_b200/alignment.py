@@ -307,9 +307,10 @@ class Engine:
                                        int(length), int(sentinel)), "swb_upload_bwt")
 
     def smem_batch(self, bases: np.ndarray, read_off: np.ndarray, read_len: np.ndarray, min_seed_len: int,
-                   min_intv: int = 1, cap_per_read: int = 64):
-        """SMEMFinder.findAllSMEMs per read on the resident FM index ->
-        (SMEM_DTYPE [n_reads * cap_per_read], n_out); read r's SMEMs are
+                   min_intv: int = 1, cap_per_read: int = 64, split_len: int = 0, split_width: int = 10):
+        """SMEMFinder.findAllSMEMs per read on the resident FM index, then (with
+        split_len > 0) BWAMemAligner.internalReseed -> (SMEM_DTYPE
+        [n_reads * cap_per_read], n_out); read r's SMEMs are
         out[r * cap : r * cap + n_out[r]]."""
         bases = np.ascontiguousarray(bases, dtype=np.uint8)
         read_off = np.ascontiguousarray(read_off, dtype=np.uint64)
@@ -318,7 +319,8 @@ class Engine:
         out = np.zeros(max(n * cap_per_read, 1), SMEM_DTYPE)
         n_out = np.zeros(max(n, 1), np.uint32)
         _check(self.lib.swb_smem_batch(self.h, ptr(bases), bases.size, read_off.ctypes.data, read_len.ctypes.data, n,
-                                       int(min_seed_len), int(min_intv), int(cap_per_read), out.ctypes.data,
+                                       int(min_seed_len), int(min_intv), int(split_len), int(split_width),
+                                       int(cap_per_read), out.ctypes.data,
                                        n_out.ctypes.data), "swb_smem_batch")
         return out, n_out[:n]
 

@@ -35,6 +35,7 @@ struct SeedArgs {
     uint32_t n_reads;
     int32_t min_seed_len;
     int64_t min_intv;
+    int32_t split_len, split_width;   // internal re-seeding (split_len <= 0: off)
     uint32_t cap;
     swb_smem *out;
     uint32_t *n_out;
@@ -127,7 +128,7 @@ struct Emit {
 
 // SMEMFinder.findSMEMsAtPosition (SMEMFinder.swift:89-268); returns nextPos.
 __device__ int smems_at(const SeedArgs &g, const uint8_t *__restrict__ q, int readLength, int startPos,
-                        const Prev &prev, Emit &emit, unsigned long long &exts) {
+                        int64_t minIntv, const Prev &prev, Emit &emit, unsigned long long &exts) {
     int nextPos = startPos + 1;
     const int a = q[startPos];
     if (a >= 4) return nextPos;                                              // :104-107
@@ -141,13 +142,13 @@ __device__ int smems_at(const SeedArgs &g, const uint8_t *__restrict__ q, int re
         const Intv ext = backward_ext(g, smem.l, smem.k, smem.s, 3 - base);
         ++exts;
         if (ext.s != smem.s) prev.put(numPrev++, smem);
-        if (ext.s < g.min_intv) {
+        if (ext.s < minIntv) {
             nextPos = j;
             break;
         }
         smem = Cand{ext.l, ext.k, ext.s, smem.m, j};
     }
-    if (smem.s >= g.min_intv) prev.put(numPrev++, smem);                     // :160-163
+    if (smem.s >= minIntv) prev.put(numPrev++, smem);                     // :160-163
     for (int x = 0, y = numPrev - 1; x < y; ++x, --y) {                      // :166 (longest first)
         const Cand cx = prev.get(x), cy = prev.get(y);
         prev.put(x, cy);
@@ -163,11 +164,11 @@ __device__ int smems_at(const SeedArgs &g, const uint8_t *__restrict__ q, int re
             const Cand iv = prev.get(p);
             const Intv ext = backward_ext(g, iv.k, iv.l, iv.s, base);
             ++exts;
-            if (ext.s < g.min_intv && (iv.n - iv.m + 1) >= g.min_seed_len) { // condition 1: emit, stop
+            if (ext.s < minIntv && (iv.n - iv.m + 1) >= g.min_seed_len) { // condition 1: emit, stop
                 emit.add(iv);
                 break;
             }
-            if (ext.s >= g.min_intv && ext.s != currS) {                     // condition 2: keep, stop
+            if (ext.s >= minIntv && ext.s != currS) {                     // condition 2: keep, stop
                 currS = ext.s;
                 prev.put(numCurr++, Cand{ext.k, ext.l, ext.s, bj, iv.n});
                 break;
@@ -177,7 +178,7 @@ __device__ int smems_at(const SeedArgs &g, const uint8_t *__restrict__ q, int re
             const Cand iv = prev.get(p);
             const Intv ext = backward_ext(g, iv.k, iv.l, iv.s, base);
             ++exts;
-            if (ext.s >= g.min_intv && ext.s != currS) {
+            if (ext.s >= minIntv && ext.s != currS) {
                 currS = ext.s;
                 prev.put(numCurr++, Cand{ext.k, ext.l, ext.s, bj, iv.n});
             }
@@ -190,6 +191,20 @@ __device__ int smems_at(const SeedArgs &g, const uint8_t *__restrict__ q, int re
         if ((iv.n - iv.m + 1) >= g.min_seed_len) emit.add(iv);
     }
     return nextPos;
+}
+
+// Sort by query begin, longer first (SMEMFinder.swift:53-58); equal keys
+// are equal SMEMs, so their order cannot differ from the reference's.
+__device__ void sort_smems(swb_smem *w, uint32_t n) {
+    for (uint32_t i = 1; i < n; ++i) {
+        const swb_smem x = w[i];
+        uint32_t j = i;
+        while (j > 0 && (w[j - 1].qb > x.qb || (w[j - 1].qb == x.qb && w[j - 1].qe - w[j - 1].qb < x.qe - x.qb))) {
+            w[j] = w[j - 1];
+            --j;
+        }
+        w[j] = x;
+    }
 }
 
 __global__ void __launch_bounds__(kSeedT) smem_kernel(SeedArgs g) {
@@ -207,23 +222,25 @@ __global__ void __launch_bounds__(kSeedT) smem_kernel(SeedArgs g) {
             const uint8_t *q = g.bases + g.read_off[r];
             const int len = g.read_len[r];
             Emit emit{g.out + (size_t)r * g.cap, g.cap};
-            for (int pos = 0; pos < len;) pos = smems_at(g, q, len, pos, prev, emit, exts);   // :41-51
-            g.n_out[r] = emit.n;
-            if (emit.n > g.cap) {
-                atomicMin(g.first_over, r);
-            } else {
-                // Sort by query begin, longer first (:53-58); equal keys are equal SMEMs.
-                swb_smem *w = emit.w;
-                for (uint32_t i = 1; i < emit.n; ++i) {
-                    const swb_smem x = w[i];
-                    uint32_t j = i;
-                    while (j > 0 && (w[j - 1].qb > x.qb || (w[j - 1].qb == x.qb && w[j - 1].qe - w[j - 1].qb < x.qe - x.qb))) {
-                        w[j] = w[j - 1];
-                        --j;
+            for (int pos = 0; pos < len;) pos = smems_at(g, q, len, pos, g.min_intv, prev, emit, exts);   // :41-51
+            if (emit.n <= g.cap) {
+                sort_smems(emit.w, emit.n);
+                // Internal re-seeding (BWAMemAligner.swift:283-304): the first
+                // pass's SMEMs stay at the front of the window while new ones
+                // are appended behind them.
+                const uint32_t n0 = emit.n;
+                if (g.split_len > 0) {
+                    for (uint32_t i = 0; i < n0; ++i) {   // originals: w[0 .. n0), never overwritten
+                        const swb_smem sm = emit.w[i];
+                        const int64_t cnt = sm.l - sm.k + 1;
+                        if (sm.qe - sm.qb < g.split_len || cnt > (int64_t)g.split_width) continue;
+                        smems_at(g, q, len, (sm.qb + sm.qe) / 2, cnt + 1, prev, emit, exts);
                     }
-                    w[j] = x;
+                    if (emit.n > n0 && emit.n <= g.cap) sort_smems(emit.w, emit.n);
                 }
             }
+            g.n_out[r] = emit.n;
+            if (emit.n > g.cap) atomicMin(g.first_over, r);
         }
     }
     for (int o = 16; o > 0; o >>= 1) exts += __shfl_down_sync(0xFFFFFFFFu, exts, o);
@@ -259,7 +276,7 @@ int swb_upload_bwt(swb_ctx *ctx, const swb_bwt_checkpoint *cp, uint64_t n_cp, co
 
 int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uint64_t *read_off,
                    const int32_t *read_len, size_t n_reads, int32_t min_seed_len, int64_t min_intv,
-                   uint32_t cap_per_read, swb_smem *out, uint32_t *n_out) {
+                   int32_t split_len, int32_t split_width, uint32_t cap_per_read, swb_smem *out, uint32_t *n_out) {
     if (!ctx || (n_reads && (!read_off || !read_len || !n_out || (!out && cap_per_read))) || (!bases && n_bases))
         return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
     if (n_reads > 0xFFFFFFF0ull) return set_error(SWB_ERR_TOO_LARGE, "more than 2^32-16 reads in one batch");
@@ -315,6 +332,8 @@ int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uin
     g.n_reads = (uint32_t)n_reads;
     g.min_seed_len = min_seed_len;
     g.min_intv = min_intv;
+    g.split_len = split_len;
+    g.split_width = split_width;
     g.cap = cap_per_read;
     g.out = d_out;
     g.n_out = d_n;

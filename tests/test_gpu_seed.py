@@ -49,14 +49,17 @@ def _reads(ref, seed, n, L):
     return out.reshape(-1), np.arange(n, dtype=np.uint64) * L, lens
 
 
-@pytest.mark.parametrize("min_intv", [1, 20])
-def test_smems_equal_oracle(engine, oracle_mod, index, min_intv):
+@pytest.mark.parametrize("min_intv,split_len", [(1, 0), (20, 0), (1, 28)])
+def test_smems_equal_oracle(engine, oracle_mod, index, min_intv, split_len):
+    """min_intv 20: the re-seeding pass's threshold; split_len 28: with the
+    internal re-seeding of BWAMemAligner.internalReseed (split width 10)."""
     ref, idx = index
     engine.upload_bwt(idx.cp, idx.count, idx.length, idx.sentinel)
-    bases, off, lens = _reads(ref, 5 + min_intv, 3000, 150)
+    bases, off, lens = _reads(ref, 5 + min_intv + split_len, 3000, 150)
     cap = 128
-    got, gn = engine.smem_batch(bases, off, lens, 19, min_intv=min_intv, cap_per_read=cap)
-    exp, en, over = oracle_mod.smem_batch(idx, bases, off, lens, 19, min_intv=min_intv, cap=cap, n_threads=8)
+    got, gn = engine.smem_batch(bases, off, lens, 19, min_intv=min_intv, cap_per_read=cap, split_len=split_len)
+    exp, en, over = oracle_mod.smem_batch(idx, bases, off, lens, 19, min_intv=min_intv, cap=cap, n_threads=8,
+                                          split_len=split_len, split_width=10)
     assert over == 0 and np.array_equal(gn, en) and en.sum() > 0
     for r in range(len(lens)):
         assert np.array_equal(got[r * cap: r * cap + gn[r]], exp[r * cap: r * cap + en[r]]), f"read {r}"

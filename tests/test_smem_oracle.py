@@ -153,3 +153,41 @@ def test_workload_index_builder_matches_oracle_builder(n, tandem):
     b = W.fm_index(ref, device="cpu")
     assert np.array_equal(a.cp, b.cp) and np.array_equal(a.count, b.count)
     assert (a.length, a.sentinel) == (b.length, b.sentinel)
+
+
+def test_internal_reseed_adds_exact_more_specific_seeds():
+    """BWAMemAligner.internalReseed (the arena form, BWAMemAligner.swift:259-305):
+    the first pass's SMEMs are kept, and every added one is an exact match of
+    at least minSeedLen found from the midpoint of a first-pass SMEM at least
+    split_len long with at most split_width occurrences, with more occurrences
+    than that SMEM; the list stays sorted by begin, longer first."""
+    assert oracle.split_len_of(19, 1.5) == 28
+    ref = _ref(7, 6000)
+    ref[3000:3200] = ref[500:700]                    # extra copies make lower-count sub-seeds
+    ref[4000:4100] = ref[520:620]
+    idx = oracle.bwt_build(ref)
+    tb = _text(ref).tobytes()
+    reads = _reads(ref, 8, 80, 100)
+    bases = np.concatenate(reads)
+    off = np.arange(len(reads), dtype=np.uint64) * 100
+    ln = np.full(len(reads), 100, np.int32)
+    base, nb, _ = oracle.smem_batch(idx, bases, off, ln, 19, cap=512)
+    rs, nr, over = oracle.smem_batch(idx, bases, off, ln, 19, cap=512, split_len=28, split_width=10)
+    assert over == 0 and np.all(nr >= nb) and nr.sum() > nb.sum()
+    for r, q in enumerate(reads):
+        a = base[r * 512: r * 512 + nb[r]]
+        b = rs[r * 512: r * 512 + nr[r]]
+        keys = list(zip(b["qb"].tolist(), (-(b["qe"] - b["qb"])).tolist()))
+        assert keys == sorted(keys)
+        first = {tuple(x) for x in a.tolist()}
+        assert first <= {tuple(x) for x in b.tolist()}
+        parents = [s for s in a if s["qe"] - s["qb"] >= 28 and s["l"] - s["k"] + 1 <= 10]
+        for s in b:
+            if tuple(s.tolist()) in first:
+                continue
+            qb, qe = int(s["qb"]), int(s["qe"])
+            occ = _count(tb, q[qb:qe].tobytes())
+            assert qe - qb >= 19 and occ == int(s["l"] - s["k"] + 1)
+            assert any(p["qb"] <= (int(p["qb"]) + int(p["qe"])) // 2 < p["qe"] and
+                       (int(p["qb"]) + int(p["qe"])) // 2 in range(qb, qe) and occ > int(p["l"] - p["k"] + 1)
+                       for p in parents)
