@@ -379,6 +379,27 @@ struct ZRow {
     }
 };
 
+// One lockstep step at column c (both lanes): row i at c, row i+1 at c-1.
+// Returns the two backpointer codes; stores row i+1's word c.
+struct NwLane2 {
+    uint32_t h, hp2, e, f, wdp, selp;
+};
+__device__ __forceinline__ void nw_both(const NwPairConsts &k, const RowTable &rt0, const RowTable &rt1,
+                                        uint32_t *__restrict__ he, const uint8_t *__restrict__ qs, int T, int c,
+                                        NwLane2 &st, uint32_t &code0, uint32_t &code1) {
+    const uint32_t wd = he[(c + 1) * T];                          // [H(i-1,c) | E(i-1,c)]
+    const uint32_t sel = nw_sel(qs[c * T]);
+    const uint32_t DG = __byte_perm(st.wdp, st.hp2, 0x5410);      // [H(i-1,c-1), H(i,c-2)]
+    const uint32_t UH = __byte_perm(wd, st.h, 0x5410);            // [H(i-1,c),   H(i,c-1)]
+    const uint32_t UE = __byte_perm(wd, st.e, 0x5432);            // [E(i-1,c),   E(i,c-1)]
+    const uint32_t S = prmt(rt1.lo, rt1.hi, st.selp) * 65536u + prmt(rt0.lo, rt0.hi, sel);
+    st.hp2 = st.h;
+    nw_pair_step(k, DG, UH, UE, S, st.h, st.e, st.f, code0, code1);
+    he[c * T] = __byte_perm(st.h, st.e, 0x7632);                  // row i+1's word c: H, E of column c-1
+    st.wdp = wd;
+    st.selp = sel;
+}
+
 __device__ int global_dp_pair16(const DevScoring &sc, uint32_t *__restrict__ he, const uint8_t *__restrict__ qs,
                                 int T, const GlobalArgs &a, const swb_global_task &tk, int w, const ZPacked &zp,
                                 unsigned long long &cells) {
@@ -395,6 +416,7 @@ __device__ int global_dp_pair16(const DevScoring &sc, uint32_t *__restrict__ he,
         he[j * T] = ((uint32_t)hv & 0xFFFFu) | negHi;
     }
     const size_t rstride = (size_t)zp.ncw * zp.nslots;
+    const size_t ns = zp.nslots;
     for (int i = 0; i < tlen; i += 2) {                                          // :89-142, two rows at a time
         const bool pair = i + 1 < tlen;
         const int beg0 = imax(0, i - w), end0 = imin(qlen, i + w + 1);
@@ -404,49 +426,70 @@ __device__ int global_dp_pair16(const DevScoring &sc, uint32_t *__restrict__ he,
         const int hBeg0 = beg0 == 0 ? 0 - (oeDel + eDel * i) : kNeg;
         const int hBeg1 = beg1 == 0 ? 0 - (oeDel + eDel * (i + 1)) : kNeg;
         cells += (unsigned long long)(end0 - beg0) + (unsigned long long)(end1 - beg1);
-        ZRow z0{zp.z + (size_t)i * rstride, zp.nslots}, z1{zp.z + (size_t)(i + 1) * rstride, zp.nslots};
+        uint32_t *z0w = zp.z + (size_t)i * rstride, *z1w = z0w + rstride;
+        ZRow z0{z0w, ns}, z1{z1w, ns};
         // Lane 0 state: H of row i at column beg0-1 is hBeg0 (the reference's h[beg0]); F starts at -inf.
-        uint32_t h = (uint32_t)hBeg0 & 0xFFFFu, hp2 = h, e = 0u, f = (uint32_t)(uint16_t)kNeg;
-        uint32_t wdp = he[beg0 * T];                 // word beg0: its H is row i's first diagonal
-        uint32_t selp = 0u;                          // query selector of the previous column
-        bool started = false;                        // lane 1 running
-        int c = beg0;
-        // Lane 1 begins at column beg1 (step beg1 + 1): H at beg1-1 is hBeg1,
-        // F is -inf, and the reference's h[beg1] = hBeg1 is stored.
-        auto start1 = [&]() {
-            h = (h & 0xFFFFu) | ((uint32_t)hBeg1 << 16);
-            f = (f & 0xFFFFu) | negHi;
-            reinterpret_cast<int16_t *>(he + beg1 * T)[0] = (int16_t)hBeg1;
-            started = true;
-        };
-        for (; c < end0; ++c) {
-            const uint32_t wd = he[(c + 1) * T];     // [H(i-1,c) | E(i-1,c)]
-            const uint32_t sel = nw_sel(qs[c * T]);
-            const bool two = pair && c >= beg1 + 1;
-            if (two && !started) start1();
-            const uint32_t DG = __byte_perm(wdp, hp2, 0x5410);    // [H(i-1,c-1), H(i,c-2)]
-            const uint32_t UH = __byte_perm(wd, h, 0x5410);       // [H(i-1,c),   H(i,c-1)]
-            const uint32_t UE = __byte_perm(wd, e, 0x5432);       // [E(i-1,c),   E(i,c-1)]
-            const uint32_t S = prmt(rt1.lo, rt1.hi, selp) * 65536u + prmt(rt0.lo, rt0.hi, sel);
-            hp2 = h;
-            uint32_t code0, code1;
-            nw_pair_step(k, DG, UH, UE, S, h, e, f, code0, code1);
-            z0.put(c, code0, end0 - 1);
-            if (two) {
-                he[c * T] = __byte_perm(h, e, 0x7632);             // row i+1's word c: H, E of column c-1
-                z1.put(c - 1, code1, end1 - 1);
-            } else if (!pair) {
-                he[(c + 1) * T] = __byte_perm(h, e, 0x5410);       // last row alone: its own words
+        NwLane2 st{(uint32_t)hBeg0 & 0xFFFFu, (uint32_t)hBeg0 & 0xFFFFu, 0u, (uint32_t)(uint16_t)kNeg,
+                   he[beg0 * T], 0u};
+        uint32_t code0, code1;
+        if (!pair) {                                   // the last row alone: it stores its own words
+            for (int c = beg0; c < end0; ++c) {
+                const uint32_t wd = he[(c + 1) * T];
+                const uint32_t sel = nw_sel(qs[c * T]);
+                const uint32_t DG = __byte_perm(st.wdp, st.hp2, 0x5410);
+                const uint32_t UH = __byte_perm(wd, st.h, 0x5410);
+                const uint32_t UE = __byte_perm(wd, st.e, 0x5432);
+                st.hp2 = st.h;
+                nw_pair_step(k, DG, UH, UE, prmt(rt0.lo, rt0.hi, sel), st.h, st.e, st.f, code0, code1);
+                he[(c + 1) * T] = __byte_perm(st.h, st.e, 0x5410);
+                z0.put(c, code0, end0 - 1);
+                st.wdp = wd;
             }
-            wdp = wd;
-            selp = sel;
+            continue;
         }
-        if (!pair) continue;
+        // Row i alone up to column beg1 (lane 1 starts at column beg1, step beg1 + 1).
+        int c = beg0;
+        const int aEnd = imin(beg1, end0 - 1);
+        for (; c <= aEnd; ++c) {
+            nw_both(k, rt0, rt1, he, qs, T, c, st, code0, code1);
+            z0.put(c, code0, end0 - 1);
+        }
+        // Lane 1: H at beg1-1 is hBeg1, F is -inf; the reference's h[beg1] = hBeg1.
+        st.h = (st.h & 0xFFFFu) | ((uint32_t)hBeg1 << 16);
+        st.f = (st.f & 0xFFFFu) | negHi;
+        reinterpret_cast<int16_t *>(he + beg1 * T)[0] = (int16_t)hBeg1;
+        // Both rows, columns c .. end0-1 (row i+1 at c-1): first up to a multiple of 8.
+        for (; c < end0 && (c & 7); ++c) {
+            nw_both(k, rt0, rt1, he, qs, T, c, st, code0, code1);
+            z0.put(c, code0, end0 - 1);
+            z1.put(c - 1, code1, end1 - 1);
+        }
+        // Blocks of 8 aligned columns: row i fills word c/8 (nibbles 0..7), row i+1
+        // completes word c/8 - 1 (nibble 7, column c-1) then fills nibbles 0..6 of word c/8.
+        for (; c + 8 <= end0; c += 8) {
+            uint32_t w0 = 0, w1;
+            nw_both(k, rt0, rt1, he, qs, T, c, st, code0, code1);
+            w0 |= code0;
+            z1w[(size_t)((c >> 3) - 1) * ns] = z1.acc | (code1 << 28);
+            w1 = 0;
+#pragma unroll
+            for (int s2 = 1; s2 < 8; ++s2) {
+                nw_both(k, rt0, rt1, he, qs, T, c + s2, st, code0, code1);
+                w0 |= code0 << (4 * s2);
+                w1 |= code1 << (4 * (s2 - 1));
+            }
+            z0w[(size_t)(c >> 3) * ns] = w0;
+            z1.acc = w1;
+        }
+        for (; c < end0; ++c) {
+            nw_both(k, rt0, rt1, he, qs, T, c, st, code0, code1);
+            z0.put(c, code0, end0 - 1);
+            z1.put(c - 1, code1, end1 - 1);
+        }
         // Row i+1 alone for its columns past row i's band (c = end0 .. end1).
         // Row i's H at end0-1 (or hBeg0) is its diagonal at column end0.
-        uint32_t hLast0 = h & 0xFFFFu, eLast0 = e & 0xFFFFu, hLast0p = hp2 & 0xFFFFu;
+        const uint32_t hLast0 = st.h & 0xFFFFu, eLast0 = st.e & 0xFFFFu, hLast0p = st.hp2 & 0xFFFFu;
         for (c = imax(end0, beg1 + 1); c <= end1; ++c) {
-            if (!started) start1();
             const uint32_t sel = nw_sel(qs[(c - 1) * T]);
             uint32_t DG, UH, UE;
             if (c - 1 < end0) {             // column end0-1: row i's values from registers
@@ -459,10 +502,8 @@ __device__ int global_dp_pair16(const DevScoring &sc, uint32_t *__restrict__ he,
                 UH = wd << 16;
                 UE = wd & 0xFFFF0000u;
             }
-            const uint32_t S = prmt(rt1.lo, rt1.hi, sel) * 65536u;
-            uint32_t code0, code1;
-            nw_pair_step(k, DG, UH, UE, S, h, e, f, code0, code1);
-            he[c * T] = __byte_perm(h, e, 0x7632);
+            nw_pair_step(k, DG, UH, UE, prmt(rt1.lo, rt1.hi, sel) * 65536u, st.h, st.e, st.f, code0, code1);
+            he[c * T] = __byte_perm(st.h, st.e, 0x7632);
             z1.put(c - 1, code1, end1 - 1);
         }
     }
