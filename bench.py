@@ -422,7 +422,7 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
         times = []
         for _ in range(3):
             t0 = time.perf_counter()
-            sm6, n6 = eng.smem_batch(wl6.bases, off6, len6, 19, cap_per_read=cap6, split_len=split6)
+            sm6, n6, o6 = eng.smem_batch(wl6.bases, off6, len6, 19, cap_per_read=cap6, split_len=split6)
             times.append(time.perf_counter() - t0)
         e2e6 = float(np.median(times))
         ms6, exts6 = eng.last_batch_stats()
@@ -448,7 +448,7 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
                                             f"{dt6:.1f} s"}
             same6 = bool(np.array_equal(n6[:s6], en6))
             for r in range(s6):
-                if not np.array_equal(sm6[r * cap6: r * cap6 + n6[r]], e6[r * cap6: r * cap6 + en6[r]]):
+                if not np.array_equal(sm6[o6[r]: o6[r] + n6[r]], e6[r * cap6: r * cap6 + en6[r]]):
                     same6 = False
                     break
             c6["bitexact_sample"] = f"{s6} reads: {'all equal' if same6 else 'DIFFERENT'}"

@@ -433,17 +433,23 @@ int swb_upload_bwt(swb_ctx *ctx, const swb_bwt_checkpoint *cp, uint64_t n_cp, co
  * SMEMs join the list (split_len = Int(Float(minSeedLength) * seedSplitRatio
  * + 0.499) as the reference computes it, 28 for the defaults; split_width =
  * splitWidth, 10).  Read r is bases[read_off[r] ..+ read_len[r])
- * (codes 0-4, N = 4).  Its SMEMs, sorted by query begin then longest first,
- * go to out[r * cap_per_read ..+ n_out[r]].  When a read has more than
- * cap_per_read SMEMs, n_out[r] still counts them all, its window holds the
- * first cap_per_read in the order found, and the call returns
- * SWB_ERR_TOO_LARGE naming the first such read, so the caller can retry
- * with a larger window (every other read's results are complete).  Replaces
+ * (codes 0-4, N = 4).  Its n_out[r] SMEMs, sorted by query begin then
+ * longest first, are out[out_off[r] ..+ n_out[r]] (out_off = the running
+ * sum of n_out, so the reads' lists are packed in read order); out holds
+ * out_cap entries.  cap_per_read bounds the SMEMs of one read the device
+ * keeps while it searches.  When a read has more than cap_per_read SMEMs,
+ * n_out[r] still counts them all, only the first cap_per_read found (in
+ * the order found) are written at its offset, and the call returns
+ * SWB_ERR_TOO_LARGE naming the first such read; when the total exceeds
+ * out_cap the call returns SWB_ERR_TOO_LARGE with n_out and out_off filled
+ * and nothing written to out.  Either way the caller can retry with larger
+ * bounds, and every other read's results are complete.  Replaces
  * the CPU loop of BWAMemAligner.alignReadPhase1to3 (BWAMemAligner.swift:133-139)
  * and the Metal forward kernel (Kernels/smem_forward.metal:117) for a batch. */
 int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uint64_t *read_off,
                    const int32_t *read_len, size_t n_reads, int32_t min_seed_len, int64_t min_intv,
-                   int32_t split_len, int32_t split_width, uint32_t cap_per_read, swb_smem *out, uint32_t *n_out);
+                   int32_t split_len, int32_t split_width, uint32_t cap_per_read, swb_smem *out, size_t out_cap,
+                   uint32_t *n_out, uint64_t *out_off);
 
 /* ------------------------------------------------ serving (continuous batching) */
 /* A request loop over one context's GPU for extension batches of differing

@@ -209,7 +209,7 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.swb_upload_bwt.argtypes = [vp, vp, C.c_uint64, P(C.c_int64), C.c_int64, C.c_int64]
     lib.swb_upload_bwt.restype = C.c_int
     lib.swb_smem_batch.argtypes = [vp, vp, C.c_size_t, vp, vp, C.c_size_t, C.c_int32, C.c_int64, C.c_int32,
-                                   C.c_int32, C.c_uint32, vp, vp]
+                                   C.c_int32, C.c_uint32, vp, C.c_size_t, vp, vp]
     lib.swb_smem_batch.restype = C.c_int
     lib.swb_banded_sw_align.argtypes = [vp, u8p, C.c_int32, u8p, C.c_int32, P(Scoring),
                                         C.c_int32, C.c_int32, C.c_int32, P(ExtResult)]

@@ -307,22 +307,32 @@ class Engine:
                                        int(length), int(sentinel)), "swb_upload_bwt")
 
     def smem_batch(self, bases: np.ndarray, read_off: np.ndarray, read_len: np.ndarray, min_seed_len: int,
-                   min_intv: int = 1, cap_per_read: int = 64, split_len: int = 0, split_width: int = 10):
+                   min_intv: int = 1, cap_per_read: int = 64, split_len: int = 0, split_width: int = 10,
+                   out_cap: Optional[int] = None):
         """SMEMFinder.findAllSMEMs per read on the resident FM index, then (with
-        split_len > 0) BWAMemAligner.internalReseed -> (SMEM_DTYPE
-        [n_reads * cap_per_read], n_out); read r's SMEMs are
-        out[r * cap : r * cap + n_out[r]]."""
+        split_len > 0) BWAMemAligner.internalReseed -> (SMEM_DTYPE packed
+        SMEMs, n_out, out_off); read r's SMEMs are out[out_off[r] : out_off[r] + n_out[r]]."""
         bases = np.ascontiguousarray(bases, dtype=np.uint8)
         read_off = np.ascontiguousarray(read_off, dtype=np.uint64)
         read_len = np.ascontiguousarray(read_len, dtype=np.int32)
         n = read_off.size
-        out = np.zeros(max(n * cap_per_read, 1), SMEM_DTYPE)
+        grow = out_cap is None
+        if grow:
+            out_cap = int(read_len.astype(np.int64).clip(0).sum()) + 16   # usually enough; grown below if not
         n_out = np.zeros(max(n, 1), np.uint32)
-        _check(self.lib.swb_smem_batch(self.h, ptr(bases), bases.size, read_off.ctypes.data, read_len.ctypes.data, n,
-                                       int(min_seed_len), int(min_intv), int(split_len), int(split_width),
-                                       int(cap_per_read), out.ctypes.data,
-                                       n_out.ctypes.data), "swb_smem_batch")
-        return out, n_out[:n]
+        out_off = np.zeros(max(n, 1), np.uint64)
+        while True:
+            out = np.zeros(max(out_cap, 1), SMEM_DTYPE)
+            rc = self.lib.swb_smem_batch(self.h, ptr(bases), bases.size, read_off.ctypes.data, read_len.ctypes.data,
+                                         n, int(min_seed_len), int(min_intv), int(split_len), int(split_width),
+                                         int(cap_per_read), out.ctypes.data, int(out_cap), n_out.ctypes.data,
+                                         out_off.ctypes.data)
+            total = int(out_off[n - 1]) + int(n_out[n - 1]) if n else 0
+            if grow and rc == abi.SWB_ERR_TOO_LARGE and total > out_cap:
+                out_cap = total
+                continue
+            _check(rc, "swb_smem_batch")
+            return out, n_out[:n], out_off[:n]
 
     def ext_batch_plain_device(self, sc: Scoring, d_bases: int, d_tasks: int, n: int, d_out: int, stream: int = 0):
         """swb_ext_batch_plain_device: the plain one-launch-per-batch kernel (the

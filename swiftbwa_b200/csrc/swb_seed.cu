@@ -14,8 +14,12 @@
 // intervals (at most one per query base) lives in a column of global
 // scratch laid out [entry][thread], so a warp's threads touch adjacent
 // words when they are at the same entry.  A read's SMEMs go to its own
-// output window in the order found and are then sorted there (query begin,
-// longer first), as the reference sorts its array.
+// window in the order found and are then sorted there (query begin, longer
+// first), as the reference sorts its array; a scan of the counts and a
+// gather pack the windows in read order, and only those entries are copied
+// back to the host.
+#include <cub/device/device_scan.cuh>
+
 #include <algorithm>
 
 #include "swb_internal.h"
@@ -247,6 +251,24 @@ __global__ void __launch_bounds__(kSeedT) smem_kernel(SeedArgs g) {
     if (lane == 0 && exts) atomicAdd(g.exts, exts);
 }
 
+// Packs every read's window into the output in read order: read r's first
+// min(n[r], cap) SMEMs go to off[r] (off = exclusive sum of n).
+__global__ void smem_pack_kernel(const swb_smem *__restrict__ win, const uint32_t *__restrict__ n,
+                                 const unsigned long long *__restrict__ off, uint32_t n_reads, uint32_t cap,
+                                 swb_smem *__restrict__ out) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_reads) return;
+    const uint32_t k = min(n[r], cap);
+    const swb_smem *src = win + (size_t)r * cap;
+    swb_smem *dst = out + off[r];
+    for (uint32_t i = 0; i < k; ++i) dst[i] = src[i];
+}
+
+__global__ void u32_to_u64_kernel(const uint32_t *__restrict__ a, unsigned long long *__restrict__ b, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i];
+}
+
 }  // namespace
 }  // namespace swb
 
@@ -276,8 +298,10 @@ int swb_upload_bwt(swb_ctx *ctx, const swb_bwt_checkpoint *cp, uint64_t n_cp, co
 
 int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uint64_t *read_off,
                    const int32_t *read_len, size_t n_reads, int32_t min_seed_len, int64_t min_intv,
-                   int32_t split_len, int32_t split_width, uint32_t cap_per_read, swb_smem *out, uint32_t *n_out) {
-    if (!ctx || (n_reads && (!read_off || !read_len || !n_out || (!out && cap_per_read))) || (!bases && n_bases))
+                   int32_t split_len, int32_t split_width, uint32_t cap_per_read, swb_smem *out, size_t out_cap,
+                   uint32_t *n_out, uint64_t *out_off) {
+    if (!ctx || (n_reads && (!read_off || !read_len || !n_out || !out_off)) || (!out && out_cap) ||
+        (!bases && n_bases))
         return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
     if (n_reads > 0xFFFFFFF0ull) return set_error(SWB_ERR_TOO_LARGE, "more than 2^32-16 reads in one batch");
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -298,9 +322,13 @@ int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uin
     auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
     const size_t b_bytes = al(n_bases), o_bytes = al(n_reads * 8), l_bytes = al(n_reads * 4);
     const size_t out_bytes = al(n_reads * (size_t)cap_per_read * sizeof(swb_smem)), n_bytes = al(n_reads * 4);
+    const size_t off_bytes = al(n_reads * 8);
+    size_t scan_bytes = 0;
+    SWB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (unsigned long long *)nullptr,
+                                           (unsigned long long *)nullptr, (int)n_reads, ctx->stream));
     int rc;
     if ((rc = ensure_dev(ctx, ctx->d_bases, b_bytes + o_bytes + l_bytes + 256)) ||
-        (rc = ensure_dev(ctx, ctx->d_out, out_bytes + n_bytes + 256)))
+        (rc = ensure_dev(ctx, ctx->d_out, out_bytes + n_bytes + 2 * off_bytes + al(scan_bytes) + 256)))
         return rc;
     char *in = (char *)ctx->d_bases.p;
     uint8_t *d_b = (uint8_t *)in;
@@ -309,6 +337,9 @@ int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uin
     uint32_t *d_misc = (uint32_t *)(in + b_bytes + o_bytes + l_bytes);   // claim, first_over
     swb_smem *d_out = (swb_smem *)ctx->d_out.p;
     uint32_t *d_n = (uint32_t *)((char *)ctx->d_out.p + out_bytes);
+    unsigned long long *d_n64 = (unsigned long long *)((char *)ctx->d_out.p + out_bytes + n_bytes);
+    unsigned long long *d_off64 = d_n64 + off_bytes / 8;
+    void *d_scan_tmp = (char *)ctx->d_out.p + out_bytes + n_bytes + 2 * off_bytes;
     // Persistent grid: resident blocks on every SM, each thread with a
     // candidate column of max_len entries (32 bytes each).
     int per_sm = 0;
@@ -359,12 +390,31 @@ int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uin
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
     SWB_CUDA(cudaEventRecord(ctx->ev_stop, st));
+    // Offsets: the running sum of every read's full count.
+    const unsigned cb = 256, cg = (unsigned)((n_reads + cb - 1) / cb);
+    u32_to_u64_kernel<<<cg, cb, 0, st>>>(d_n, d_n64, (uint32_t)n_reads);
+    ctx->launches++;
+    SWB_CUDA(cudaGetLastError());
+    SWB_CUDA(cub::DeviceScan::ExclusiveSum(d_scan_tmp, scan_bytes, d_n64, d_off64, (int)n_reads, st));
     uint32_t first_over = 0;
     SWB_CUDA(cudaMemcpyAsync(n_out, d_n, n_reads * 4, cudaMemcpyDeviceToHost, st));
-    if (cap_per_read)
-        SWB_CUDA(cudaMemcpyAsync(out, d_out, n_reads * (size_t)cap_per_read * sizeof(swb_smem), cudaMemcpyDeviceToHost, st));
+    SWB_CUDA(cudaMemcpyAsync(out_off, d_off64, n_reads * 8, cudaMemcpyDeviceToHost, st));
     SWB_CUDA(cudaMemcpyAsync(&first_over, d_misc + 1, 4, cudaMemcpyDeviceToHost, st));
     SWB_CUDA(cudaStreamSynchronize(st));
+    const uint64_t total = out_off[n_reads - 1] + n_out[n_reads - 1];
+    if (total > out_cap)
+        return set_error(SWB_ERR_TOO_LARGE, std::to_string(total) + " SMEMs, more than out_cap (" +
+                                                std::to_string(out_cap) + ")");
+    if (total) {
+        // Pack the windows in read order, then copy just those entries back.
+        if ((rc = ensure_dev(ctx, ctx->d_aux, total * sizeof(swb_smem)))) return rc;
+        swb_smem *d_pack = (swb_smem *)ctx->d_aux.p;
+        smem_pack_kernel<<<cg, cb, 0, st>>>(d_out, d_n, d_off64, (uint32_t)n_reads, cap_per_read, d_pack);
+        ctx->launches++;
+        SWB_CUDA(cudaGetLastError());
+        SWB_CUDA(cudaMemcpyAsync(out, d_pack, total * sizeof(swb_smem), cudaMemcpyDeviceToHost, st));
+        SWB_CUDA(cudaStreamSynchronize(st));
+    }
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) ctx->last_ms = ms;
     unsigned long long exts = 0;

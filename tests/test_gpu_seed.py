@@ -57,12 +57,14 @@ def test_smems_equal_oracle(engine, oracle_mod, index, min_intv, split_len):
     engine.upload_bwt(idx.cp, idx.count, idx.length, idx.sentinel)
     bases, off, lens = _reads(ref, 5 + min_intv + split_len, 3000, 150)
     cap = 128
-    got, gn = engine.smem_batch(bases, off, lens, 19, min_intv=min_intv, cap_per_read=cap, split_len=split_len)
+    got, gn, goff = engine.smem_batch(bases, off, lens, 19, min_intv=min_intv, cap_per_read=cap,
+                                      split_len=split_len)
     exp, en, over = oracle_mod.smem_batch(idx, bases, off, lens, 19, min_intv=min_intv, cap=cap, n_threads=8,
                                           split_len=split_len, split_width=10)
     assert over == 0 and np.array_equal(gn, en) and en.sum() > 0
+    assert np.array_equal(goff, np.concatenate([[0], np.cumsum(en.astype(np.uint64))[:-1]]))
     for r in range(len(lens)):
-        assert np.array_equal(got[r * cap: r * cap + gn[r]], exp[r * cap: r * cap + en[r]]), f"read {r}"
+        assert np.array_equal(got[goff[r]: goff[r] + gn[r]], exp[r * cap: r * cap + en[r]]), f"read {r}"
 
 
 def test_small_window_reports_counts(engine, oracle_mod, index):
@@ -77,8 +79,11 @@ def test_small_window_reports_counts(engine, oracle_mod, index):
     assert ei.value.status == abi.SWB_ERR_TOO_LARGE
     first = int(np.nonzero(en > 1)[0][0])
     assert f"read {first}:".encode() in engine.lib.swb_last_error_message()
-    got, gn = engine.smem_batch(bases, off, lens, 15, cap_per_read=256)   # usable afterwards
+    got, gn, _ = engine.smem_batch(bases, off, lens, 15, cap_per_read=256)   # usable afterwards
     assert np.array_equal(gn, en)
+    with pytest.raises(SWBError) as ei:                          # output array too small
+        engine.smem_batch(bases, off, lens, 15, cap_per_read=256, out_cap=int(en.sum()) - 1)
+    assert ei.value.status == abi.SWB_ERR_TOO_LARGE and b"out_cap" in engine.lib.swb_last_error_message()
 
 
 def test_empty_and_invalid_inputs(engine, index):
@@ -92,11 +97,11 @@ def test_empty_and_invalid_inputs(engine, index):
     finally:
         fresh.close()
     engine.upload_bwt(idx.cp, idx.count, idx.length, idx.sentinel)
-    out, n = engine.smem_batch(np.zeros(1, np.uint8), np.zeros(0, np.uint64), np.zeros(0, np.int32), 19)
-    assert n.size == 0
+    out, n, o = engine.smem_batch(np.zeros(1, np.uint8), np.zeros(0, np.uint64), np.zeros(0, np.int32), 19)
+    assert n.size == 0 and o.size == 0
     with pytest.raises(SWBError) as ei:                          # span beyond the bases buffer
         engine.smem_batch(np.zeros(10, np.uint8), np.array([5]), np.array([10]), 19)
     assert ei.value.status == abi.SWB_ERR_INVALID_ARG
     bases, off, lens = _reads(ref, 13, 50, 100)
-    got, gn = engine.smem_batch(bases, off, lens, 19)
+    got, gn, _ = engine.smem_batch(bases, off, lens, 19)
     assert gn.sum() > 0
