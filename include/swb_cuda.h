@@ -256,17 +256,19 @@ int swb_ext_batch_plain_device(swb_ctx *ctx, const swb_scoring *sc,
                                const uint8_t *d_bases, const swb_ext_task *d_tasks,
                                size_t n_tasks, swb_ext_result *d_out, void *stream);
 
-/* Length classes of the extension bins: ascending query-length bounds
- * (1..15 values within [8, 256]); each class has an int8-row and an
- * int16-row bin (two target rows per pass, one task per thread), and
- * queries above the last bound, or with scores beyond int16, run one warp
- * per extension.  Defaults: 32 48 64 80 96 112 128 160 192 256.  No
- * reference counterpart: the reference dispatches every batch to one
+/* Length classes of the extension bins: ascending bounds on the row length
+ * a task keeps, min(qlen, 2w + 2) with w the band after the reference's
+ * clamp (BandedSWScalar.swift:52-62) -- a band narrower than the query is
+ * kept as a ring of its columns -- as 1..15 values within [8, 256]; each
+ * class has an int8-row and an int16-row bin (two target rows per pass, one
+ * task per thread), and rows above the last bound, or scores beyond int16,
+ * run one warp per extension.  Defaults: 32 48 64 80 96 112 128 160 192 256.
+ * No reference counterpart: the reference dispatches every batch to one
  * kernel (BandedSWDispatcher.swift:48,107). */
 int swb_set_ext_bins(swb_ctx *ctx, const int32_t *qmax, int n);
 int swb_get_ext_bins(swb_ctx *ctx, int32_t *qmax, int cap, int *n);
 /* Autotuner: times candidate class sets (the defaults, uniform steps, and
- * quantiles of the batch's query lengths and estimated cells) on the given
+ * quantiles of the batch's row lengths and estimated cells) on the given
  * sample batch (host arrays, as swb_ext_batch; best of two runs after a
  * warm-up each) and keeps the fastest in the context, the defaults unless
  * another set is more than 2 % faster.  Writes the chosen classes

@@ -2,12 +2,14 @@
 // BandedSWScalar.align (Sources/Alignment/BandedSWScalar.swift:21-191).
 //
 // Layout and schedule
-//   * Tasks are binned on the device by row width and query-length class:
+//   * Tasks are binned on the device by row width and row-length class:
 //     int8 rows when the score bound h0 + qlen*maxScore is at most 255,
 //     int16 rows when it is at most 32000, each in the context's length
 //     classes (ExtBins: up to 15 bounds, defaults 32..256, chosen by
-//     swb_tune_ext_bins); everything else (queries above the last bound,
-//     larger scores, gap costs beyond a 16-bit lane) goes to the int32 bin.
+//     swb_tune_ext_bins) of the columns the task keeps, min(qlen, 2w + 2)
+//     (ext_row_len: a band narrower than the query is kept as a ring);
+//     everything else (rows above the last bound, larger scores, gap costs
+//     beyond a 16-bit lane) goes to the int32 bin.
 //     The bounds are static, so no row ever saturates and nothing is re-run.
 //     A CUB radix sort orders the tasks by (bin, longest query, longest
 //     target).
@@ -22,7 +24,8 @@
 //     in shared memory, [column][thread]: a 16-bit (int8 scores) or 32-bit
 //     (int16) H|E word and a query byte per column.  A class bound sizes only
 //     these rows; bounds that are multiples of 16 get a kernel instance with
-//     the bound as a constant.
+//     the bound as a constant.  A warp whose tasks all keep their whole query
+//     runs the plain row code, else the ring form.
 //   * The int32 bin runs one warp per extension for queries up to 4096
 //     (swb_ext_warp.cuh) and one thread per extension over int32 rows in
 //     global scratch above that (swb_ext_dp.cuh).
@@ -60,28 +63,35 @@ __device__ __forceinline__ bool fits8(int qlen, int h0, int max_mat) {
     return h0 >= 0 && (long long)h0 + (long long)qlen * (max_mat > 0 ? max_mat : 0) <= 255;
 }
 
+// Columns the two-row code keeps for a task (less one), see ext_row_len.
+__device__ __host__ __forceinline__ int task_row_len(const swb_ext_task &t, const DevScoring &sc) {
+    return ext_row_len(t.qlen, ext_band_w(t.qlen, t.w, t.end_bonus, sc));
+}
+
 // pair_ok: the gap costs fit a 16-bit lane (the two-row kernels of both row
-// widths); otherwise every task takes the int32 bin.
-__device__ __forceinline__ int ext_bin(const swb_ext_task &t, int max_mat, bool pair_ok, uint32_t warp_cells,
+// widths); otherwise every task takes the int32 bin.  Columns run in 16-bit
+// lanes, so queries above kMaxLen take it too (and are refused there).
+__device__ __forceinline__ int ext_bin(const swb_ext_task &t, const DevScoring &sc, bool pair_ok, uint32_t warp_cells,
                                        const ExtBins &bins) {
     if (t.qlen <= 0 || t.tlen <= 0) return 0;
     const int big = 2 * bins.n;
-    if (!pair_ok || t.qlen > bins.q[bins.n - 1] || !fits16(t.qlen, t.h0, max_mat)) return big;
+    const int len = task_row_len(t, sc);
+    if (!pair_ok || len > bins.q[bins.n - 1] || t.qlen > kMaxLen || !fits16(t.qlen, t.h0, sc.max_mat)) return big;
     if (warp_cells && (unsigned long long)t.qlen * (unsigned long long)t.tlen > warp_cells) return big;
     int b = 0;
-    while (t.qlen > bins.q[b]) ++b;
-    return fits8(t.qlen, t.h0, max_mat) ? b : bins.n + b;
+    while (len > bins.q[b]) ++b;
+    return fits8(t.qlen, t.h0, sc.max_mat) ? b : bins.n + b;
 }
 
-// Sort key: bin in bits 27-31, then query and target length, longest first.
-__global__ void ext_keys_kernel(const swb_ext_task *__restrict__ tasks, size_t n, int max_mat, int pair_ok,
+// Sort key: bin in bits 27-31, then row length and target length, longest first.
+__global__ void ext_keys_kernel(const swb_ext_task *__restrict__ tasks, size_t n, DevScoring sc, int pair_ok,
                                 uint32_t warp_cells, ExtBins bins, uint32_t *__restrict__ keys,
                                 uint32_t *__restrict__ idx, int *__restrict__ big_max_q) {
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const swb_ext_task t = tasks[i];
-    const int b = ext_bin(t, max_mat, pair_ok != 0, warp_cells, bins);
-    const uint32_t q = (uint32_t)min(max(t.qlen, 0), 4095);
+    const int b = ext_bin(t, sc, pair_ok != 0, warp_cells, bins);
+    const uint32_t q = (uint32_t)min(max(b < 2 * bins.n ? task_row_len(t, sc) : t.qlen, 0), 4095);
     const uint32_t tl = (uint32_t)min(max(t.tlen, 0), 32767);
     // Within a bin the longest tasks come first: they are claimed first, so
     // they overlap the rest instead of finishing the bin alone.
@@ -111,8 +121,9 @@ __global__ void bin_bounds_kernel(const uint32_t *__restrict__ sorted_keys, size
 template <int QMAX, int T, bool U8>
 __global__ void __launch_bounds__(T) ext_fast_kernel(ExtArgs a, int bin, int qcap_arg) {
     extern __shared__ uint32_t sm[];
-    // Rows: (qcap + 1) words of 2 (int8 scores) or 4 bytes (int16), then qcap
-    // query bytes; qcap is the bin's class bound (the rows' only use of it).
+    // Rows: (qcap + 1) words of 2 (int8 scores) or 4 bytes (int16), then
+    // qcap + 1 query bytes; qcap is the bin's class bound (the rows' only use
+    // of it).
     const int qcap = QMAX > 0 ? QMAX : qcap_arg;
     uint16_t *he16 = reinterpret_cast<uint16_t *>(sm) + threadIdx.x;
     uint32_t *he32 = sm + threadIdx.x;
@@ -129,17 +140,34 @@ __global__ void __launch_bounds__(T) ext_fast_kernel(ExtArgs a, int bin, int qca
         base = __shfl_sync(0xFFFFFFFFu, base, 0);
         if (base >= span) break;
         const uint32_t pos = lo + base + threadIdx.x;
+        uint32_t ti = 0;
+        swb_ext_task tk{};
         if (pos < hi) {
-            const uint32_t ti = a.order[pos];
-            const swb_ext_task tk = a.tasks[ti];
+            ti = a.order[pos];
+            tk = a.tasks[ti];
+        }
+        // The ring form only for warps that hold a task whose band is
+        // narrower than its query.
+        const bool ring = __any_sync(0xFFFFFFFFu, pos < hi && task_row_len(tk, a.sc) < tk.qlen);
+        if (pos < hi) {
             swb_ext_result r;
             const bool sym = a.sc.o_del + a.sc.e_del == a.sc.o_ins + a.sc.e_ins;
-            if constexpr (U8) {
-                if (sym) ext_pair_one<T, true, false>(a, tk, he16, qc, r, cells);
-                else ext_pair_one<T, false, false>(a, tk, he16, qc, r, cells);
+            if (ring) {
+                if constexpr (U8) {
+                    if (sym) ext_pair_one<T, true, false, true>(a, tk, he16, qc, r, cells);
+                    else ext_pair_one<T, false, false, true>(a, tk, he16, qc, r, cells);
+                } else {
+                    if (sym) ext_pair_one<T, true, true, true>(a, tk, he32, qc, r, cells);
+                    else ext_pair_one<T, false, true, true>(a, tk, he32, qc, r, cells);
+                }
             } else {
-                if (sym) ext_pair_one<T, true, true>(a, tk, he32, qc, r, cells);
-                else ext_pair_one<T, false, true>(a, tk, he32, qc, r, cells);
+                if constexpr (U8) {
+                    if (sym) ext_pair_one<T, true, false, false>(a, tk, he16, qc, r, cells);
+                    else ext_pair_one<T, false, false, false>(a, tk, he16, qc, r, cells);
+                } else {
+                    if (sym) ext_pair_one<T, true, true, false>(a, tk, he32, qc, r, cells);
+                    else ext_pair_one<T, false, true, false>(a, tk, he32, qc, r, cells);
+                }
             }
             a.out[ti] = r;
         }
@@ -266,11 +294,11 @@ __global__ void __launch_bounds__(T) ext_plain_kernel(ExtArgs a, size_t n, int q
             swb_ext_result r;
             const bool sym = a.sc.o_del + a.sc.e_del == a.sc.o_ins + a.sc.e_ins;
             if constexpr (U8) {
-                if (sym) ext_pair_one<T, true, false>(a, tk, he16, qc, r, cells);
-                else ext_pair_one<T, false, false>(a, tk, he16, qc, r, cells);
+                if (sym) ext_pair_one<T, true, false, false>(a, tk, he16, qc, r, cells);
+                else ext_pair_one<T, false, false, false>(a, tk, he16, qc, r, cells);
             } else {
-                if (sym) ext_pair_one<T, true, true>(a, tk, he32, qc, r, cells);
-                else ext_pair_one<T, false, true>(a, tk, he32, qc, r, cells);
+                if (sym) ext_pair_one<T, true, true, false>(a, tk, he32, qc, r, cells);
+                else ext_pair_one<T, false, true, false>(a, tk, he32, qc, r, cells);
             }
             a.out[pos] = r;
         }
@@ -280,7 +308,8 @@ __global__ void __launch_bounds__(T) ext_plain_kernel(ExtArgs a, size_t n, int q
 
 // A 16-bit (int8 scores) or 32-bit (int16) word and a query byte per column.
 size_t fast_smem_bytes(int qcap, bool u8) {
-    return ((size_t)(qcap + 1) * kFastT * (u8 ? sizeof(uint16_t) : sizeof(uint32_t)) + (size_t)qcap * kFastT + 15) &
+    return ((size_t)(qcap + 1) * kFastT * (u8 ? sizeof(uint16_t) : sizeof(uint32_t)) + (size_t)(qcap + 1) * kFastT +
+            15) &
            ~(size_t)15;
 }
 
@@ -388,8 +417,8 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
         ProfScope ps(ctx, s, "ext_keys", -1);
         // Two target rows per pass on 16-bit lanes: the gap costs must fit a lane.
         const int pair_ok = sc.o_del + sc.e_del <= 32767 && sc.o_ins + sc.e_ins <= 32767;
-        ext_keys_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(d_tasks, n, sc.max_mat, pair_ok, warp_cells, bins,
-                                                                       keys, idx, big_max_q);
+        ext_keys_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(d_tasks, n, sc, pair_ok, warp_cells, bins, keys,
+                                                                       idx, big_max_q);
     }
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
@@ -475,7 +504,8 @@ int ext_big_max_q_range(const swb_ctx *ctx, const swb_ext_task *tasks, size_t lo
     for (size_t i = lo; i < hi; ++i) {
         const swb_ext_task &t = tasks[i];
         if (t.qlen <= 0 || t.tlen <= 0) continue;
-        if (!pair_ok || t.qlen > top || !fits16(t.qlen, t.h0, sc.max_mat)) m = t.qlen > m ? t.qlen : m;
+        if (!pair_ok || task_row_len(t, sc) > top || t.qlen > kMaxLen || !fits16(t.qlen, t.h0, sc.max_mat))
+            m = t.qlen > m ? t.qlen : m;
     }
     return m;
 }

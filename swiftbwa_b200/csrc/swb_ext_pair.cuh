@@ -38,6 +38,13 @@
 //     results are used; row i+1's own checks follow in order;
 //   * band narrowing after row i+1: the first nonzero word by the reference's
 //     scan, the last one from lane 1's last column with H > 0.
+// Ring rows (RING = true): when the band is narrower than the query, the task
+// keeps P = 2w + 3 columns, column c in slot c mod P.  A row pair starting at
+// row i touches only columns i-w .. i+w+2 (the band clamps, the row-end word
+// and the zero tail), so a slot is reused only after its column has left the
+// band for good; columns P..qlen take their first-row value (the h0 ramp) and
+// query base when they enter, at the row pair whose last column reaches them.
+// The lockstep loop runs in segments that end where the slot wraps.
 // The diagonal's M != 0 rule is min(M + s, Mcap) relu with Mcap >= M + s
 // when M > 0 and 0 when M = 0: M*128 for byte scores, a 0/1 lane mask times
 // 0x7FFF for 16-bit ones.  The row max (last column on ties) is a u16x2 key
@@ -139,7 +146,7 @@ struct RowTrack {
     }
 };
 
-template <int T, bool SYM, bool W16>
+template <int T, bool SYM, bool W16, bool RING>
 __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_task &tk, RowWord<W16> *__restrict__ he,
                                              uint8_t *__restrict__ qc, swb_ext_result &res,
                                              unsigned long long &cells) {
@@ -158,11 +165,24 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
     pc.negEDel = (uint32_t)(uint16_t)(-eDel) * 0x10001u;
     pc.negEIns = (uint32_t)(uint16_t)(-eIns) * 0x10001u;
 
-    // Query profile and the first row from h0 (:44-50, :65-77).
+    const int w = ext_band_w(qlen, tk.w, tk.end_bonus, sc);                  // :52-62
+    // Columns held: the whole query, or the band's ring of 2w + 3.
+    const int P = RING ? ext_row_len(qlen, w) + 1 : qlen + 1;
+    int wb = 0;   // ring: a multiple of P at or below every live column
+    auto sl = [&](int c) -> int {
+        if constexpr (!RING) {
+            return c;
+        } else {
+            const int r = c - wb;
+            return r >= P ? r - P : r;
+        }
+    };
+    // Query profile and the first row from h0 (:44-50, :65-77); with a ring,
+    // the columns that fit it (the rest enter with the band, below).
     {
         int hv = h0;
         bool ramp = h0 > oIns + eIns;
-        for (int j = 0; j <= qlen; ++j) {
+        for (int j = 0; j < P; ++j) {
             int hj = 0;
             if (j == 0) {
                 hj = h0;
@@ -176,13 +196,6 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
             if (j < qlen) qc[j * T] = (uint8_t)span_base(a.bases, a.pac, tk.q_off, j, qlen, tk.flags, false);
             he[j * T] = (Word)hj;
         }
-    }
-    int w = tk.w;                                                              // :52-62
-    {
-        const int maxIns = (int)((double)(qlen * sc.max_mat + tk.end_bonus - oIns) / (double)eIns + 1.0);
-        w = imin(w, imax(1, maxIns));
-        const int maxDel = (int)((double)(qlen * sc.max_mat + tk.end_bonus - oDel) / (double)eDel + 1.0);
-        w = imin(w, imax(1, maxDel));
     }
     const bool tref = (tk.flags & SWB_T_FROM_REF) != 0;
     const bool tcomp = (tk.flags & SWB_T_COMPLEMENT) != 0;
@@ -202,6 +215,19 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
     int beg = 0, end = qlen;
     int i = 0;
     while (i < tlen) {
+        if constexpr (RING) {
+            // Slide the ring's base with the band, then bring in the columns
+            // this row pair reaches first: the first-row value h0 - oIns -
+            // eIns*c while positive (:65-77), else 0, and the query base.
+            while (i - w >= wb + P) wb += P;
+            const int cHi = imin(qlen, i + w + 2);
+            for (int cc = imax(P, i + w + 1); cc <= cHi; ++cc) {
+                const long long v = h0 > oIns + eIns ? (long long)h0 - oIns - (long long)eIns * cc : 0;
+                const int k = sl(cc);
+                he[k * T] = (Word)(v > 0 ? v : 0);
+                if (cc < qlen) qc[k * T] = (uint8_t)span_base(a.bases, a.pac, tk.q_off, cc, qlen, tk.flags, false);
+            }
+        }
         if (beg < i - w) beg = i - w;                                          // :95-97
         if (end > i + w + 1) end = i + w + 1;
         if (end > qlen) end = qlen;
@@ -217,8 +243,9 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
         uint32_t hPrev = 0u, nEPrev = 0u, sPrev = 0u;   // row i's word and selector for column c-1
         bool started = false;
         for (; c < e0; ++c) {
-            const uint32_t wd = he[c * T];
-            const uint32_t sel = sel_of(qc[c * T]);
+            const int k = sl(c);
+            const uint32_t wd = he[k * T];
+            const uint32_t sel = sel_of(qc[k * T]);
             const uint32_t hb = h1;
             const uint32_t up = single_cell<SYM, W16>(pc, rt0, wd, sel, c, h1, f, key, lastJ);
             hPrev = hb;
@@ -244,10 +271,11 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
             h1p |= (beg1 == 0 ? h1_init(i + 1) : 0u) << 16;
             uint32_t hPrevP = hPrev;    // lane 0 of h1 before the previous step
             uint32_t jp = (uint32_t)c | ((uint32_t)(c - 1) << 16);
-#pragma unroll 2
-            for (; c < e0; ++c, jp += 0x10001u) {
-                const uint32_t wd = he[c * T];
-                const uint32_t sel = sel_of(qc[c * T]);
+            // One lockstep step: row i's word for column c from slot ls, row i+1's
+            // word for column c-1 into slot ss.
+            auto step = [&](int ls, int ss) {
+                const uint32_t wd = he[ls * T];
+                const uint32_t sel = sel_of(qc[ls * T]);
                 const uint32_t Mp = W16 ? __byte_perm(wd, hPrevP, 0x5410) : __byte_perm(wd, hPrevP, 0x5450);   // [H(i-1,c-1), H(i,c-2)]
                 const uint32_t ep = W16 ? __byte_perm(wd, nEPrev, 0x5432) : __byte_perm(wd, nEPrev, 0x5451);   // [E(i,c),     E(i+1,c-1)]
                 const uint32_t sp = lane_score(rt1, sPrev) * 65536u + lane_score(rt0, sel);
@@ -258,7 +286,7 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
                 const uint32_t tIns = SYM ? tDel : __viaddmax_s16x2(d, pc.negOeIns, 0x80008000u);
                 fp = __viaddmax_s16x2_relu(fp, pc.negEIns, tIns);
                 // row i+1's word for c-1
-                store_up<W16>(he, T, c - 1, W16 ? __byte_perm(h1p, nE, 0x7632) : __byte_perm(h1p, nE, 0x0062));
+                store_up<W16>(he, T, ss, W16 ? __byte_perm(h1p, nE, 0x7632) : __byte_perm(h1p, nE, 0x0062));
                 if constexpr (W16) {
                     keyp = (uint32_t)__viaddmax_s32((int)__byte_perm(H, 0u, 0x1044), c, (int)keyp);
                     key1w = (uint32_t)__viaddmax_s32((int)(H & 0xFFFF0000u), c, (int)key1w);
@@ -273,6 +301,23 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
                 sPrev = sel;
                 nEPrev = nE;    // low field = row i's E', the high lane's upper bits never reach a word
                 h1p = H;
+            };
+            if constexpr (!RING) {
+#pragma unroll 2
+                for (; c < e0; ++c, jp += 0x10001u) step(c, c - 1);
+            } else {
+                int cs = sl(c);
+                while (c < e0) {
+                    if (cs == 0) {   // column c-1 sits in the ring's last slot
+                        step(0, P - 1);
+                        ++c, jp += 0x10001u, cs = 1;
+                        continue;
+                    }
+                    const int segEnd = imin(e0, c + (P - cs));
+#pragma unroll 2
+                    for (; c < segEnd; ++c, ++cs, jp += 0x10001u) step(cs, cs - 1);
+                    if (cs == P) cs = 0;
+                }
             }
             hPrev = hPrevP & 0xFFFFu;
         }
@@ -300,28 +345,29 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
         if (!started) f1 = 0u, k1 = 0u, lj1 = 0u;
         for (; s < e1; ++s) {
             // Row i's word for column s: from registers (c-1 = e0-1), the row-end word, or untouched.
-            uint32_t wd = he[s * T];
+            const int k = sl(s);
+            uint32_t wd = he[k * T];
             if (s == e0 - 1) wd = hPrev | ((nEPrev & kLoMask) << (W16 ? 16 : 8));
             else if (s == e0) wd = (uint32_t)h1i;
-            const uint32_t up = single_cell<SYM, W16>(pc, rt1, wd, sel_of(qc[s * T]), s, h1b, f1, k1, lj1);
-            store_up<W16>(he, T, s, up);
+            const uint32_t up = single_cell<SYM, W16>(pc, rt1, wd, sel_of(qc[k * T]), s, h1b, f1, k1, lj1);
+            store_up<W16>(he, T, k, up);
         }
         // H of row i+1's last valid column: from the register if it was the last
         // cell computed, else from the word the lockstep stored at column e1.
         int h1last = (int)(h1b & 0xFFFFu);
         const bool overran = started && e1 <= e0 - 2;
-        if (overran) h1last = (int)(he[e1 * T] & kLoMask);
+        if (overran) h1last = (int)(he[sl(e1) * T] & kLoMask);
         const int key1 = W16 ? (int)k1 : (int)(k1 & 0xFFFFu);
         const int rowMax1 = e1 > b1 ? (W16 ? key1 >> 16 : key1 >> 8) : 0;
         const int rowMaxJ1 = W16 ? key1 & 0xFFFF : key1 & 0xFF;
         // Words the reference holds after row i+1: h[e1] = H(e1-1), e[e1] = 0,
         // then row i's zero tail up to e0.
-        he[e1 * T] = (Word)h1last;
-        for (int z = e1 + 1; z <= e0; ++z) he[z * T] = 0;
+        he[sl(e1) * T] = (Word)h1last;
+        for (int z = e1 + 1; z <= e0; ++z) he[sl(z) * T] = 0;
         if (!tr.finish(i + 1, rowMax1, rowMaxJ1, h1last, e1 == qlen, zDrop, eDel, eIns)) break;
         // Narrowing after row i+1 (:175-180).
         int nb = b1;
-        while (nb < e1 && he[nb * T] == 0) ++nb;
+        while (nb < e1 && he[sl(nb) * T] == 0) ++nb;
         beg = nb;
         // The last nonzero word is one past the last column with H > 0 (lane 1's
         // tracker; columns past e1 computed ahead of row i's end only decay from it).

@@ -49,6 +49,24 @@ __device__ __host__ __forceinline__ bool fits16(int qlen, int h0, int max_mat) {
     return h0 >= 0 && hi <= 32000;
 }
 
+// The band half-width an extension runs with: the task's w clamped by the
+// longest insertion and deletion that can still score
+// (BandedSWScalar.swift:52-62).
+__device__ __host__ __forceinline__ int ext_band_w(int qlen, int w, int end_bonus, const DevScoring &sc) {
+    const int maxIns = (int)((double)(qlen * sc.max_mat + end_bonus - sc.o_ins) / (double)sc.e_ins + 1.0);
+    w = w < (maxIns > 1 ? maxIns : 1) ? w : (maxIns > 1 ? maxIns : 1);
+    const int maxDel = (int)((double)(qlen * sc.max_mat + end_bonus - sc.o_del) / (double)sc.e_del + 1.0);
+    return w < (maxDel > 1 ? maxDel : 1) ? w : (maxDel > 1 ? maxDel : 1);
+}
+
+// Columns a two-row extension keeps in shared memory, less one: the whole
+// query (qlen + 1 words), or, when the band is narrower than the query, a
+// ring of 2w + 3 words -- every column a row pair reads or writes lies within
+// [i - w, i + w + 2] of its first row i.
+__device__ __host__ __forceinline__ int ext_row_len(int qlen, int w_band) {
+    return (w_band >= 0 && 2LL * w_band + 2 < (long long)qlen) ? 2 * w_band + 2 : qlen;
+}
+
 // Cell counters: one per kernel family (indices below) in ctx->d_counters.
 enum CounterIdx {
     kCntExtBin0 = 0,      // extension bins 0..30 -> 0..30

@@ -292,9 +292,10 @@ using namespace swb;
 namespace {
 
 // Candidate length-class sets for a batch: the defaults, uniform steps, and
-// quantiles of the shared-memory bins' query lengths by task count and by
-// estimated cells (qlen * min(tlen, 2w+1)), 6 to 15 classes, bounds rounded
-// up to multiples of 8 and the last one covering the longest such query.
+// quantiles of the shared-memory bins' row lengths (min(qlen, 2w+2) after the
+// band clamp, ext_row_len) by task count and by estimated cells
+// (qlen * min(tlen, 2w+1)), 6 to 15 classes, bounds rounded up to multiples
+// of 8 and the last one covering the longest such row.
 std::vector<ExtBins> ext_bin_candidates(const swb_ext_task *tasks, size_t n, const DevScoring &sc) {
     std::vector<ExtBins> out;
     auto add = [&](std::vector<int> q) {
@@ -316,13 +317,15 @@ std::vector<ExtBins> ext_bin_candidates(const swb_ext_task *tasks, size_t n, con
     add(s16);
     add(s32);
     const bool pair_ok = sc.o_del + sc.e_del <= 32767 && sc.o_ins + sc.e_ins <= 32767;
-    std::vector<std::pair<int, uint64_t>> ql;   // (qlen, estimated cells) of the shared-memory bins' tasks
+    std::vector<std::pair<int, uint64_t>> ql;   // (row length, estimated cells) of the shared-memory bins' tasks
     const size_t step = std::max<size_t>(1, n / 200000);
     for (size_t i = 0; i < n; i += step) {
         const swb_ext_task &t = tasks[i];
-        if (t.qlen <= 0 || t.tlen <= 0 || !pair_ok || t.qlen > kExtSmemMaxQ || !fits16(t.qlen, t.h0, sc.max_mat)) continue;
+        if (t.qlen <= 0 || t.tlen <= 0 || !pair_ok || t.qlen > kMaxLen || !fits16(t.qlen, t.h0, sc.max_mat)) continue;
+        const int len = ext_row_len(t.qlen, ext_band_w(t.qlen, t.w, t.end_bonus, sc));
+        if (len > kExtSmemMaxQ) continue;
         const uint64_t band = 2 * (uint64_t)std::max(t.w, 0) + 1;
-        ql.push_back({t.qlen, (uint64_t)t.qlen * std::min<uint64_t>((uint64_t)t.tlen, band)});
+        ql.push_back({len, (uint64_t)t.qlen * std::min<uint64_t>((uint64_t)t.tlen, band)});
     }
     if (ql.empty()) return out;
     std::sort(ql.begin(), ql.end());

@@ -95,6 +95,23 @@ def test_ext_fuzz(engine, oracle_mod, si):
     assert gcells == cells
 
 
+@pytest.mark.parametrize("si", [0, 1, 3])
+def test_ext_ring_rows(engine, oracle_mod, si):
+    """Queries longer than their band (up to 2500 bases, w 1-150) keep a ring
+    of 2w+3 columns in the shared-memory bins: the oracle's results, with
+    first-row values (h0 up to 120) entering the ring late and queries above
+    256 bases that the int32 bin took before."""
+    sc = Scoring.default(**SCORINGS[si])
+    d = gen.ext_tasks(4242 + si, 1500, qmax=2500, ref_len=20000)
+    engine.upload_reference(d["pac"], d["ref_bases"])
+    got = engine.ext_batch(sc, d["bases"], d["tasks"])
+    exp, cells = oracle_mod.ext_batch(sc, d["bases"], d["tasks"], pac=d["pac"], ref_bases=d["ref_bases"],
+                                      n_threads=8)
+    bad = _cmp_struct(got, exp, got.dtype.names)
+    assert bad.size == 0, f"{bad.size} mismatches, first {bad[:5]}: {got[bad[:3]]} vs {exp[bad[:3]]} tasks {d['tasks'][bad[:3]]}"
+    assert engine.last_batch_stats()[1] == cells
+
+
 def test_ext_fuzz_int32_path(engine, oracle_mod):
     sc = Scoring.default()
     d = gen.ext_tasks(77, 500, qmax=120, big_scores=True)
