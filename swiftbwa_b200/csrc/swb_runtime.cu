@@ -496,26 +496,28 @@ int swb_ext_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, siz
     SWB_CUDA(cudaSetDevice(ctx->device));
     const DevScoring dsc = make_dev_scoring(*sc);
 
-    // Chunks of at least 512K tasks: a short first one (1/16 of the batch, so
-    // the GPU starts after a short copy), then seven equal ones; smaller
-    // batches are up to eight equal chunks.  The host checks chunk k (spans,
-    // the bases prefix it needs, the longest query of the int32 bin) while the
+    // Large batches (8M tasks and up): chunks that grow by half from 1/32 of
+    // the batch, so each chunk's copy (≈2.6 ns per config-1 task) ends within
+    // the kernels of the one before (≈3.6 ns per task) and the GPU waits only
+    // for the first, then two short chunks (6 % and 3 %) so that the last
+    // pass and its copy back are short.  Smaller batches: up to eight equal
+    // chunks of at least 512K tasks.  The host checks chunk k (spans, the
+    // bases prefix it needs, the longest query of the int32 bin) while the
     // GPU works on the chunks before it; chunk k starts once the prefix of
     // `bases` its tasks reference is on the device.
     const size_t kMinChunk = 1u << 19;
     std::vector<size_t> cb{0};   // chunk k is tasks[cb[k], cb[k + 1])
     {
-        const size_t n16 = n_tasks / 16;
-        if (n16 >= kMinChunk) {
-            cb.push_back(n16);
-            const size_t per7 = (n_tasks - n16 + 6) / 7;
-            for (size_t k = 1; k <= 7; ++k) cb.push_back(std::min(n_tasks, n16 + k * per7));
+        static const double kGrow[] = {1.0 / 32, 0.078, 0.148, 0.254, 0.412, 0.65, 0.91, 0.97};   // cumulative
+        if (n_tasks / 16 >= kMinChunk) {
+            for (double f : kGrow) cb.push_back((size_t)(f * (double)n_tasks));
+            cb.push_back(n_tasks);
         } else {
             const size_t m = std::min<size_t>(8, std::max<size_t>(1, n_tasks / kMinChunk)), p = (n_tasks + m - 1) / m;
             for (size_t k = 1; k <= m; ++k) cb.push_back(std::min(n_tasks, k * p));
         }
     }
-    static_assert(kMaxChunks >= 8, "chunk events");
+    static_assert(kMaxChunks >= 9, "chunk events");
     const size_t nchunks = cb.size() - 1;
     size_t per = 0;   // the largest chunk (sizes the scratch sets)
     for (size_t k = 0; k < nchunks; ++k) per = std::max(per, cb[k + 1] - cb[k]);
@@ -596,10 +598,19 @@ int swb_ext_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases, siz
         // k-1's bins may still run while chunk k sorts and starts its own.
         if (k >= 2) SWB_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->chunk_done[k - 2], 0));
         const ExtPipe pipe{(int)(k & 1), per, ctx->d2h};
-        if ((rc = launch_ext(ctx, dsc, d_b, d_t + lo, hi - lo, d_o + lo, tm.d_cells, ctx->stream, big_q, 0, &pipe))) {
+        // Small batches take the one-launch form: with too few tasks to fill
+        // the GPU, the sort and the per-bin launches cost more than they save.
+        rc = n_tasks <= kExtPlainMaxTasks
+                 ? launch_ext_plain(ctx, dsc, d_b, d_t + lo, hi - lo, d_o + lo, tm.d_cells, ctx->stream)
+                 : launch_ext(ctx, dsc, d_b, d_t + lo, hi - lo, d_o + lo, tm.d_cells, ctx->stream, big_q, 0, &pipe);
+        if (rc) {
             cudaStreamSynchronize(ctx->d2h);
             cudaStreamSynchronize(ctx->stream);
             return rc;
+        }
+        if (n_tasks <= kExtPlainMaxTasks) {   // the plain launch ran on the launching stream
+            SWB_CUDA(cudaEventRecord(ctx->fork_ev, ctx->stream));
+            SWB_CUDA(cudaStreamWaitEvent(ctx->d2h, ctx->fork_ev, 0));
         }
         // The D2H stream has waited for every bin of chunk k.
         SWB_CUDA(cudaEventRecord(ctx->chunk_done[k], ctx->d2h));

@@ -11,9 +11,11 @@
 // over the resident index, so the kernel is bound by memory latency and
 // keeps as many reads in flight as the SMs hold threads.  Warps claim 32
 // reads at a time from a counter.  Each thread's list of candidate
-// intervals (at most one per query base) lives in a column of global
-// scratch laid out [entry][thread], so a warp's threads touch adjacent
-// words when they are at the same entry.  A read's SMEMs go to its own
+// intervals (at most one per query base) keeps its first kShE entries in
+// shared memory -- the entries every backward step reads and rewrites, off
+// the chain of dependent loads -- and the rest in a column of global
+// scratch; both are laid out [entry][thread], so a warp's threads touch
+// adjacent words when they are at the same entry.  A read's SMEMs go to its own
 // window in the order found and are then sorted there (query begin, longer
 // first), as the reference sorts its array; a scan of the counts and a
 // gather pack the windows in read order, and only those entries are copied
@@ -28,6 +30,7 @@ namespace swb {
 namespace {
 
 constexpr int kSeedT = 128;   // threads per block
+constexpr int kShE = 8;       // candidate entries per thread in shared memory (28 bytes each)
 
 struct SeedArgs {
     const swb_bwt_checkpoint *cp;
@@ -46,7 +49,7 @@ struct SeedArgs {
     uint32_t *claim;            // next unclaimed read
     uint32_t *first_over;       // lowest read index with more SMEMs than cap (~0 = none)
     unsigned long long *exts;   // backward extensions (work counter)
-    // candidate intervals, [entry][slot]
+    // candidate intervals past the first kShE, [entry - kShE][slot]
     int64_t *pk, *pl, *ps;
     int2 *pmn;
     size_t nslots;
@@ -104,16 +107,34 @@ struct Cand {   // SMEMFinder.BidiInterval
     int32_t m, n;
 };
 
+// A thread's candidate list: entries 0..kShE-1 in shared memory (this
+// thread's column of sk/sl/ss, query bounds m|n as two 16-bit halves; reads
+// are at most 65535 bases), the rest in global scratch.
 struct Prev {
     const SeedArgs &g;
     size_t slot;
+    int64_t *sk, *sl, *ss;   // shared, [entry][thread], already offset by the thread
+    uint32_t *smn;
     __device__ __forceinline__ Cand get(int e) const {
-        const size_t i = (size_t)e * g.nslots + slot;
+        if (e < kShE) {
+            const int i = e * kSeedT;
+            const uint32_t mn = smn[i];
+            return {sk[i], sl[i], ss[i], (int)(mn & 0xFFFFu), (int)(mn >> 16)};
+        }
+        const size_t i = (size_t)(e - kShE) * g.nslots + slot;
         const int2 mn = g.pmn[i];
         return {g.pk[i], g.pl[i], g.ps[i], mn.x, mn.y};
     }
     __device__ __forceinline__ void put(int e, const Cand &c) const {
-        const size_t i = (size_t)e * g.nslots + slot;
+        if (e < kShE) {
+            const int i = e * kSeedT;
+            sk[i] = c.k;
+            sl[i] = c.l;
+            ss[i] = c.s;
+            smn[i] = (uint32_t)c.m | ((uint32_t)c.n << 16);
+            return;
+        }
+        const size_t i = (size_t)(e - kShE) * g.nslots + slot;
         g.pk[i] = c.k;
         g.pl[i] = c.l;
         g.ps[i] = c.s;
@@ -212,9 +233,11 @@ __device__ void sort_smems(swb_smem *w, uint32_t n) {
 }
 
 __global__ void __launch_bounds__(kSeedT) smem_kernel(SeedArgs g) {
+    __shared__ int64_t sh_k[kShE * kSeedT], sh_l[kShE * kSeedT], sh_s[kShE * kSeedT];
+    __shared__ uint32_t sh_mn[kShE * kSeedT];
     const size_t slot = blockIdx.x * (size_t)kSeedT + threadIdx.x;
     const int lane = threadIdx.x & 31;
-    const Prev prev{g, slot};
+    const Prev prev{g, slot, sh_k + threadIdx.x, sh_l + threadIdx.x, sh_s + threadIdx.x, sh_mn + threadIdx.x};
     unsigned long long exts = 0;
     for (;;) {
         uint32_t base = 0;
@@ -341,12 +364,13 @@ int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uin
     unsigned long long *d_off64 = d_n64 + off_bytes / 8;
     void *d_scan_tmp = (char *)ctx->d_out.p + out_bytes + n_bytes + 2 * off_bytes;
     // Persistent grid: resident blocks on every SM, each thread with a
-    // candidate column of max_len entries (32 bytes each).
+    // candidate column of max_len entries (32 bytes each) past the kShE it
+    // keeps in shared memory.
     int per_sm = 0;
     SWB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, smem_kernel, kSeedT, 0));
     per_sm = std::max(per_sm, 1);
     size_t blocks = std::min<size_t>((size_t)ctx->sm_count * per_sm, (n_reads + kSeedT - 1) / kSeedT);
-    const size_t entries = (size_t)std::max(max_len, 1);
+    const size_t entries = (size_t)std::max(max_len - kShE, 1);
     const size_t per_slot = entries * 32;
     const size_t avail = ctx->budget > ctx->allocated ? (ctx->budget - ctx->allocated) / 2 : 0;
     while (blocks > 1 && blocks * kSeedT * per_slot > avail) blocks /= 2;

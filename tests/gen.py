@@ -155,3 +155,18 @@ def local_tasks(seed, n, qmax=260, tmax=800, ref_len=0):
         tasks[k] = (off, off + qlen, qlen, tlen, int(rng.choice([19, 0, 5, 30, 300])), flags)
         off += qlen + tlen
     return dict(bases=np.concatenate(chunks), tasks=tasks)
+
+
+def ext_batch_binned(engine, sc, bases, tasks):
+    """Runs tasks through swb_ext_batch_device (HBM-resident inputs): always
+    the binned pass -- the host entry sends batches of up to 16384 tasks to
+    the one-launch form instead."""
+    import torch
+    from swiftbwa_b200.abi import EXT_RESULT_DTYPE
+    d_b = torch.from_numpy(np.ascontiguousarray(bases)).to("cuda:0")
+    d_t = torch.from_numpy(np.ascontiguousarray(tasks).view(np.uint8)).to("cuda:0")
+    d_o = torch.full((max(len(tasks), 1) * EXT_RESULT_DTYPE.itemsize,), 0xA5, dtype=torch.uint8, device="cuda:0")
+    s = torch.cuda.Stream()
+    engine.ext_batch_device(sc, d_b.data_ptr(), d_t.data_ptr(), len(tasks), d_o.data_ptr(), s.cuda_stream)
+    s.synchronize()
+    return d_o.cpu().numpy().view(EXT_RESULT_DTYPE)[: len(tasks)]

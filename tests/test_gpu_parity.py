@@ -86,13 +86,16 @@ def test_ext_fuzz(engine, oracle_mod, si):
     sc = Scoring.default(**SCORINGS[si])
     d = gen.ext_tasks(1000 + si, 3000, qmax=300, ref_len=5000)
     engine.upload_reference(d["pac"], d["ref_bases"])
-    got = engine.ext_batch(sc, d["bases"], d["tasks"])
+    got = engine.ext_batch(sc, d["bases"], d["tasks"])   # host entry: the one-launch form at this size
     exp, cells = oracle_mod.ext_batch(sc, d["bases"], d["tasks"], pac=d["pac"], ref_bases=d["ref_bases"],
                                       n_threads=8)
     bad = _cmp_struct(got, exp, got.dtype.names)
     assert bad.size == 0, f"{bad.size} mismatches, first {bad[:5]}: {got[bad[:3]]} vs {exp[bad[:3]]} tasks {d['tasks'][bad[:3]]}"
     ms, gcells = engine.last_batch_stats()
     assert gcells == cells
+    binned = gen.ext_batch_binned(engine, sc, d["bases"], d["tasks"])
+    bad = _cmp_struct(binned, exp, got.dtype.names)
+    assert bad.size == 0, f"binned: {bad.size} mismatches, first {bad[:5]}"
 
 
 @pytest.mark.parametrize("si", [0, 1, 3])
@@ -104,12 +107,18 @@ def test_ext_ring_rows(engine, oracle_mod, si):
     sc = Scoring.default(**SCORINGS[si])
     d = gen.ext_tasks(4242 + si, 1500, qmax=2500, ref_len=20000)
     engine.upload_reference(d["pac"], d["ref_bases"])
-    got = engine.ext_batch(sc, d["bases"], d["tasks"])
+    engine.profile(True)
+    engine.profile_reset()
+    try:
+        got = gen.ext_batch_binned(engine, sc, d["bases"], d["tasks"])
+        prof = engine.profile_read()
+    finally:
+        engine.profile(False)
     exp, cells = oracle_mod.ext_batch(sc, d["bases"], d["tasks"], pac=d["pac"], ref_bases=d["ref_bases"],
                                       n_threads=8)
     bad = _cmp_struct(got, exp, got.dtype.names)
     assert bad.size == 0, f"{bad.size} mismatches, first {bad[:5]}: {got[bad[:3]]} vs {exp[bad[:3]]} tasks {d['tasks'][bad[:3]]}"
-    assert engine.last_batch_stats()[1] == cells
+    assert sum(v[2] for k, v in prof.items() if k.startswith("ext_")) == cells
 
 
 def test_ext_fuzz_int32_path(engine, oracle_mod):
@@ -133,10 +142,9 @@ def test_ext_length_classes(engine, oracle_mod, bins):
     try:
         engine.set_ext_bins(bins)
         assert engine.ext_bins() == bins
-        got = engine.ext_batch(sc, d["bases"], d["tasks"])
+        got = gen.ext_batch_binned(engine, sc, d["bases"], d["tasks"])
         bad = _cmp_struct(got, exp, got.dtype.names)
         assert bad.size == 0, f"{bins}: {bad.size} mismatches, first {bad[:5]}"
-        assert engine.last_batch_stats()[1] == cells
     finally:
         engine.set_ext_bins(default)
 
@@ -217,9 +225,9 @@ def test_ext_config_workloads_chunked(engine, oracle_mod):
 
 
 def test_ext_large_batch_chunk_schedules(engine):
-    """A batch large enough for the host entry point's ramped chunks (a
-    short first chunk, then seven equal ones) gives the same results as its
-    two halves, each cut into equal chunks."""
+    """A batch large enough for the host entry point's growing chunks (from
+    1/32 of the batch, then two short ones at the end) gives the same results
+    as its two halves, each cut into equal chunks."""
     from swiftbwa_b200 import workloads as W
     sc = Scoring.default()
     wl = W.config1(n_reads=4_300_000, ref_len=10_000_000)
