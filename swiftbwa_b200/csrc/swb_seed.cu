@@ -13,9 +13,8 @@
 // reads at a time from a counter.  Each thread's list of candidate
 // intervals (at most one per query base) keeps its first kShE entries in
 // shared memory -- the entries every backward step reads and rewrites, off
-// the chain of dependent loads -- and the rest in a column of global
-// scratch; both are laid out [entry][thread], so a warp's threads touch
-// adjacent words when they are at the same entry.  A read's SMEMs go to its own
+// the chain of dependent loads -- laid out [entry][thread], and the rest in
+// the thread's own row of global scratch, one 32-byte sector per entry.  A read's SMEMs go to its own
 // window in the order found and are then sorted there (query begin, longer
 // first), as the reference sorts its array; a scan of the counts and a
 // gather pack the windows in read order, and only those entries are copied
@@ -49,10 +48,10 @@ struct SeedArgs {
     uint32_t *claim;            // next unclaimed read
     uint32_t *first_over;       // lowest read index with more SMEMs than cap (~0 = none)
     unsigned long long *exts;   // backward extensions (work counter)
-    // candidate intervals past the first kShE, [entry - kShE][slot]
-    int64_t *pk, *pl, *ps;
-    int2 *pmn;
-    size_t nslots;
+    // candidate intervals past the first kShE: [slot][entry - kShE], 32 bytes
+    // each ({k, l}, {s, m | n << 32})
+    longlong2 *cand;
+    size_t entries;
 };
 
 struct Intv {
@@ -121,9 +120,9 @@ struct Prev {
             const uint32_t mn = smn[i];
             return {sk[i], sl[i], ss[i], (int)(mn & 0xFFFFu), (int)(mn >> 16)};
         }
-        const size_t i = (size_t)(e - kShE) * g.nslots + slot;
-        const int2 mn = g.pmn[i];
-        return {g.pk[i], g.pl[i], g.ps[i], mn.x, mn.y};
+        const longlong2 *p = g.cand + 2 * (slot * g.entries + (size_t)(e - kShE));
+        const longlong2 kl = p[0], sm = p[1];
+        return {kl.x, kl.y, sm.x, (int)(uint32_t)sm.y, (int)((unsigned long long)sm.y >> 32)};
     }
     __device__ __forceinline__ void put(int e, const Cand &c) const {
         if (e < kShE) {
@@ -134,11 +133,9 @@ struct Prev {
             smn[i] = (uint32_t)c.m | ((uint32_t)c.n << 16);
             return;
         }
-        const size_t i = (size_t)(e - kShE) * g.nslots + slot;
-        g.pk[i] = c.k;
-        g.pl[i] = c.l;
-        g.ps[i] = c.s;
-        g.pmn[i] = make_int2(c.m, c.n);
+        longlong2 *p = g.cand + 2 * (slot * g.entries + (size_t)(e - kShE));
+        p[0] = make_longlong2(c.k, c.l);
+        p[1] = make_longlong2(c.s, (long long)((unsigned long long)(uint32_t)c.m | ((unsigned long long)(uint32_t)c.n << 32)));
     }
 };
 
@@ -394,11 +391,8 @@ int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uin
     g.n_out = d_n;
     g.claim = d_misc;
     g.first_over = d_misc + 1;
-    g.pk = (int64_t *)sp;
-    g.pl = g.pk + entries * nslots;
-    g.ps = g.pl + entries * nslots;
-    g.pmn = (int2 *)(g.ps + entries * nslots);
-    g.nslots = nslots;
+    g.cand = (longlong2 *)sp;
+    g.entries = entries;
     if (n_bases) SWB_CUDA(cudaMemcpyAsync(d_b, bases, n_bases, cudaMemcpyHostToDevice, st));
     SWB_CUDA(cudaMemcpyAsync(d_off, read_off, n_reads * 8, cudaMemcpyHostToDevice, st));
     SWB_CUDA(cudaMemcpyAsync(d_len, read_len, n_reads * 4, cudaMemcpyHostToDevice, st));
