@@ -29,7 +29,9 @@ namespace swb {
 namespace {
 
 constexpr int kSeedT = 128;   // threads per block
-constexpr int kShE = 8;       // candidate entries per thread in shared memory (28 bytes each)
+// Candidate entries per thread in shared memory (28 bytes each): 7 keep 8
+// blocks of 128 threads resident per SM (64 registers, 25 KB each).
+constexpr int kShE = 7;
 
 struct SeedArgs {
     const swb_bwt_checkpoint *cp;
@@ -229,7 +231,7 @@ __device__ void sort_smems(swb_smem *w, uint32_t n) {
     }
 }
 
-__global__ void __launch_bounds__(kSeedT) smem_kernel(SeedArgs g) {
+__global__ void __launch_bounds__(kSeedT, 8) smem_kernel(SeedArgs g) {
     __shared__ int64_t sh_k[kShE * kSeedT], sh_l[kShE * kSeedT], sh_s[kShE * kSeedT];
     __shared__ uint32_t sh_mn[kShE * kSeedT];
     const size_t slot = blockIdx.x * (size_t)kSeedT + threadIdx.x;
