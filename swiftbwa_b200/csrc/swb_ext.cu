@@ -6,7 +6,8 @@
 //     int8 rows when the score bound h0 + qlen*maxScore is at most 255,
 //     int16 rows when it is at most 32000, each in the context's length
 //     classes (ExtBins: up to 15 bounds, defaults 32..256, chosen by
-//     swb_tune_ext_bins) of the columns the task keeps, min(qlen, 2w + 2)
+//     swb_tune_ext_bins) of the columns the task keeps: its query length,
+//     or, for a query longer than the last bound, min(qlen, 2w + 2)
 //     (ext_row_len: a band narrower than the query is kept as a ring);
 //     everything else (rows above the last bound, larger scores, gap costs
 //     beyond a 16-bit lane) goes to the int32 bin.
@@ -63,9 +64,15 @@ __device__ __forceinline__ bool fits8(int qlen, int h0, int max_mat) {
     return h0 >= 0 && (long long)h0 + (long long)qlen * (max_mat > 0 ? max_mat : 0) <= 255;
 }
 
-// Columns the two-row code keeps for a task (less one), see ext_row_len.
-__device__ __host__ __forceinline__ int task_row_len(const swb_ext_task &t, const DevScoring &sc) {
-    return ext_row_len(t.qlen, ext_band_w(t.qlen, t.w, t.end_bonus, sc));
+// Columns the two-row code keeps for a task (less one): the query length,
+// or for queries longer than `ring_above` (the last length class) the
+// band's ring, ext_row_len.  Only those long queries take rings: for the
+// rest, binning by ring length mixes tasks of very different row counts in
+// a bin, and small passes -- a serving wave of 131k config-2-like tasks --
+// ran a third slower that way (100M -> 67M ext/s), for 4 % on a 20M-task
+// pass.
+__device__ __host__ __forceinline__ int task_row_len(const swb_ext_task &t, const DevScoring &sc, int ring_above) {
+    return t.qlen > ring_above ? ext_row_len(t.qlen, ext_band_w(t.qlen, t.w, t.end_bonus, sc)) : t.qlen;
 }
 
 // pair_ok: the gap costs fit a 16-bit lane (the two-row kernels of both row
@@ -75,7 +82,7 @@ __device__ __forceinline__ int ext_bin(const swb_ext_task &t, const DevScoring &
                                        const ExtBins &bins) {
     if (t.qlen <= 0 || t.tlen <= 0) return 0;
     const int big = 2 * bins.n;
-    const int len = task_row_len(t, sc);
+    const int len = task_row_len(t, sc, bins.q[bins.n - 1]);
     if (!pair_ok || len > bins.q[bins.n - 1] || t.qlen > kMaxLen || !fits16(t.qlen, t.h0, sc.max_mat)) return big;
     if (warp_cells && (unsigned long long)t.qlen * (unsigned long long)t.tlen > warp_cells) return big;
     int b = 0;
@@ -83,7 +90,10 @@ __device__ __forceinline__ int ext_bin(const swb_ext_task &t, const DevScoring &
     return fits8(t.qlen, t.h0, sc.max_mat) ? b : bins.n + b;
 }
 
-// Sort key: bin in bits 27-31, then row length and target length, longest first.
+// Sort key: bin in bits 27-31, then target length (the rows a task runs) and
+// row length, longest first: within a bin the tasks with the most rows start
+// first, so a band narrower than its query (a short ring row over many
+// target rows) does not start last and hold the bin up.
 __global__ void ext_keys_kernel(const swb_ext_task *__restrict__ tasks, size_t n, DevScoring sc, int pair_ok,
                                 uint32_t warp_cells, ExtBins bins, uint32_t *__restrict__ keys,
                                 uint32_t *__restrict__ idx, int *__restrict__ big_max_q) {
@@ -91,11 +101,11 @@ __global__ void ext_keys_kernel(const swb_ext_task *__restrict__ tasks, size_t n
     if (i >= n) return;
     const swb_ext_task t = tasks[i];
     const int b = ext_bin(t, sc, pair_ok != 0, warp_cells, bins);
-    const uint32_t q = (uint32_t)min(max(b < 2 * bins.n ? task_row_len(t, sc) : t.qlen, 0), 4095);
+    const uint32_t q = (uint32_t)min(max(b < 2 * bins.n ? task_row_len(t, sc, bins.q[bins.n - 1]) : t.qlen, 0), 4095);
     const uint32_t tl = (uint32_t)min(max(t.tlen, 0), 32767);
     // Within a bin the longest tasks come first: they are claimed first, so
     // they overlap the rest instead of finishing the bin alone.
-    keys[i] = ((uint32_t)b << 27) | ((4095u - q) << 15) | (32767u - tl);
+    keys[i] = ((uint32_t)b << 27) | ((32767u - tl) << 12) | (4095u - q);
     idx[i] = (uint32_t)i;
     if (b == 2 * bins.n) atomicMax(big_max_q, t.qlen);
 }
@@ -148,7 +158,7 @@ __global__ void __launch_bounds__(T) ext_fast_kernel(ExtArgs a, int bin, int qca
         }
         // The ring form only for warps that hold a task whose band is
         // narrower than its query.
-        const bool ring = __any_sync(0xFFFFFFFFu, pos < hi && task_row_len(tk, a.sc) < tk.qlen);
+        const bool ring = __any_sync(0xFFFFFFFFu, pos < hi && task_row_len(tk, a.sc, a.ring_above) < tk.qlen);
         if (pos < hi) {
             swb_ext_result r;
             const bool sym = a.sc.o_del + a.sc.e_del == a.sc.o_ins + a.sc.e_ins;
@@ -465,7 +475,7 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
 
     // Fork: every bin runs on its own stream after the sort, then joins back
     // (into the pipeline's join stream for pipelined passes).
-    ExtArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_out, idx2, bin_start, d_cells, claim};
+    ExtArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_out, idx2, bin_start, d_cells, claim, bins.q[bins.n - 1]};
     const cudaStream_t js = pipe ? pipe->join : s;
     ProfScope pass(ctx, s, pipe ? nullptr : "ext_pass", -1);   // fork to join, on the launching stream
     SWB_CUDA(cudaEventRecord(ctx->fork_ev, s));
@@ -504,7 +514,7 @@ int ext_big_max_q_range(const swb_ctx *ctx, const swb_ext_task *tasks, size_t lo
     for (size_t i = lo; i < hi; ++i) {
         const swb_ext_task &t = tasks[i];
         if (t.qlen <= 0 || t.tlen <= 0) continue;
-        if (!pair_ok || task_row_len(t, sc) > top || t.qlen > kMaxLen || !fits16(t.qlen, t.h0, sc.max_mat))
+        if (!pair_ok || task_row_len(t, sc, top) > top || t.qlen > kMaxLen || !fits16(t.qlen, t.h0, sc.max_mat))
             m = t.qlen > m ? t.qlen : m;
     }
     return m;

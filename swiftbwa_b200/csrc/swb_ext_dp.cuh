@@ -19,6 +19,7 @@ struct ExtArgs {
     const uint32_t *bin_start;  // bins + 1 entries
     unsigned long long *cells;
     uint32_t *claim = nullptr;  // per-bin claim counters (zeroed per pass)
+    int ring_above = 0x7FFFFFFF;   // queries longer than this keep their band as a ring (ext_row_len)
 };
 
 // ---------------------------------------------------------------- row stores

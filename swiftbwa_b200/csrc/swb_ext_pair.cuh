@@ -38,8 +38,9 @@
 //     results are used; row i+1's own checks follow in order;
 //   * band narrowing after row i+1: the first nonzero word by the reference's
 //     scan, the last one from lane 1's last column with H > 0.
-// Ring rows (RING = true): when the band is narrower than the query, the task
-// keeps P = 2w + 3 columns, column c in slot c mod P.  A row pair starting at
+// Ring rows (RING = true, for queries longer than the largest length class):
+// when the band is narrower than the query, the task keeps P = 2w + 3
+// columns, column c in slot c mod P.  A row pair starting at
 // row i touches only columns i-w .. i+w+2 (the band clamps, the row-end word
 // and the zero tail), so a slot is reused only after its column has left the
 // band for good; columns P..qlen take their first-row value (the h0 ramp) and
@@ -167,7 +168,7 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
 
     const int w = ext_band_w(qlen, tk.w, tk.end_bonus, sc);                  // :52-62
     // Columns held: the whole query, or the band's ring of 2w + 3.
-    const int P = RING ? ext_row_len(qlen, w) + 1 : qlen + 1;
+    const int P = RING && qlen > a.ring_above ? ext_row_len(qlen, w) + 1 : qlen + 1;
     int wb = 0;   // ring: a multiple of P at or below every live column
     auto sl = [&](int c) -> int {
         if constexpr (!RING) {
@@ -211,22 +212,40 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
         return (uint32_t)imax(h0 - (oDel + eDel * (row + 1)), 0);
     };
 
+    // Ring: query bases of columns past the ring's first fill (0 elsewhere),
+    // and the first-row value of a column (:65-77).
+    auto ring_q = [&](int c) -> uint32_t {
+        return RING && c >= P && c < qlen ? span_base(a.bases, a.pac, tk.q_off, c, qlen, tk.flags, false) : 0u;
+    };
+    auto ramp = [&](int c) -> int {
+        const long long v = h0 > oIns + eIns ? (long long)h0 - oIns - (long long)eIns * c : 0;
+        return v > 0 ? (int)v : 0;
+    };
+    uint32_t qA = ring_q(w + 1), qB = ring_q(w + 2);   // columns i+w+1, i+w+2 of the next row pair
     RowTrack tr{h0, -1, -1, -1, -1, 0};
     int beg = 0, end = qlen;
     int i = 0;
     while (i < tlen) {
         if constexpr (RING) {
-            // Slide the ring's base with the band, then bring in the columns
-            // this row pair reaches first: the first-row value h0 - oIns -
-            // eIns*c while positive (:65-77), else 0, and the query base.
+            // Slide the ring's base with the band, then bring in the two
+            // columns this row pair reaches first: the first-row value
+            // h0 - oIns - eIns*c while positive (:65-77), else 0, and the
+            // query base, loaded one row pair ahead.
             while (i - w >= wb + P) wb += P;
-            const int cHi = imin(qlen, i + w + 2);
-            for (int cc = imax(P, i + w + 1); cc <= cHi; ++cc) {
-                const long long v = h0 > oIns + eIns ? (long long)h0 - oIns - (long long)eIns * cc : 0;
-                const int k = sl(cc);
-                he[k * T] = (Word)(v > 0 ? v : 0);
-                if (cc < qlen) qc[k * T] = (uint8_t)span_base(a.bases, a.pac, tk.q_off, cc, qlen, tk.flags, false);
+            const int c0 = i + w + 1;
+            const uint32_t nA = ring_q(c0 + 2), nB = ring_q(c0 + 3);
+            if (c0 >= P && c0 <= qlen) {
+                const int k = sl(c0);
+                he[k * T] = (Word)ramp(c0);
+                if (c0 < qlen) qc[k * T] = (uint8_t)qA;
             }
+            if (c0 + 1 >= P && c0 + 1 <= qlen) {
+                const int k = sl(c0 + 1);
+                he[k * T] = (Word)ramp(c0 + 1);
+                if (c0 + 1 < qlen) qc[k * T] = (uint8_t)qB;
+            }
+            qA = nA;
+            qB = nB;
         }
         if (beg < i - w) beg = i - w;                                          // :95-97
         if (end > i + w + 1) end = i + w + 1;

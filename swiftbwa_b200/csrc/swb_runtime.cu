@@ -292,8 +292,9 @@ using namespace swb;
 namespace {
 
 // Candidate length-class sets for a batch: the defaults, uniform steps, and
-// quantiles of the shared-memory bins' row lengths (min(qlen, 2w+2) after the
-// band clamp, ext_row_len) by task count and by estimated cells
+// quantiles of the shared-memory bins' row lengths (the query length, or for
+// queries above 256 bases min(qlen, 2w+2) after the band clamp, ext_row_len)
+// by task count and by estimated cells
 // (qlen * min(tlen, 2w+1)), 6 to 15 classes, bounds rounded up to multiples
 // of 8 and the last one covering the longest such row.
 std::vector<ExtBins> ext_bin_candidates(const swb_ext_task *tasks, size_t n, const DevScoring &sc) {
@@ -322,7 +323,7 @@ std::vector<ExtBins> ext_bin_candidates(const swb_ext_task *tasks, size_t n, con
     for (size_t i = 0; i < n; i += step) {
         const swb_ext_task &t = tasks[i];
         if (t.qlen <= 0 || t.tlen <= 0 || !pair_ok || t.qlen > kMaxLen || !fits16(t.qlen, t.h0, sc.max_mat)) continue;
-        const int len = ext_row_len(t.qlen, ext_band_w(t.qlen, t.w, t.end_bonus, sc));
+        const int len = t.qlen <= kExtSmemMaxQ ? t.qlen : ext_row_len(t.qlen, ext_band_w(t.qlen, t.w, t.end_bonus, sc));
         if (len > kExtSmemMaxQ) continue;
         const uint64_t band = 2 * (uint64_t)std::max(t.w, 0) + 1;
         ql.push_back({len, (uint64_t)t.qlen * std::min<uint64_t>((uint64_t)t.tlen, band)});

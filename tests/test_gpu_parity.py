@@ -100,10 +100,10 @@ def test_ext_fuzz(engine, oracle_mod, si):
 
 @pytest.mark.parametrize("si", [0, 1, 3])
 def test_ext_ring_rows(engine, oracle_mod, si):
-    """Queries longer than their band (up to 2500 bases, w 1-150) keep a ring
-    of 2w+3 columns in the shared-memory bins: the oracle's results, with
-    first-row values (h0 up to 120) entering the ring late and queries above
-    256 bases that the int32 bin took before."""
+    """Queries above the last length class (256 bases; here up to 2500, w
+    1-150) whose band is narrower than the query keep a ring of 2w+3 columns
+    in the shared-memory bins instead of taking the int32 bin: the oracle's
+    results, with first-row values (h0 up to 120) entering the ring late."""
     sc = Scoring.default(**SCORINGS[si])
     d = gen.ext_tasks(4242 + si, 1500, qmax=2500, ref_len=20000)
     engine.upload_reference(d["pac"], d["ref_bases"])
