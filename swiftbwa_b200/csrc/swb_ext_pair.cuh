@@ -212,40 +212,26 @@ __device__ __forceinline__ void ext_pair_one(const ExtArgs &a, const swb_ext_tas
         return (uint32_t)imax(h0 - (oDel + eDel * (row + 1)), 0);
     };
 
-    // Ring: query bases of columns past the ring's first fill (0 elsewhere),
-    // and the first-row value of a column (:65-77).
-    auto ring_q = [&](int c) -> uint32_t {
-        return RING && c >= P && c < qlen ? span_base(a.bases, a.pac, tk.q_off, c, qlen, tk.flags, false) : 0u;
-    };
+    // Ring: the first-row value of a column entering the ring (:65-77).
     auto ramp = [&](int c) -> int {
         const long long v = h0 > oIns + eIns ? (long long)h0 - oIns - (long long)eIns * c : 0;
         return v > 0 ? (int)v : 0;
     };
-    uint32_t qA = ring_q(w + 1), qB = ring_q(w + 2);   // columns i+w+1, i+w+2 of the next row pair
     RowTrack tr{h0, -1, -1, -1, -1, 0};
     int beg = 0, end = qlen;
     int i = 0;
     while (i < tlen) {
         if constexpr (RING) {
-            // Slide the ring's base with the band, then bring in the two
-            // columns this row pair reaches first: the first-row value
-            // h0 - oIns - eIns*c while positive (:65-77), else 0, and the
-            // query base, loaded one row pair ahead.
+            // Slide the ring's base with the band, then bring in the columns
+            // this row pair reaches first: the first-row value h0 - oIns -
+            // eIns*c while positive (:65-77), else 0, and the query base.
             while (i - w >= wb + P) wb += P;
-            const int c0 = i + w + 1;
-            const uint32_t nA = ring_q(c0 + 2), nB = ring_q(c0 + 3);
-            if (c0 >= P && c0 <= qlen) {
-                const int k = sl(c0);
-                he[k * T] = (Word)ramp(c0);
-                if (c0 < qlen) qc[k * T] = (uint8_t)qA;
+            const int cHi = imin(qlen, i + w + 2);
+            for (int cc = imax(P, i + w + 1); cc <= cHi; ++cc) {
+                const int k = sl(cc);
+                he[k * T] = (Word)ramp(cc);
+                if (cc < qlen) qc[k * T] = (uint8_t)span_base(a.bases, a.pac, tk.q_off, cc, qlen, tk.flags, false);
             }
-            if (c0 + 1 >= P && c0 + 1 <= qlen) {
-                const int k = sl(c0 + 1);
-                he[k * T] = (Word)ramp(c0 + 1);
-                if (c0 + 1 < qlen) qc[k * T] = (uint8_t)qB;
-            }
-            qA = nA;
-            qB = nB;
         }
         if (beg < i - w) beg = i - w;                                          // :95-97
         if (end > i + w + 1) end = i + w + 1;
