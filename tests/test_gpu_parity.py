@@ -121,6 +121,23 @@ def test_ext_ring_rows(engine, oracle_mod, si):
     assert sum(v[2] for k, v in prof.items() if k.startswith("ext_")) == cells
 
 
+def test_ext_host_entry_small_batch_threshold(engine, oracle_mod):
+    """The host entry runs batches of up to 16384 tasks in one launch and
+    larger ones through the bins: both sides of the threshold give the
+    oracle's results and cell counts."""
+    sc = Scoring.default()
+    d = gen.ext_tasks(515, 16385, qmax=300, ref_len=8000)
+    engine.upload_reference(d["pac"], d["ref_bases"])
+    exp, _ = oracle_mod.ext_batch(sc, d["bases"], d["tasks"], pac=d["pac"], ref_bases=d["ref_bases"], n_threads=8)
+    for n in (16384, 16385):
+        got = engine.ext_batch(sc, d["bases"], d["tasks"][:n])
+        bad = _cmp_struct(got, exp[:n], got.dtype.names)
+        assert bad.size == 0, f"{n} tasks: {bad.size} mismatches, first {bad[:5]}"
+        _, cells = oracle_mod.ext_batch(sc, d["bases"], d["tasks"][:n], pac=d["pac"], ref_bases=d["ref_bases"],
+                                        n_threads=8)
+        assert engine.last_batch_stats()[1] == cells
+
+
 def test_ext_fuzz_int32_path(engine, oracle_mod):
     sc = Scoring.default()
     d = gen.ext_tasks(77, 500, qmax=120, big_scores=True)
