@@ -118,10 +118,22 @@ __device__ PassOut striped_pass(const LocalArgs &a, const swb_local_task &tk, bo
     int nPeaks = 0, lastPeak = 0;                        // lastPeak = (score << 16) | col
     bool nil = false;
     const int tLenAll = max(act ? tLen : 0, __shfl_xor_sync(kFull, act ? tLen : 0, 16));
+    // Target bases, 16 columns per load: lane l holds column c0 + l of its
+    // half's task (c0 a multiple of 16), the next 16 are loaded a block ahead,
+    // and column i is a shuffle from lane i % 16.
+    auto tload = [&](int c) -> uint32_t {
+        return act && c < tLen ? span_base(a.bases, a.pac, tk.t_off, rev ? (tLen - 1 - c) : c, tk.tlen, tk.flags, true)
+                               : 4u;
+    };
+    uint32_t tcur = tload(lane), tnext = tload(16 + lane);
     for (int i = 0; i < tLenAll; ++i) {
         const bool live = act && !nil && i < tLen;
-        uint32_t tb = 4;
-        if (live) tb = span_base(a.bases, a.pac, tk.t_off, rev ? (tLen - 1 - i) : i, tk.tlen, tk.flags, true);
+        if (i > 0 && (i & 15) == 0) {   // warp-uniform
+            tcur = tnext;
+            tnext = tload(i + 16 + lane);
+        }
+        uint32_t tb = __shfl_sync(kFull, tcur, i & 15, 16);
+        if (!live) tb = 4;
         tb = min(tb, 4u);                                // :202
         const RowTable rt = prof_table(sc, tb, bias);
         int last = 0;
