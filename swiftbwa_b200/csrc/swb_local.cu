@@ -256,7 +256,9 @@ __device__ PassOut striped_pass(const LocalArgs &a, const swb_local_task &tk, bo
     return o;
 }
 
-// Five 128-thread blocks per SM (96 registers, no spills; six spill).
+// Five 128-thread blocks per SM (96 registers; one 4-byte spill since the
+// target rows are loaded 16 columns ahead, which still ran 5 % faster; six
+// blocks spill more).
 template <int SN>
 __global__ void __launch_bounds__(kLT, 5) local_striped_kernel(LocalArgs a, int bin, uint32_t *peaks_base,
                                                             int peak_stride) {
