@@ -150,73 +150,6 @@ struct Emit {
     }
 };
 
-// SMEMFinder.findSMEMsAtPosition (SMEMFinder.swift:89-268); returns nextPos.
-__device__ int smems_at(const SeedArgs &g, const uint8_t *__restrict__ q, int readLength, int startPos,
-                        int64_t minIntv, const Prev &prev, Emit &emit, unsigned long long &exts) {
-    int nextPos = startPos + 1;
-    const int a = q[startPos];
-    if (a >= 4) return nextPos;                                              // :104-107
-    Cand smem{g.count[a], g.count[3 - a], g.count[a + 1] - g.count[a], startPos, startPos};
-    int numPrev = 0;
-    for (int j = startPos + 1; j < readLength; ++j) {                        // :124-157
-        const int base = q[j];
-        nextPos = j + 1;
-        if (base >= 4) break;
-        // Forward extension: backward extension with k/l swapped and the complement base.
-        const Intv ext = backward_ext(g, smem.l, smem.k, smem.s, 3 - base);
-        ++exts;
-        if (ext.s != smem.s) prev.put(numPrev++, smem);
-        if (ext.s < minIntv) {
-            nextPos = j;
-            break;
-        }
-        smem = Cand{ext.l, ext.k, ext.s, smem.m, j};
-    }
-    if (smem.s >= minIntv) prev.put(numPrev++, smem);                     // :160-163
-    for (int x = 0, y = numPrev - 1; x < y; ++x, --y) {                      // :166 (longest first)
-        const Cand cx = prev.get(x), cy = prev.get(y);
-        prev.put(x, cy);
-        prev.put(y, cx);
-    }
-    for (int bj = startPos - 1; bj >= 0; --bj) {                             // :169-250
-        const int base = q[bj];
-        if (base >= 4) break;
-        int numCurr = 0;
-        int64_t currS = -1;
-        int p = 0;
-        for (; p < numPrev; ++p) {
-            const Cand iv = prev.get(p);
-            const Intv ext = backward_ext(g, iv.k, iv.l, iv.s, base);
-            ++exts;
-            if (ext.s < minIntv && (iv.n - iv.m + 1) >= g.min_seed_len) { // condition 1: emit, stop
-                emit.add(iv);
-                break;
-            }
-            if (ext.s >= minIntv && ext.s != currS) {                     // condition 2: keep, stop
-                currS = ext.s;
-                prev.put(numCurr++, Cand{ext.k, ext.l, ext.s, bj, iv.n});
-                break;
-            }
-        }
-        for (p += 1; p < numPrev; ++p) {                                     // :231-246
-            const Cand iv = prev.get(p);
-            const Intv ext = backward_ext(g, iv.k, iv.l, iv.s, base);
-            ++exts;
-            if (ext.s >= minIntv && ext.s != currS) {
-                currS = ext.s;
-                prev.put(numCurr++, Cand{ext.k, ext.l, ext.s, bj, iv.n});
-            }
-        }
-        numPrev = numCurr;
-        if (numCurr == 0) break;
-    }
-    if (numPrev != 0) {                                                      // :253-265
-        const Cand iv = prev.get(0);
-        if ((iv.n - iv.m + 1) >= g.min_seed_len) emit.add(iv);
-    }
-    return nextPos;
-}
-
 // Sort by query begin, longer first (SMEMFinder.swift:53-58); equal keys
 // are equal SMEMs, so their order cannot differ from the reference's.
 __device__ void sort_smems(swb_smem *w, uint32_t n) {
@@ -231,42 +164,231 @@ __device__ void sort_smems(swb_smem *w, uint32_t n) {
     }
 }
 
-__global__ void __launch_bounds__(kSeedT, 8) smem_kernel(SeedArgs g) {
+// SMEMFinder.findAllSMEMs for one read (SMEMFinder.swift:28-59; its
+// findSMEMsAtPosition calls :89-268) followed by the internal re-seeding of
+// BWAMemAligner (BWAMemAligner.swift:283-304), written as a state machine in
+// which every step waits for one backward extension.  next() makes the
+// transitions that need none and returns the extension the read waits for
+// (false once the read is done); apply() consumes its result.  The lanes of
+// a warp walk different reads, so a warp runs next(), one backward extension
+// on every lane that has one, then apply(): the rank queries, which are the
+// work, run with the lanes converged instead of one code path at a time.
+struct Walker {
+    enum State : int { kStart, kFwd, kBwd, kDone };
+    const SeedArgs *g;
+    const uint8_t *q;
+    int len;
+    State st;
+    bool reseed;          // in the re-seeding pass (the first pass is sorted)
+    bool phase2;          // backward row: past the first kept or emitted interval
+    int pos;              // first pass: the next start position
+    uint32_t ri, n0;      // re-seeding: the next original SMEM, the originals' count
+    int64_t minIntv;      // of the current findSMEMsAtPosition call
+    int startPos, nextPos, j, bj, p, numPrev, numCurr, bbase;
+    int64_t currS;
+    Cand smem, iv;
+    Emit emit;
+
+    __device__ __forceinline__ void start(const SeedArgs &args, uint32_t r) {
+        g = &args;
+        q = args.bases + args.read_off[r];
+        len = args.read_len[r];
+        st = kStart;
+        reseed = false;
+        pos = 0;
+        emit = Emit{args.out + (size_t)r * args.cap, args.cap, 0};
+    }
+    __device__ __forceinline__ void end_call() {
+        if (!reseed) pos = nextPos;                                          // :41-51
+        st = kStart;
+    }
+    // One findSMEMsAtPosition call (:89-123).
+    __device__ __forceinline__ void call(int sp, int64_t mi) {
+        startPos = sp;
+        minIntv = mi;
+        nextPos = sp + 1;
+        const int a = q[sp];
+        if (a >= 4) {                                                        // :104-107
+            end_call();
+            return;
+        }
+        smem = Cand{g->count[a], g->count[3 - a], g->count[a + 1] - g->count[a], sp, sp};
+        numPrev = 0;
+        j = sp + 1;
+        st = kFwd;
+    }
+    __device__ __forceinline__ void bwd_done(const Prev &prev) {             // :253-265
+        if (numPrev != 0) {
+            const Cand c = prev.get(0);
+            if ((c.n - c.m + 1) >= g->min_seed_len) emit.add(c);
+        }
+        end_call();
+    }
+    // The backward phase at query position bj (:169-176).
+    __device__ __forceinline__ void bwd_row(const Prev &prev) {
+        if (bj < 0 || q[bj] >= 4) {
+            bwd_done(prev);
+            return;
+        }
+        bbase = q[bj];
+        numCurr = 0;
+        currS = -1;
+        p = 0;
+        phase2 = false;
+        st = kBwd;
+    }
+    __device__ __forceinline__ void fwd_done(const Prev &prev) {             // :160-166 (longest first)
+        if (smem.s >= minIntv) prev.put(numPrev++, smem);
+        for (int x = 0, y = numPrev - 1; x < y; ++x, --y) {
+            const Cand cx = prev.get(x), cy = prev.get(y);
+            prev.put(x, cy);
+            prev.put(y, cx);
+        }
+        bj = startPos - 1;
+        bwd_row(prev);
+    }
+    // Transitions up to the next backward extension (its interval and base
+    // in k, l, s, a); false when the read is done.
+    __device__ bool next(const Prev &prev, int64_t &k, int64_t &l, int64_t &s, int &a) {
+        for (;;) {
+            if (st == kFwd) {                                                // :124-157
+                if (j >= len) {
+                    fwd_done(prev);
+                    continue;
+                }
+                const int base = q[j];
+                nextPos = j + 1;
+                if (base >= 4) {
+                    fwd_done(prev);
+                    continue;
+                }
+                // Forward extension: backward extension with k/l swapped and the complement base.
+                k = smem.l;
+                l = smem.k;
+                s = smem.s;
+                a = 3 - base;
+                return true;
+            }
+            if (st == kBwd) {
+                if (p >= numPrev) {                                          // :248-249
+                    numPrev = numCurr;
+                    if (numCurr == 0) {
+                        bwd_done(prev);
+                        continue;
+                    }
+                    --bj;
+                    bwd_row(prev);
+                    continue;
+                }
+                iv = prev.get(p);
+                k = iv.k;
+                l = iv.l;
+                s = iv.s;
+                a = bbase;
+                return true;
+            }
+            if (st == kDone) return false;
+            // kStart
+            if (!reseed) {
+                if (pos < len) {                                             // :41-51
+                    call(pos, g->min_intv);
+                    continue;
+                }
+                // First pass done: sort it (:53-58); then re-seeding, unless
+                // the window overflowed.
+                if (emit.n > g->cap) {
+                    st = kDone;
+                    continue;
+                }
+                sort_smems(emit.w, emit.n);
+                if (g->split_len <= 0) {
+                    st = kDone;
+                    continue;
+                }
+                n0 = emit.n;
+                ri = 0;
+                reseed = true;
+                continue;
+            }
+            // Re-seeding: the first-pass SMEMs (w[0 .. n0), never overwritten:
+            // new ones are appended behind them) that are long and rare enough.
+            bool found = false;
+            while (ri < n0) {
+                const swb_smem sm = emit.w[ri++];
+                const int64_t cnt = sm.l - sm.k + 1;
+                if (sm.qe - sm.qb < g->split_len || cnt > (int64_t)g->split_width) continue;
+                call((sm.qb + sm.qe) / 2, cnt + 1);
+                found = true;
+                break;
+            }
+            if (found) continue;
+            if (emit.n > n0 && emit.n <= g->cap) sort_smems(emit.w, emit.n);
+            st = kDone;
+        }
+    }
+    // The result of the extension next() asked for.
+    __device__ __forceinline__ void apply(const Prev &prev, const Intv &ext) {
+        if (st == kFwd) {
+            if (ext.s != smem.s) prev.put(numPrev++, smem);
+            if (ext.s < minIntv) {
+                nextPos = j;
+                fwd_done(prev);
+                return;
+            }
+            smem = Cand{ext.l, ext.k, ext.s, smem.m, j};
+            ++j;
+            return;
+        }
+        // Backward row (:177-246): until the first interval that is emitted
+        // (condition 1) or kept (condition 2), then every further one kept
+        // whose size differs from the last kept.
+        if (!phase2) {
+            if (ext.s < minIntv && (iv.n - iv.m + 1) >= g->min_seed_len) {
+                emit.add(iv);
+                phase2 = true;
+            } else if (ext.s >= minIntv && ext.s != currS) {
+                currS = ext.s;
+                prev.put(numCurr++, Cand{ext.k, ext.l, ext.s, bj, iv.n});
+                phase2 = true;
+            }
+        } else if (ext.s >= minIntv && ext.s != currS) {
+            currS = ext.s;
+            prev.put(numCurr++, Cand{ext.k, ext.l, ext.s, bj, iv.n});
+        }
+        ++p;
+    }
+};
+
+__global__ void __launch_bounds__(kSeedT, 5) smem_kernel(SeedArgs g) {
     __shared__ int64_t sh_k[kShE * kSeedT], sh_l[kShE * kSeedT], sh_s[kShE * kSeedT];
     __shared__ uint32_t sh_mn[kShE * kSeedT];
     const size_t slot = blockIdx.x * (size_t)kSeedT + threadIdx.x;
     const int lane = threadIdx.x & 31;
     const Prev prev{g, slot, sh_k + threadIdx.x, sh_l + threadIdx.x, sh_s + threadIdx.x, sh_mn + threadIdx.x};
     unsigned long long exts = 0;
+    // Each lane claims its next read as soon as its current one is done, so
+    // the lanes of a warp keep walking while any read remains.
+    Walker w;
+    uint32_t r = atomicAdd(g.claim, 1u);
+    bool have = r < g.n_reads;
+    if (have) w.start(g, r);
     for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(g.claim, 32u);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        if (base >= g.n_reads) break;
-        const uint32_t r = base + lane;
-        if (r < g.n_reads) {
-            const uint8_t *q = g.bases + g.read_off[r];
-            const int len = g.read_len[r];
-            Emit emit{g.out + (size_t)r * g.cap, g.cap};
-            for (int pos = 0; pos < len;) pos = smems_at(g, q, len, pos, g.min_intv, prev, emit, exts);   // :41-51
-            if (emit.n <= g.cap) {
-                sort_smems(emit.w, emit.n);
-                // Internal re-seeding (BWAMemAligner.swift:283-304): the first
-                // pass's SMEMs stay at the front of the window while new ones
-                // are appended behind them.
-                const uint32_t n0 = emit.n;
-                if (g.split_len > 0) {
-                    for (uint32_t i = 0; i < n0; ++i) {   // originals: w[0 .. n0), never overwritten
-                        const swb_smem sm = emit.w[i];
-                        const int64_t cnt = sm.l - sm.k + 1;
-                        if (sm.qe - sm.qb < g.split_len || cnt > (int64_t)g.split_width) continue;
-                        smems_at(g, q, len, (sm.qb + sm.qe) / 2, cnt + 1, prev, emit, exts);
-                    }
-                    if (emit.n > n0 && emit.n <= g.cap) sort_smems(emit.w, emit.n);
-                }
-            }
-            g.n_out[r] = emit.n;
-            if (emit.n > g.cap) atomicMin(g.first_over, r);
+        int64_t k = 0, l = 0, s = 0;
+        int a = 0;
+        bool need = false;
+        while (have) {
+            need = w.next(prev, k, l, s, a);
+            if (need) break;
+            g.n_out[r] = w.emit.n;
+            if (w.emit.n > g.cap) atomicMin(g.first_over, r);
+            r = atomicAdd(g.claim, 1u);
+            have = r < g.n_reads;
+            if (have) w.start(g, r);
+        }
+        if (!__any_sync(0xFFFFFFFFu, need)) break;
+        if (need) {
+            w.apply(prev, backward_ext(g, k, l, s, a));
+            ++exts;
         }
     }
     for (int o = 16; o > 0; o >>= 1) exts += __shfl_down_sync(0xFFFFFFFFu, exts, o);
