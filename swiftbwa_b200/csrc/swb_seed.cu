@@ -29,8 +29,8 @@ namespace swb {
 namespace {
 
 constexpr int kSeedT = 128;   // threads per block
-// Candidate entries per thread in shared memory (28 bytes each): 7 keep 8
-// blocks of 128 threads resident per SM (64 registers, 25 KB each).
+// Candidate entries per thread in shared memory (32 bytes each; 28 KB per
+// block of 128 threads).
 constexpr int kShE = 7;
 
 struct SeedArgs {
@@ -74,33 +74,20 @@ __device__ __forceinline__ void occ4(const swb_bwt_checkpoint *__restrict__ cp, 
 }
 
 // BackwardSearch.backwardExt: the interval of base a prepended (a < 4).
+// Branch-free, so the lanes of a warp stay together: both checkpoints are
+// read even when sp and ep share a block (the second read then hits the
+// same cache line), and the base selects with conditional moves.
 __device__ __forceinline__ Intv backward_ext(const SeedArgs &g, int64_t k, int64_t l, int64_t s, int a) {
     const int64_t sp = k, ep = k + s;
     int64_t osp[4], oep[4];
     occ4(g.cp, sp, osp);
-    if ((sp >> 6) == (ep >> 6)) {
-        // Same block: the ranks at ep add the bits between sp and ep.
-        const swb_bwt_checkpoint *c = g.cp + (sp >> 6);
-        const int ys = (int)(sp & 63), ye = (int)(ep & 63);
-        const unsigned long long m = (ye == 0 ? 0ull : ~(~0ull >> ye)) & ~(ys == 0 ? 0ull : ~(~0ull >> ys));
-        const longlong2 *p = reinterpret_cast<const longlong2 *>(c);
-        const longlong2 b01 = __ldg(p + 2), b23 = __ldg(p + 3);
-        oep[0] = osp[0] + __popcll((unsigned long long)b01.x & m);
-        oep[1] = osp[1] + __popcll((unsigned long long)b01.y & m);
-        oep[2] = osp[2] + __popcll((unsigned long long)b23.x & m);
-        oep[3] = osp[3] + __popcll((unsigned long long)b23.y & m);
-    } else {
-        occ4(g.cp, ep, oep);
-    }
+    occ4(g.cp, ep, oep);
     const int64_t s0 = oep[0] - osp[0], s1 = oep[1] - osp[1], s2 = oep[2] - osp[2], s3 = oep[3] - osp[3];
     const int64_t sentinelOffset = (sp <= g.sentinel && ep > g.sentinel) ? 1 : 0;
     const int64_t l3 = l + sentinelOffset, l2 = l3 + s3, l1 = l2 + s2, l0 = l1 + s1;
-    switch (a) {
-        case 0: return {g.count[0] + osp[0], l0, s0};
-        case 1: return {g.count[1] + osp[1], l1, s1};
-        case 2: return {g.count[2] + osp[2], l2, s2};
-        default: return {g.count[3] + osp[3], l3, s3};
-    }
+    const int64_t c = a == 0 ? g.count[0] : a == 1 ? g.count[1] : a == 2 ? g.count[2] : g.count[3];
+    const int64_t o = a == 0 ? osp[0] : a == 1 ? osp[1] : a == 2 ? osp[2] : osp[3];
+    return {c + o, a == 0 ? l0 : a == 1 ? l1 : a == 2 ? l2 : l3, a == 0 ? s0 : a == 1 ? s1 : a == 2 ? s2 : s3};
 }
 
 struct Cand {   // SMEMFinder.BidiInterval
@@ -109,35 +96,25 @@ struct Cand {   // SMEMFinder.BidiInterval
 };
 
 // A thread's candidate list: entries 0..kShE-1 in shared memory (this
-// thread's column of sk/sl/ss, query bounds m|n as two 16-bit halves; reads
-// are at most 65535 bases), the rest in global scratch.
+// thread's column of two [entry][thread] arrays of 16-byte pairs), the rest
+// in the thread's row of global scratch, one 32-byte sector per entry; both
+// hold {k, l} and {s, m | n << 32}.  An entry is read and written through a
+// generic pointer chosen by a select, so lanes whose entries live in
+// different memories do not split the warp.
 struct Prev {
-    const SeedArgs &g;
-    size_t slot;
-    int64_t *sk, *sl, *ss;   // shared, [entry][thread], already offset by the thread
-    uint32_t *smn;
+    longlong2 *shkl, *shsm;   // shared, already offset by the thread
+    longlong2 *row;           // global: entry kShE + i at row[2i], row[2i + 1]
+    __device__ __forceinline__ longlong2 *kl(int e) const { return e < kShE ? shkl + e * kSeedT : row + 2 * (e - kShE); }
+    __device__ __forceinline__ longlong2 *sm(int e) const {
+        return e < kShE ? shsm + e * kSeedT : row + 2 * (e - kShE) + 1;
+    }
     __device__ __forceinline__ Cand get(int e) const {
-        if (e < kShE) {
-            const int i = e * kSeedT;
-            const uint32_t mn = smn[i];
-            return {sk[i], sl[i], ss[i], (int)(mn & 0xFFFFu), (int)(mn >> 16)};
-        }
-        const longlong2 *p = g.cand + 2 * (slot * g.entries + (size_t)(e - kShE));
-        const longlong2 kl = p[0], sm = p[1];
-        return {kl.x, kl.y, sm.x, (int)(uint32_t)sm.y, (int)((unsigned long long)sm.y >> 32)};
+        const longlong2 a = *kl(e), b = *sm(e);
+        return {a.x, a.y, b.x, (int)(uint32_t)b.y, (int)((unsigned long long)b.y >> 32)};
     }
     __device__ __forceinline__ void put(int e, const Cand &c) const {
-        if (e < kShE) {
-            const int i = e * kSeedT;
-            sk[i] = c.k;
-            sl[i] = c.l;
-            ss[i] = c.s;
-            smn[i] = (uint32_t)c.m | ((uint32_t)c.n << 16);
-            return;
-        }
-        longlong2 *p = g.cand + 2 * (slot * g.entries + (size_t)(e - kShE));
-        p[0] = make_longlong2(c.k, c.l);
-        p[1] = make_longlong2(c.s, (long long)((unsigned long long)(uint32_t)c.m | ((unsigned long long)(uint32_t)c.n << 32)));
+        *kl(e) = make_longlong2(c.k, c.l);
+        *sm(e) = make_longlong2(c.s, (long long)((unsigned long long)(uint32_t)c.m | ((unsigned long long)(uint32_t)c.n << 32)));
     }
 };
 
@@ -360,11 +337,10 @@ struct Walker {
 };
 
 __global__ void __launch_bounds__(kSeedT, 5) smem_kernel(SeedArgs g) {
-    __shared__ int64_t sh_k[kShE * kSeedT], sh_l[kShE * kSeedT], sh_s[kShE * kSeedT];
-    __shared__ uint32_t sh_mn[kShE * kSeedT];
+    __shared__ longlong2 sh_kl[kShE * kSeedT], sh_sm[kShE * kSeedT];
     const size_t slot = blockIdx.x * (size_t)kSeedT + threadIdx.x;
     const int lane = threadIdx.x & 31;
-    const Prev prev{g, slot, sh_k + threadIdx.x, sh_l + threadIdx.x, sh_s + threadIdx.x, sh_mn + threadIdx.x};
+    const Prev prev{sh_kl + threadIdx.x, sh_sm + threadIdx.x, g.cand + 2 * slot * g.entries};
     unsigned long long exts = 0;
     // Each lane claims its next read as soon as its current one is done, so
     // the lanes of a warp keep walking while any read remains.
