@@ -9,16 +9,18 @@
 // chain of rank queries into the checkpoint array (64 bytes per 64 BWT
 // positions, at most 2 checkpoints per backward extension): random reads
 // over the resident index, so the kernel is bound by memory latency and
-// keeps as many reads in flight as the SMs hold threads.  Warps claim 32
-// reads at a time from a counter.  Each thread's list of candidate
-// intervals (at most one per query base) keeps its first kShE entries in
-// shared memory -- the entries every backward step reads and rewrites, off
-// the chain of dependent loads -- laid out [entry][thread], and the rest in
-// the thread's own row of global scratch, one 32-byte sector per entry.  A read's SMEMs go to its own
-// window in the order found and are then sorted there (query begin, longer
-// first), as the reference sorts its array; a scan of the counts and a
-// gather pack the windows in read order, and only those entries are copied
-// back to the host.
+// keeps as many reads in flight as the SMs hold threads.  The walk is a
+// state machine (Walker) whose every step is one backward extension, so the
+// lanes of a warp run their rank queries together; each lane claims its next
+// read from a counter when its current one is done.  Each thread's list of
+// candidate intervals (at most one per query base) keeps its first kShE
+// entries in shared memory -- the entries every backward step reads and
+// rewrites, off the chain of dependent loads -- and the rest in the
+// thread's own row of global scratch, one 32-byte sector per entry.  A
+// read's SMEMs go to its own window in the order found and are then sorted
+// there (query begin, longer first), as the reference sorts its array; a
+// scan of the counts and a gather pack the windows in read order, and only
+// those entries are copied back to the host.
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
