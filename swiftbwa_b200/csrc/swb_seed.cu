@@ -495,9 +495,14 @@ int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uin
     g.first_over = d_misc + 1;
     g.cand = (longlong2 *)sp;
     g.entries = entries;
-    if (n_bases) SWB_CUDA(cudaMemcpyAsync(d_b, bases, n_bases, cudaMemcpyHostToDevice, st));
-    SWB_CUDA(cudaMemcpyAsync(d_off, read_off, n_reads * 8, cudaMemcpyHostToDevice, st));
-    SWB_CUDA(cudaMemcpyAsync(d_len, read_len, n_reads * 4, cudaMemcpyHostToDevice, st));
+    // Inputs through the context's pinned staging buffer in the device layout
+    // (host threads copy, then one transfer).
+    if ((rc = ensure_host(ctx, ctx->h_in, b_bytes + o_bytes + l_bytes))) return rc;
+    char *stage = (char *)ctx->h_in.p;
+    par_copy(stage, bases, n_bases);
+    par_copy(stage + b_bytes, read_off, n_reads * 8);
+    par_copy(stage + b_bytes + o_bytes, read_len, n_reads * 4);
+    SWB_CUDA(cudaMemcpyAsync(in, stage, b_bytes + o_bytes + l_bytes, cudaMemcpyHostToDevice, st));
     SWB_CUDA(cudaMemsetAsync(d_misc, 0, 4, st));
     SWB_CUDA(cudaMemsetAsync(d_misc + 1, 0xFF, 4, st));
     SWB_CUDA(cudaMemsetAsync(ctx->d_counters, 0, sizeof(unsigned long long) * kNumCounters, st));
@@ -517,10 +522,9 @@ int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uin
     SWB_CUDA(cudaGetLastError());
     SWB_CUDA(cub::DeviceScan::ExclusiveSum(d_scan_tmp, scan_bytes, d_n64, d_off64, (int)n_reads, st));
     uint32_t first_over = 0;
-    SWB_CUDA(cudaMemcpyAsync(n_out, d_n, n_reads * 4, cudaMemcpyDeviceToHost, st));
-    SWB_CUDA(cudaMemcpyAsync(out_off, d_off64, n_reads * 8, cudaMemcpyDeviceToHost, st));
-    SWB_CUDA(cudaMemcpyAsync(&first_over, d_misc + 1, 4, cudaMemcpyDeviceToHost, st));
-    SWB_CUDA(cudaStreamSynchronize(st));
+    if ((rc = d2h_staged(ctx, st, {DevSpan{d_n, n_out, n_reads * 4}, DevSpan{d_off64, out_off, n_reads * 8},
+                                   DevSpan{d_misc + 1, &first_over, 4}})))
+        return rc;
     const uint64_t total = out_off[n_reads - 1] + n_out[n_reads - 1];
     if (total > out_cap)
         return set_error(SWB_ERR_TOO_LARGE, std::to_string(total) + " SMEMs, more than out_cap (" +
@@ -532,8 +536,7 @@ int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uin
         smem_pack_kernel<<<cg, cb, 0, st>>>(d_out, d_n, d_off64, (uint32_t)n_reads, cap_per_read, d_pack);
         ctx->launches++;
         SWB_CUDA(cudaGetLastError());
-        SWB_CUDA(cudaMemcpyAsync(out, d_pack, total * sizeof(swb_smem), cudaMemcpyDeviceToHost, st));
-        SWB_CUDA(cudaStreamSynchronize(st));
+        if ((rc = d2h_staged(ctx, st, {DevSpan{d_pack, out, total * sizeof(swb_smem)}}))) return rc;
     }
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) ctx->last_ms = ms;
