@@ -21,6 +21,7 @@
 // there (query begin, longer first), as the reference sorts its array; a
 // scan of the counts and a gather pack the windows in read order, and only
 // those entries are copied back to the host.
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
@@ -49,7 +50,8 @@ struct SeedArgs {
     uint32_t cap;
     swb_smem *out;
     uint32_t *n_out;
-    uint32_t *claim;            // next unclaimed read
+    uint32_t *claim;            // next unclaimed position of `order`
+    const uint32_t *order;      // reads, least complex (most work) first
     uint32_t *first_over;       // lowest read index with more SMEMs than cap (~0 = none)
     unsigned long long *exts;   // backward extensions (work counter)
     // candidate intervals past the first kShE: [slot][entry - kShE], 32 bytes
@@ -347,8 +349,9 @@ __global__ void __launch_bounds__(kSeedT, 5) smem_kernel(SeedArgs g) {
     // Each lane claims its next read as soon as its current one is done, so
     // the lanes of a warp keep walking while any read remains.
     Walker w;
-    uint32_t r = atomicAdd(g.claim, 1u);
-    bool have = r < g.n_reads;
+    uint32_t c = atomicAdd(g.claim, 1u), r = 0;
+    bool have = c < g.n_reads;
+    if (have) r = g.order[c];
     if (have) w.start(g, r);
     for (;;) {
         int64_t k = 0, l = 0, s = 0;
@@ -359,8 +362,9 @@ __global__ void __launch_bounds__(kSeedT, 5) smem_kernel(SeedArgs g) {
             if (need) break;
             g.n_out[r] = w.emit.n;
             if (w.emit.n > g.cap) atomicMin(g.first_over, r);
-            r = atomicAdd(g.claim, 1u);
-            have = r < g.n_reads;
+            c = atomicAdd(g.claim, 1u);
+            have = c < g.n_reads;
+            if (have) r = g.order[c];
             if (have) w.start(g, r);
         }
         if (!__any_sync(0xFFFFFFFFu, need)) break;
@@ -371,6 +375,40 @@ __global__ void __launch_bounds__(kSeedT, 5) smem_kernel(SeedArgs g) {
     }
     for (int o = 16; o > 0; o >>= 1) exts += __shfl_down_sync(0xFFFFFFFFu, exts, o);
     if (lane == 0 && exts) atomicAdd(g.exts, exts);
+}
+
+// Claim order of the reads: the number of distinct 4-mers of each read as
+// the sort key, so the least complex reads -- tandem repeats, whose SA
+// intervals stay large and whose walks take many more extensions -- are
+// claimed first and the cheap ones fill the end of the launch.
+__global__ void seed_order_keys_kernel(const uint8_t *__restrict__ bases, const uint64_t *__restrict__ read_off,
+                                       const int32_t *__restrict__ read_len, uint32_t n_reads,
+                                       uint32_t *__restrict__ keys, uint32_t *__restrict__ idx) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_reads) return;
+    const uint8_t *q = bases + read_off[r];
+    const int len = read_len[r];
+    uint32_t seen[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t kmer = 0;
+    int run = 0;   // bases since the last N
+    for (int j = 0; j < len; ++j) {
+        const uint32_t b = q[j];
+        if (b >= 4) {
+            run = 0;
+            continue;
+        }
+        kmer = ((kmer << 2) | b) & 0xFFu;
+        if (++run >= 4) {
+#pragma unroll
+            for (int w = 0; w < 8; ++w)
+                if ((int)(kmer >> 5) == w) seen[w] |= 1u << (kmer & 31);
+        }
+    }
+    uint32_t d = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) d += __popc(seen[w]);
+    keys[r] = d;
+    idx[r] = r;
 }
 
 // Packs every read's window into the output in read order: read r's first
@@ -448,7 +486,14 @@ int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uin
     size_t scan_bytes = 0;
     SWB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (unsigned long long *)nullptr,
                                            (unsigned long long *)nullptr, (int)n_reads, ctx->stream));
+    size_t sort_bytes = 0;
+    SWB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (uint32_t *)nullptr, (uint32_t *)nullptr,
+                                             (uint32_t *)nullptr, (uint32_t *)nullptr, (int)n_reads, 0, 9, ctx->stream));
     int rc;
+    if ((rc = ensure_dev(ctx, ctx->d_keys, n_reads * 4)) || (rc = ensure_dev(ctx, ctx->d_keys2, n_reads * 4)) ||
+        (rc = ensure_dev(ctx, ctx->d_idx, n_reads * 4)) || (rc = ensure_dev(ctx, ctx->d_idx2, n_reads * 4)) ||
+        (rc = ensure_dev(ctx, ctx->d_sort_tmp, sort_bytes)))
+        return rc;
     if ((rc = ensure_dev(ctx, ctx->d_bases, b_bytes + o_bytes + l_bytes + 256)) ||
         (rc = ensure_dev(ctx, ctx->d_out, out_bytes + n_bytes + 2 * off_bytes + al(scan_bytes) + 256)))
         return rc;
@@ -508,6 +553,19 @@ int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uin
     SWB_CUDA(cudaMemsetAsync(ctx->d_counters, 0, sizeof(unsigned long long) * kNumCounters, st));
     g.exts = ctx->d_counters + kCntSeed;
     SWB_CUDA(cudaEventRecord(ctx->ev_start, st));
+    {
+        ProfScope ps(ctx, st, "seed_order", -1);
+        uint32_t *keys = (uint32_t *)ctx->d_keys.p, *keys2 = (uint32_t *)ctx->d_keys2.p;
+        uint32_t *idx = (uint32_t *)ctx->d_idx.p, *order = (uint32_t *)ctx->d_idx2.p;
+        const unsigned ob = 256;
+        seed_order_keys_kernel<<<(unsigned)((n_reads + ob - 1) / ob), ob, 0, st>>>(d_b, d_off, d_len, (uint32_t)n_reads,
+                                                                                   keys, idx);
+        ctx->launches++;
+        SWB_CUDA(cudaGetLastError());
+        SWB_CUDA(cub::DeviceRadixSort::SortPairs(ctx->d_sort_tmp.p, sort_bytes, keys, keys2, idx, order, (int)n_reads, 0,
+                                                 9, st));
+        g.order = order;
+    }
     {
         ProfScope ps(ctx, st, "smem_search", kCntSeed);
         smem_kernel<<<(unsigned)blocks, kSeedT, 0, st>>>(g);
