@@ -19,6 +19,7 @@
 // The host only reads one count per round.  Regions are written in place
 // (chain c's at out[seed_off ...]) and copied back once at the end.
 #include <algorithm>
+#include <thread>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -327,27 +328,62 @@ extern "C" int swb_extend_chains(swb_ctx *ctx, const swb_scoring *sc, const uint
     if (!ctx->d_pac || genome_len > ctx->ref_bases)
         return set_error(SWB_ERR_NO_REFERENCE, "the forward strand (genome_len bases) must be uploaded first");
     // Validation: spans inside the inputs, seed ranges of different chains
-    // disjoint (regions are written at each chain's seed_off).
+    // disjoint (regions are written at each chain's seed_off).  Host threads
+    // check ranges of chains; the first failing chain is reported.
+    const size_t nth = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()),
+                                        std::max<size_t>(1, n_chains / 16384));
+    struct Part {
+        size_t bad = SIZE_MAX;
+        std::string msg;
+        int max_read = 0;
+        bool sorted = true;
+        uint64_t first_off = UINT64_MAX, max_end = 0;
+    };
+    std::vector<Part> parts(nth);
+    const size_t per = (n_chains + nth - 1) / nth;
+    auto check = [&](size_t t) {
+        Part &pt = parts[t];
+        const size_t lo = std::min(n_chains, t * per), hi = std::min(n_chains, lo + per);
+        for (size_t i = lo; i < hi; ++i) {
+            const swb_chain &ch = chains[i];
+            if ((uint64_t)ch.seed_off + ch.n_seeds > n_seeds || ch.read_len < 0 || ch.read_len > kMaxLen ||
+                ch.read_off + (uint64_t)ch.read_len > n_bases) {
+                pt.bad = i;
+                pt.msg = "chain " + std::to_string(i) + ": seeds or read outside the inputs";
+                return;
+            }
+            pt.max_read = std::max(pt.max_read, ch.read_len);
+            for (uint32_t k = 0; k < ch.n_seeds; ++k) {
+                const swb_seed &sd = seeds[ch.seed_off + k];
+                if (sd.qbeg < 0 || sd.len < 0 || sd.qbeg + sd.len > ch.read_len || sd.rbeg < 0 ||
+                    sd.rbeg + sd.len > 2 * (int64_t)genome_len) {
+                    pt.bad = i;
+                    pt.msg = "chain " + std::to_string(i) + ": seed " + std::to_string(k) + " out of range";
+                    return;
+                }
+            }
+            if (ch.n_seeds) {
+                if (pt.first_off == UINT64_MAX) pt.first_off = ch.seed_off;
+                if (ch.seed_off < pt.max_end) pt.sorted = false;
+                pt.max_end = std::max<uint64_t>(pt.max_end, (uint64_t)ch.seed_off + ch.n_seeds);
+            }
+        }
+    };
+    if (nth == 1) {
+        check(0);
+    } else {
+        std::vector<std::thread> th;
+        for (size_t t = 0; t < nth; ++t) th.emplace_back(check, t);
+        for (auto &x : th) x.join();
+    }
     int max_read = 0;
     bool sorted = true;
     uint64_t prev_end = 0;
-    for (size_t i = 0; i < n_chains; ++i) {
-        const swb_chain &ch = chains[i];
-        if ((uint64_t)ch.seed_off + ch.n_seeds > n_seeds || ch.read_len < 0 || ch.read_len > kMaxLen ||
-            ch.read_off + (uint64_t)ch.read_len > n_bases)
-            return set_error(SWB_ERR_INVALID_ARG, "chain " + std::to_string(i) + ": seeds or read outside the inputs");
-        max_read = std::max(max_read, ch.read_len);
-        for (uint32_t k = 0; k < ch.n_seeds; ++k) {
-            const swb_seed &s = seeds[ch.seed_off + k];
-            if (s.qbeg < 0 || s.len < 0 || s.qbeg + s.len > ch.read_len || s.rbeg < 0 ||
-                s.rbeg + s.len > 2 * (int64_t)genome_len)
-                return set_error(SWB_ERR_INVALID_ARG,
-                                 "chain " + std::to_string(i) + ": seed " + std::to_string(k) + " out of range");
-        }
-        if (ch.n_seeds) {
-            if (ch.seed_off < prev_end) sorted = false;
-            prev_end = std::max<uint64_t>(prev_end, (uint64_t)ch.seed_off + ch.n_seeds);
-        }
+    for (const Part &pt : parts) {
+        if (pt.bad != SIZE_MAX) return set_error(SWB_ERR_INVALID_ARG, pt.msg);
+        max_read = std::max(max_read, pt.max_read);
+        sorted = sorted && pt.sorted && (pt.first_off == UINT64_MAX || pt.first_off >= prev_end);
+        prev_end = std::max(prev_end, pt.max_end);
     }
     if (!sorted) {
         std::vector<std::pair<uint32_t, uint32_t>> r;
@@ -394,9 +430,19 @@ extern "C" int swb_extend_chains(swb_ctx *ctx, const swb_scoring *sc, const uint
 
     SWB_CUDA(cudaMemsetAsync(ctx->d_counters, 0, sizeof(unsigned long long) * kNumCounters, st));
     SWB_CUDA(cudaEventRecord(ctx->ev_start, st));
-    if (n_bases) SWB_CUDA(cudaMemcpyAsync(ctx->d_bases.p, bases, n_bases, cudaMemcpyHostToDevice, st));
-    if (n_seeds) SWB_CUDA(cudaMemcpyAsync(d_seeds, seeds, n_seeds * sizeof(swb_seed), cudaMemcpyHostToDevice, st));
-    SWB_CUDA(cudaMemcpyAsync(d_chains, chains, nc * sizeof(swb_chain), cudaMemcpyHostToDevice, st));
+    // Inputs through the context's pinned staging buffer (host threads copy,
+    // then one transfer for the bases and one for the seeds and chains,
+    // which sit together at the start of the chain buffer).
+    {
+        const size_t sc_bytes = o_chains + nc * sizeof(swb_chain);
+        if ((rc = ensure_host(ctx, ctx->h_in, al256(n_bases) + sc_bytes))) return rc;
+        char *stage = (char *)ctx->h_in.p, *stage_sc = stage + al256(n_bases);
+        par_copy(stage, bases, n_bases);
+        par_copy(stage_sc + o_seeds, seeds, n_seeds * sizeof(swb_seed));
+        par_copy(stage_sc + o_chains, chains, nc * sizeof(swb_chain));
+        if (n_bases) SWB_CUDA(cudaMemcpyAsync(ctx->d_bases.p, stage, n_bases, cudaMemcpyHostToDevice, st));
+        SWB_CUDA(cudaMemcpyAsync(base, stage_sc, sc_bytes, cudaMemcpyHostToDevice, st));
+    }
     SWB_CUDA(cudaMemsetAsync(d_reg, 0, ns * sizeof(swb_region), st));
 
     // Seed order: stable descending sort of each chain's seeds by score (:155-158).
