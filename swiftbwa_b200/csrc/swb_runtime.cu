@@ -170,8 +170,9 @@ static int validate_spans(const swb_ctx *ctx, const Task *tasks, size_t n, size_
     return SWB_OK;
 }
 
-// One input part of a call (stage_in): host source, size, and where the
-// device pointer of the part is returned.
+// Copies each part straight from the caller's buffer (pinned or pageable)
+// into one device region, one cudaMemcpyAsync per part; returns the device
+// pointer of each part.
 struct Part {
     const void *src;
     size_t bytes;
@@ -221,22 +222,18 @@ int swb::d2h_staged(swb_ctx *ctx, cudaStream_t st, std::initializer_list<DevSpan
 
 namespace swb {
 
-// Inputs of one call into the context's device buffer, through its pinned
-// staging buffer in the device layout (host threads copy each part, then one
-// transfer).
+// Inputs of one call into the context's device buffer.
 static int stage_in(swb_ctx *ctx, std::initializer_list<Part> parts) {
     size_t total = 0;
     for (const Part &p : parts) total += align256(p.bytes);
     int rc;
-    if ((rc = ensure_dev(ctx, ctx->d_bases, total + 256)) || (rc = ensure_host(ctx, ctx->h_in, total + 256))) return rc;
-    char *stage = (char *)ctx->h_in.p;
+    if ((rc = ensure_dev(ctx, ctx->d_bases, total + 256))) return rc;
     size_t off = 0;
     for (const Part &p : parts) {
         *p.dev = (char *)ctx->d_bases.p + off;
-        par_copy(stage + off, p.src, p.bytes);
+        if (p.bytes) SWB_CUDA(cudaMemcpyAsync(*p.dev, p.src, p.bytes, cudaMemcpyHostToDevice, ctx->stream));
         off += align256(p.bytes);
     }
-    if (off) SWB_CUDA(cudaMemcpyAsync(ctx->d_bases.p, stage, off, cudaMemcpyHostToDevice, ctx->stream));
     return SWB_OK;
 }
 
