@@ -445,7 +445,8 @@ int swb_upload_bwt(swb_ctx *ctx, const swb_bwt_checkpoint *cp, uint64_t n_cp, co
  * SWB_ERR_TOO_LARGE naming the first such read; when the total exceeds
  * out_cap the call returns SWB_ERR_TOO_LARGE with n_out and out_off filled
  * and nothing written to out.  Either way the caller can retry with larger
- * bounds, and every other read's results are complete.  Replaces
+ * bounds, and every other read's results are complete.  At most 2^31-16
+ * reads per call.  Replaces
  * the CPU loop of BWAMemAligner.alignReadPhase1to3 (BWAMemAligner.swift:133-139)
  * and the Metal forward kernel (Kernels/smem_forward.metal:117) for a batch. */
 int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uint64_t *read_off,

@@ -463,7 +463,8 @@ int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uin
     if (!ctx || (n_reads && (!read_off || !read_len || !n_out || !out_off)) || (!out && out_cap) ||
         (!bases && n_bases))
         return set_error(SWB_ERR_INVALID_ARG, "NULL argument");
-    if (n_reads > 0xFFFFFFF0ull) return set_error(SWB_ERR_TOO_LARGE, "more than 2^32-16 reads in one batch");
+    // The claim order's sort and the offsets' scan take int counts.
+    if (n_reads > 0x7FFFFFF0ull) return set_error(SWB_ERR_TOO_LARGE, "more than 2^31-16 reads in one batch");
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->last_ms = 0;
     ctx->last_cells = 0;
