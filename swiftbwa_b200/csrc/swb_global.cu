@@ -24,6 +24,23 @@ namespace {
 constexpr int kGT = 64;   // threads per block
 constexpr int kNegInf = INT32_MIN / 2;   // GlobalAligner.swift:52
 
+// CIGARGenerator.generate repeats the DP with the band doubled while the
+// score is below the true score, at most three times (CIGARGenerator.swift:
+// 88-96).  Once the band covers the whole matrix (every row spans all qlen
+// columns: w >= max(qlen, tlen) - 1) a wider band computes the same matrix,
+// score and backpointers, so the attempts left are accounted for -- width,
+// attempt count and their qlen * tlen cells each -- instead of recomputed.
+// Returns true when it did so (the caller stops retrying).
+__device__ __forceinline__ bool nw_skip_covered_retries(int qlen, int tlen, int w, int retries, int &w0,
+                                                        swb_global_result &r, unsigned long long &cells) {
+    if (w < imax(qlen, tlen) - 1) return false;
+    const int left = 3 - retries;
+    w0 *= 1 << left;
+    r.attempts += left;
+    cells += (unsigned long long)left * (unsigned long long)qlen * (unsigned long long)tlen;
+    return true;
+}
+
 struct GlobalArgs {
     DevScoring sc;
     const uint8_t *bases;
@@ -179,6 +196,7 @@ __global__ void __launch_bounds__(kGT) global_kernel(GlobalArgs a, Scratch base)
             if (tk.flags & SWB_GLB_RETRY) {                                  // CIGARGenerator.swift:88-96
                 int retries = 0;
                 while (score < tk.true_score && retries < 3) {
+                    if (nw_skip_covered_retries(qlen, tlen, w, retries, w0, r, cells)) break;
                     w0 *= 2;
                     ++retries;
                     r.attempts++;
@@ -574,6 +592,7 @@ __global__ void __launch_bounds__(256) global_smem_kernel(GlobalArgs a, const ui
             if (tk.flags & SWB_GLB_RETRY) {                              // CIGARGenerator.swift:88-96
                 int retries = 0;
                 while (score < tk.true_score && retries < 3) {
+                    if (nw_skip_covered_retries(qlen, tlen, w, retries, w0, r, cells)) break;
                     w0 *= 2;
                     ++retries;
                     r.attempts++;
