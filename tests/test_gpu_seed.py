@@ -67,6 +67,37 @@ def test_smems_equal_oracle(engine, oracle_mod, index, min_intv, split_len):
         assert np.array_equal(got[goff[r]: goff[r] + gn[r]], exp[r * cap: r * cap + en[r]]), f"read {r}"
 
 
+def test_long_and_ragged_reads(engine, oracle_mod, index):
+    """Reads of 0 to 1500 bases in one batch (long ones keep many candidate
+    intervals, past those a lane holds in shared memory; short and empty
+    ones finish while their warp's other lanes walk on), with re-seeding."""
+    ref, idx = index
+    engine.upload_bwt(idx.cp, idx.count, idx.length, idx.sentinel)
+    rng = np.random.default_rng(99)
+    n = 700
+    lens = rng.integers(1, 1500, n).astype(np.int32)
+    lens[:60] = rng.integers(0, 4, 60)
+    rng.shuffle(lens)
+    chunks = []
+    for L in lens:
+        p = int(rng.integers(0, ref.n - max(int(L), 1)))
+        x = ref.codes[p:p + int(L)].copy()
+        if rng.random() < 0.5:
+            x = (3 - x[::-1]).astype(np.uint8)
+        x[rng.random(len(x)) < 0.01] = rng.integers(0, 4)
+        x[rng.random(len(x)) < 0.003] = 4
+        chunks.append(x)
+    bases = np.concatenate(chunks).astype(np.uint8)
+    off = np.concatenate([[0], np.cumsum(lens.astype(np.uint64))[:-1]]).astype(np.uint64)
+    cap = 512
+    got, gn, goff = engine.smem_batch(bases, off, lens, 15, cap_per_read=cap, split_len=28)
+    exp, en, over = oracle_mod.smem_batch(idx, bases, off, lens, 15, cap=cap, n_threads=8, split_len=28,
+                                          split_width=10)
+    assert over == 0 and np.array_equal(gn, en) and en.sum() > 0
+    for r in range(n):
+        assert np.array_equal(got[goff[r]: goff[r] + gn[r]], exp[r * cap: r * cap + en[r]]), f"read {r}"
+
+
 def test_small_window_reports_counts(engine, oracle_mod, index):
     from swiftbwa_b200.alignment import SWBError
     ref, idx = index
