@@ -65,12 +65,17 @@ __device__ __forceinline__ bool fits8(int qlen, int h0, int max_mat) {
 }
 
 // Columns the two-row code keeps for a task (less one): the query length,
-// or for queries longer than `ring_above` (the last length class) the
-// band's ring, ext_row_len.  Only those long queries take rings: for the
-// rest, binning by ring length mixes tasks of very different row counts in
-// a bin, and small passes -- a serving wave of 131k config-2-like tasks --
-// ran a third slower that way (100M -> 67M ext/s), for 4 % on a 20M-task
-// pass.
+// or for queries longer than `ring_above` the band's ring, ext_row_len.
+// A pass of fewer than kRingAllTasks tasks sets ring_above to the last
+// length class, so only queries beyond the classes take rings: binning by
+// ring length mixes tasks of very different row counts in a bin, and a
+// small pass ends with its slowest bin -- a serving wave of 131k
+// config-2-like tasks ran a third slower that way (100M -> 67M ext/s).  A
+// larger pass (0: every task whose band is narrower than its query) is
+// bound by throughput and gains from the occupancy (20M config-2 tasks:
+// 146.4 -> 141.3 ms).  Tasks beyond the classes take the int32 bin either
+// way, since a ring is never longer than the query.
+constexpr size_t kRingAllTasks = size_t(1) << 22;
 __device__ __host__ __forceinline__ int task_row_len(const swb_ext_task &t, const DevScoring &sc, int ring_above) {
     return t.qlen > ring_above ? ext_row_len(t.qlen, ext_band_w(t.qlen, t.w, t.end_bonus, sc)) : t.qlen;
 }
@@ -79,10 +84,10 @@ __device__ __host__ __forceinline__ int task_row_len(const swb_ext_task &t, cons
 // widths); otherwise every task takes the int32 bin.  Columns run in 16-bit
 // lanes, so queries above kMaxLen take it too (and are refused there).
 __device__ __forceinline__ int ext_bin(const swb_ext_task &t, const DevScoring &sc, bool pair_ok, uint32_t warp_cells,
-                                       const ExtBins &bins) {
+                                       const ExtBins &bins, int ring_above) {
     if (t.qlen <= 0 || t.tlen <= 0) return 0;
     const int big = 2 * bins.n;
-    const int len = task_row_len(t, sc, bins.q[bins.n - 1]);
+    const int len = task_row_len(t, sc, ring_above);
     if (!pair_ok || len > bins.q[bins.n - 1] || t.qlen > kMaxLen || !fits16(t.qlen, t.h0, sc.max_mat)) return big;
     if (warp_cells && (unsigned long long)t.qlen * (unsigned long long)t.tlen > warp_cells) return big;
     int b = 0;
@@ -95,13 +100,13 @@ __device__ __forceinline__ int ext_bin(const swb_ext_task &t, const DevScoring &
 // first, so a band narrower than its query (a short ring row over many
 // target rows) does not start last and hold the bin up.
 __global__ void ext_keys_kernel(const swb_ext_task *__restrict__ tasks, size_t n, DevScoring sc, int pair_ok,
-                                uint32_t warp_cells, ExtBins bins, uint32_t *__restrict__ keys,
+                                uint32_t warp_cells, ExtBins bins, int ring_above, uint32_t *__restrict__ keys,
                                 uint32_t *__restrict__ idx, int *__restrict__ big_max_q) {
     const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const swb_ext_task t = tasks[i];
-    const int b = ext_bin(t, sc, pair_ok != 0, warp_cells, bins);
-    const uint32_t q = (uint32_t)min(max(b < 2 * bins.n ? task_row_len(t, sc, bins.q[bins.n - 1]) : t.qlen, 0), 4095);
+    const int b = ext_bin(t, sc, pair_ok != 0, warp_cells, bins, ring_above);
+    const uint32_t q = (uint32_t)min(max(b < 2 * bins.n ? task_row_len(t, sc, ring_above) : t.qlen, 0), 4095);
     const uint32_t tl = (uint32_t)min(max(t.tlen, 0), 32767);
     // Within a bin the longest tasks come first: they are claimed first, so
     // they overlap the rest instead of finishing the bin alone.
@@ -414,6 +419,7 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
     // The context's length classes at the time of the call: the keys and the
     // launches below use the same copy.
     const ExtBins bins = ctx->ext_bins;
+    const int ring_above = n >= kRingAllTasks ? 0 : bins.q[bins.n - 1];
     const int nbins = 2 * bins.n + 1, big = 2 * bins.n;
     uint32_t *keys = (uint32_t *)ctx->d_keys.p, *keys2 = (uint32_t *)ctx->d_keys2.p;
     uint32_t *idx = (uint32_t *)ctx->d_idx.p, *idx2 = (uint32_t *)ctx->d_idx2.p + (size_t)slot * set;
@@ -427,8 +433,8 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
         ProfScope ps(ctx, s, "ext_keys", -1);
         // Two target rows per pass on 16-bit lanes: the gap costs must fit a lane.
         const int pair_ok = sc.o_del + sc.e_del <= 32767 && sc.o_ins + sc.e_ins <= 32767;
-        ext_keys_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(d_tasks, n, sc, pair_ok, warp_cells, bins, keys,
-                                                                       idx, big_max_q);
+        ext_keys_kernel<<<(unsigned)((n + tb - 1) / tb), tb, 0, s>>>(d_tasks, n, sc, pair_ok, warp_cells, bins,
+                                                                       ring_above, keys, idx, big_max_q);
     }
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
@@ -475,7 +481,7 @@ int launch_ext(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases,
 
     // Fork: every bin runs on its own stream after the sort, then joins back
     // (into the pipeline's join stream for pipelined passes).
-    ExtArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_out, idx2, bin_start, d_cells, claim, bins.q[bins.n - 1]};
+    ExtArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_out, idx2, bin_start, d_cells, claim, ring_above};
     const cudaStream_t js = pipe ? pipe->join : s;
     ProfScope pass(ctx, s, pipe ? nullptr : "ext_pass", -1);   // fork to join, on the launching stream
     SWB_CUDA(cudaEventRecord(ctx->fork_ev, s));
