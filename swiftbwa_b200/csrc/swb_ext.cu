@@ -6,9 +6,10 @@
 //     int8 rows when the score bound h0 + qlen*maxScore is at most 255,
 //     int16 rows when it is at most 32000, each in the context's length
 //     classes (ExtBins: up to 15 bounds, defaults 32..256, chosen by
-//     swb_tune_ext_bins) of the columns the task keeps: its query length,
-//     or, for a query longer than the last bound, min(qlen, 2w + 2)
-//     (ext_row_len: a band narrower than the query is kept as a ring);
+//     swb_tune_ext_bins) of the columns the task keeps: min(qlen, 2w + 2)
+//     (ext_row_len: a band narrower than the query is kept as a ring) in
+//     passes of kRingAllTasks tasks and up, else its query length unless
+//     the query is longer than the last bound;
 //     everything else (rows above the last bound, larger scores, gap costs
 //     beyond a 16-bit lane) goes to the int32 bin.
 //     The bounds are static, so no row ever saturates and nothing is re-run.
