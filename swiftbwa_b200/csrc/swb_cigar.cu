@@ -311,15 +311,26 @@ extern "C" int swb_cigar_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_
     unsigned long long *d_cl = (unsigned long long *)(base + o_cl), *d_ml = (unsigned long long *)(base + o_ml);
     unsigned long long *d_co = (unsigned long long *)(base + o_co), *d_mo = (unsigned long long *)(base + o_mo);
     // Inputs staged in pinned memory in the device layout (bases, tasks, DP
-    // index, DP tasks) by the host threads, then one copy.
+    // index, DP tasks) by the host threads, then one copy.  Bases and tasks
+    // the caller already holds in pinned memory are copied from there
+    // directly instead.
+    auto pinned = [](const void *p) {
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return at.type == cudaMemoryTypeHost;
+    };
+    const bool direct = n_bases > 0 && pinned(bases) && pinned(tasks);
     char *stage = (char *)ctx->h_in.p;
     {
         const size_t bper = (n_bases + nth - 1) / nth;
         parallel([&](size_t w) {
             const Range &r = rg[w];
             const size_t b0 = std::min(n_bases, w * bper), b1 = std::min(n_bases, b0 + bper);
-            if (b1 > b0) std::memcpy(stage + o_bases + b0, bases + b0, b1 - b0);
-            if (r.hi > r.lo)
+            if (!direct && b1 > b0) std::memcpy(stage + o_bases + b0, bases + b0, b1 - b0);
+            if (!direct && r.hi > r.lo)
                 std::memcpy(stage + o_tasks + r.lo * sizeof(swb_cigar_task), tasks + r.lo,
                             (r.hi - r.lo) * sizeof(swb_cigar_task));
             int32_t *dpi = (int32_t *)(stage + o_dpi);
@@ -341,7 +352,14 @@ extern "C" int swb_cigar_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_
     }
     SWB_CUDA(cudaMemsetAsync(ctx->d_counters, 0, sizeof(unsigned long long) * kNumCounters, st));
     SWB_CUDA(cudaEventRecord(ctx->ev_start, st));
-    SWB_CUDA(cudaMemcpyAsync(base, stage, o_dp + nd * sizeof(swb_global_task), cudaMemcpyHostToDevice, st));
+    if (direct) {
+        SWB_CUDA(cudaMemcpyAsync(base + o_bases, bases, n_bases, cudaMemcpyHostToDevice, st));
+        SWB_CUDA(cudaMemcpyAsync(base + o_tasks, tasks, n * sizeof(swb_cigar_task), cudaMemcpyHostToDevice, st));
+        SWB_CUDA(cudaMemcpyAsync(base + o_dpi, stage + o_dpi, o_dp - o_dpi + nd * sizeof(swb_global_task),
+                                 cudaMemcpyHostToDevice, st));
+    } else {
+        SWB_CUDA(cudaMemcpyAsync(base, stage, o_dp + nd * sizeof(swb_global_task), cudaMemcpyHostToDevice, st));
+    }
     if (nd) {
         if ((rc = launch_global(ctx, make_dev_scoring(*sc), (const uint8_t *)(base + o_bases),
                                 (const swb_global_task *)(base + o_dp), nd, (swb_global_result *)(base + o_gres),

@@ -286,12 +286,23 @@ def test_cigar_generate_fuzz(engine, oracle_mod, si):
         cases.append((qseg, rseg, qb, qe, rl_read, is_rev, true_score, iw, pos))
         off += len(qseg) + len(rseg)
     tasks = np.array(rows, dtype=CIGAR_TASK_DTYPE)
-    got = engine.cigar_batch(sc, np.concatenate(chunks), tasks)
+    bases = np.concatenate(chunks)
+    got = engine.cigar_batch(sc, bases, tasks)
     for k, c in enumerate(cases):
         exp = oracle_mod.cigar_generate(c[0], c[1], c[2], c[3], c[4], c[5], c[6], c[7], sc, c[8])
         g = got[k]
         assert (g["cigar"], g["nm"], g["md"], g["score"], g["pos"], g["used_dp"]) == \
             (exp["cigar"], exp["nm"], exp["md"], exp["score"], exp["pos"], exp["used_dp"]), (k, g, exp)
+    # Pinned inputs are copied straight to the device: the same results.
+    import torch
+    pb = torch.from_numpy(bases).pin_memory().numpy()
+    pt = torch.from_numpy(tasks.view(np.uint8)).pin_memory().numpy().view(CIGAR_TASK_DTYPE)
+    ra, ca, ma = engine.cigar_batch_raw(sc, bases, tasks)
+    rb, cb, mb = engine.cigar_batch_raw(sc, pb, pt)
+    assert np.array_equal(ra, rb)
+    nc = int((ra["cigar_off"] + ra["n_cigar"].astype(np.uint64)).max())
+    nm = int((ra["md_off"] + ra["md_len"].astype(np.uint64)).max())
+    assert np.array_equal(ca[:nc], cb[:nc]) and np.array_equal(ma[:nm], mb[:nm])
 
 
 def test_alu_probes(engine):
