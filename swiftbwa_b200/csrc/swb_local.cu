@@ -19,6 +19,9 @@
 // that restates scalarAlign/scalarSWPass (:327-492).
 #include <cub/device/device_radix_sort.cuh>
 
+#include <algorithm>
+#include <atomic>
+
 #include "swb_device.cuh"
 #include "swb_internal.h"
 
@@ -40,6 +43,7 @@ struct LocalArgs {
     uint32_t *fallback;          // task indices for the scalar kernel
     unsigned int *fallback_n;
     unsigned long long *cells;
+    uint32_t *claim;             // per-bin claim counters (zeroed per call)
 };
 
 __device__ __forceinline__ int clamp_min_sub(int v) { return v < 0 ? 0 : (v > 255 ? 255 : v); }
@@ -258,22 +262,29 @@ __device__ PassOut striped_pass(const LocalArgs &a, const swb_local_task &tk, bo
 
 // Five 128-thread blocks per SM (96 registers; one 4-byte spill since the
 // target rows are loaded 16 columns ahead, which still ran 5 % faster; six
-// blocks spill more).
+// blocks spill more).  The grid is the device's resident blocks; each
+// half-warp claims its next task of the bin from the bin's counter, longest
+// target first (the sort puts them last), so the launch ends with the work
+// rather than on a partly filled last wave of fixed slices.
 template <int SN>
 __global__ void __launch_bounds__(kLT, 5) local_striped_kernel(LocalArgs a, int bin, uint32_t *peaks_base,
                                                             int peak_stride) {
     const int lane = threadIdx.x & 15;
     const unsigned half_mask = (threadIdx.x & 16) ? 0xFFFF0000u : 0x0000FFFFu;
     const uint32_t lo = a.bin_start[bin], hi = a.bin_start[bin + 1];
-    const uint32_t halves = gridDim.x * (kLT / 16);
     const uint32_t my_half = blockIdx.x * (kLT / 16) + (threadIdx.x >> 4);
     uint32_t *peaks = peaks_base + (size_t)my_half * peak_stride;
     unsigned long long cells = 0;
     const uint32_t span = hi - lo;
-    const uint32_t iters = (span + halves - 1) / halves;
-    for (uint32_t it = 0; it < iters; ++it) {
-        const uint32_t pos = lo + it * halves + my_half;
-        const bool act = pos < hi;
+    bool done = false;
+    for (;;) {
+        uint32_t k = 0;
+        if (!done && lane == 0) k = atomicAdd(a.claim + bin, 1u);
+        k = __shfl_sync(kFull, k, threadIdx.x & 16);   // the half's claim
+        done = done || k >= span;
+        if (__all_sync(kFull, done)) break;            // both halves of the warp go on together
+        const uint32_t pos = hi - 1 - k;
+        const bool act = !done;
         const uint32_t ti = act ? a.order[pos] : 0;
         swb_local_task tk{};
         if (act) tk = a.tasks[ti];
@@ -430,7 +441,15 @@ __global__ void local_bounds_kernel(const uint32_t *__restrict__ sorted_keys, co
 template <int SN>
 int launch_sn(swb_ctx *ctx, const LocalArgs &a, cudaStream_t st, uint32_t *peaks, int peak_stride, size_t halves_cap,
               size_t n_bin) {
-    const size_t halves = std::min(halves_cap, n_bin);
+    // Resident blocks per SM of this instance (the same on every device the
+    // library runs on: sm_100).
+    static std::atomic<int> occ{0};
+    if (occ.load(std::memory_order_relaxed) == 0) {
+        int b = 0;
+        SWB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, local_striped_kernel<SN>, kLT, 0));
+        occ.store(b > 0 ? b : 1, std::memory_order_relaxed);
+    }
+    const size_t halves = std::min({halves_cap, n_bin, (size_t)ctx->sm_count * occ.load() * (kLT / 16)});
     const size_t grid = (halves + kLT / 16 - 1) / (kLT / 16);
     if (grid == 0) return SWB_OK;
     static const char *names[17] = {"", "local_striped_sn1", "local_striped_sn2", "local_striped_sn3",
@@ -463,7 +482,8 @@ int launch_local(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases, con
     uint32_t *fallback = idx2 + n;
     uint32_t *bin_start = (uint32_t *)ctx->d_misc.p;          // 18 words
     unsigned int *fallback_n = (unsigned int *)((char *)ctx->d_misc.p + 128);
-    SWB_CUDA(cudaMemsetAsync(fallback_n, 0, sizeof(unsigned), st));
+    uint32_t *claim = (uint32_t *)((char *)ctx->d_misc.p + 160);   // 17 per-bin claim counters
+    SWB_CUDA(cudaMemsetAsync(fallback_n, 0, 128, st));              // fallback count and claim counters
     local_keys_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_tasks, n, sc.a, keys, idx);
     ctx->launches++;
     SWB_CUDA(cudaGetLastError());
@@ -488,7 +508,7 @@ int launch_local(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases, con
     int *ebuf = hbuf + (size_t)(max_t + 1) * nsl;
     unsigned long long *pbuf = (unsigned long long *)(ebuf + (size_t)(max_t + 1) * nsl);
 
-    LocalArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_out, idx2, bin_start, fallback, fallback_n, d_cells};
+    LocalArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_out, idx2, bin_start, fallback, fallback_n, d_cells, claim};
     // Bin sizes are not known on the host; each instantiation's grid covers
     // up to n tasks and idles past its slice.  Only stripe counts that can
     // occur for max_q are launched.
