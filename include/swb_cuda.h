@@ -299,9 +299,9 @@ int swb_tune_ext_bins(swb_ctx *ctx, const swb_scoring *sc, const uint8_t *bases,
  * h0 + qlen*maxScore above 32000) may have at most 1024 query bases; a
  * longer one gets an all-zero result and the call returns
  * SWB_ERR_TOO_LARGE naming the first such task.  The first call on a device
- * does a one-time set-up (looks up the array's address, sizes a kernel).
- * Every call synchronises `stream` to read its status words, so no call can
- * be captured into a CUDA graph.  Calls share the array: calls from threads of one
+ * does a one-time set-up (looks up the array's address, sizes a kernel), so
+ * make that first call before any stream capture.  Every call synchronises
+ * `stream` to read its status words.  Calls share the array: calls from threads of one
  * process take turns (a per-device lock held until the stream is done);
  * calls from different processes on one GPU that overlap there race. */
 int swb_ext_batch_static(const swb_scoring *sc, const uint8_t *d_bases, const uint8_t *d_pac,

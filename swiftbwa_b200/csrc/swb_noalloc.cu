@@ -10,8 +10,9 @@
 // file-scope array below.  The driver places it on a GPU when this file's
 // device code is loaded there -- with CUDA's default lazy module loading,
 // at the first call on that GPU (a call with zero tasks is enough) -- and
-// keeps it until the process exits.  A caller that is about to give the
-// free HBM to its own arena makes that first call before.
+// keeps it until the process exits.  That first call also does the
+// one-time set-up below, so a caller makes it before any stream capture,
+// and before it gives the free HBM to its own arena.
 //
 // It runs the same device code as swb_ext_batch_device (swb_ext_dp.cuh),
 // without the sort/binning pass: tasks are taken in input order by the
