@@ -220,7 +220,9 @@ int swb_global_batch(swb_ctx *ctx, const swb_scoring *sc,
  * cigar_cap >= sum of (qlen + rlen + 2); md_cap >= sum of (6*(qlen+rlen)+8).
  * Bases and tasks in pinned host memory (cudaHostAlloc / registered) are
  * copied straight to the device; pageable ones go through the context's
- * pinned staging buffer. */
+ * pinned staging buffer.  Likewise results, cigar_out and md_out: when all
+ * three are pinned the device writes them directly, else through pinned
+ * staging and host threads. */
 int swb_cigar_batch(swb_ctx *ctx, const swb_scoring *sc,
                     const uint8_t *bases, size_t n_bases,
                     const swb_cigar_task *tasks, size_t n_tasks,

@@ -147,18 +147,32 @@ class Engine:
                "swb_local_batch")
         return out
 
-    def cigar_batch_raw(self, sc: Scoring, bases: np.ndarray, tasks: np.ndarray):
+    @staticmethod
+    def cigar_caps(tasks: np.ndarray):
+        """(cigar_cap, md_cap) that swb_cigar_batch requires for `tasks`:
+        sum of (qlen + rlen + 2) words and of (6*(qlen + rlen) + 8) bytes."""
+        n = len(tasks)
+        s = int(tasks["qlen"].sum(dtype=np.int64)) + int(tasks["rlen"].sum(dtype=np.int64))
+        return s + 2 * n + 1, 6 * s + 8 * n + 1
+
+    def cigar_batch_raw(self, sc: Scoring, bases: np.ndarray, tasks: np.ndarray, out=None):
         """CIGARGenerator.generate over CIGAR_TASK_DTYPE tasks -> (CIGAR_RESULT_DTYPE
         array, packed CIGAR words, MD bytes); task k's CIGAR is
-        cigar[cigar_off : cigar_off + n_cigar], its MD md[md_off : md_off + md_len]."""
+        cigar[cigar_off : cigar_off + n_cigar], its MD md[md_off : md_off + md_len].
+        out: optional (results, cigar words, MD bytes) arrays to write into, at
+        least len(tasks) results and cigar_caps(tasks) long (in pinned memory
+        the device writes them directly)."""
         assert tasks.dtype == abi.CIGAR_TASK_DTYPE
-        ql = tasks["qlen"].astype(np.int64)
-        rl = tasks["rlen"].astype(np.int64)
-        ccap = int((ql + rl + 2).sum()) + 1
-        mcap = int((6 * (ql + rl) + 8).sum()) + 1
-        res = np.zeros(len(tasks), abi.CIGAR_RESULT_DTYPE)
-        cig = np.empty(ccap, np.uint32)
-        md = np.empty(mcap, np.uint8)
+        if out is None:
+            ccap, mcap = self.cigar_caps(tasks)
+            res = np.zeros(len(tasks), abi.CIGAR_RESULT_DTYPE)
+            cig = np.empty(ccap, np.uint32)
+            md = np.empty(mcap, np.uint8)
+        else:
+            res, cig, md = out
+            assert res.dtype == abi.CIGAR_RESULT_DTYPE and len(res) >= len(tasks)
+            assert cig.dtype == np.uint32 and md.dtype == np.uint8
+            ccap, mcap = cig.size, md.size
         bases = np.ascontiguousarray(bases, dtype=np.uint8)
         if bases.size == 0:
             bases = np.zeros(1, np.uint8)

@@ -405,24 +405,35 @@ extern "C" int swb_cigar_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_
         ctx->launches++;
         SWB_CUDA(cudaGetLastError());
     }
-    // Results, CIGAR words and MD bytes back through pinned memory.
+    // Results, CIGAR words and MD bytes back: straight into the caller's
+    // buffers when they are pinned, else through pinned staging and host
+    // threads.
     const size_t r_bytes = n * sizeof(swb_cigar_result), c_bytes = tot_c * 4;
-    if ((rc = ensure_host(ctx, ctx->h_out, al256(r_bytes) + al256(c_bytes) + al256(tot_m)))) return rc;
-    char *back = (char *)ctx->h_out.p;
-    SWB_CUDA(cudaMemcpyAsync(back, base + o_res, r_bytes, cudaMemcpyDeviceToHost, st));
-    if (tot_c) SWB_CUDA(cudaMemcpyAsync(back + al256(r_bytes), d_cig, c_bytes, cudaMemcpyDeviceToHost, st));
-    if (tot_m) SWB_CUDA(cudaMemcpyAsync(back + al256(r_bytes) + al256(c_bytes), d_md, tot_m, cudaMemcpyDeviceToHost, st));
-    SWB_CUDA(cudaEventRecord(ctx->ev_stop, st));
-    SWB_CUDA(cudaStreamSynchronize(st));
-    parallel([&](size_t w) {
-        auto part = [&](void *dst, const char *src, size_t bytes) {
-            const size_t per = (bytes + nth - 1) / nth, a0 = std::min(bytes, w * per), a1 = std::min(bytes, a0 + per);
-            if (a1 > a0) std::memcpy((char *)dst + a0, src + a0, a1 - a0);
-        };
-        part(results, back, r_bytes);
-        part(cigar_out, back + al256(r_bytes), c_bytes);
-        part(md_out, back + al256(r_bytes) + al256(c_bytes), tot_m);
-    });
+    const bool direct_out = pinned(results) && (tot_c == 0 || pinned(cigar_out)) && (tot_m == 0 || pinned(md_out));
+    if (direct_out) {
+        SWB_CUDA(cudaMemcpyAsync(results, base + o_res, r_bytes, cudaMemcpyDeviceToHost, st));
+        if (tot_c) SWB_CUDA(cudaMemcpyAsync(cigar_out, d_cig, c_bytes, cudaMemcpyDeviceToHost, st));
+        if (tot_m) SWB_CUDA(cudaMemcpyAsync(md_out, d_md, tot_m, cudaMemcpyDeviceToHost, st));
+        SWB_CUDA(cudaEventRecord(ctx->ev_stop, st));
+        SWB_CUDA(cudaStreamSynchronize(st));
+    } else {
+        if ((rc = ensure_host(ctx, ctx->h_out, al256(r_bytes) + al256(c_bytes) + al256(tot_m)))) return rc;
+        char *back = (char *)ctx->h_out.p;
+        SWB_CUDA(cudaMemcpyAsync(back, base + o_res, r_bytes, cudaMemcpyDeviceToHost, st));
+        if (tot_c) SWB_CUDA(cudaMemcpyAsync(back + al256(r_bytes), d_cig, c_bytes, cudaMemcpyDeviceToHost, st));
+        if (tot_m) SWB_CUDA(cudaMemcpyAsync(back + al256(r_bytes) + al256(c_bytes), d_md, tot_m, cudaMemcpyDeviceToHost, st));
+        SWB_CUDA(cudaEventRecord(ctx->ev_stop, st));
+        SWB_CUDA(cudaStreamSynchronize(st));
+        parallel([&](size_t w) {
+            auto part = [&](void *dst, const char *src, size_t bytes) {
+                const size_t per = (bytes + nth - 1) / nth, a0 = std::min(bytes, w * per), a1 = std::min(bytes, a0 + per);
+                if (a1 > a0) std::memcpy((char *)dst + a0, src + a0, a1 - a0);
+            };
+            part(results, back, r_bytes);
+            part(cigar_out, back + al256(r_bytes), c_bytes);
+            part(md_out, back + al256(r_bytes) + al256(c_bytes), tot_m);
+        });
+    }
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) == cudaSuccess) ctx->last_ms = ms;
     unsigned long long c[kNumCounters] = {0};

@@ -303,6 +303,16 @@ def test_cigar_generate_fuzz(engine, oracle_mod, si):
     nc = int((ra["cigar_off"] + ra["n_cigar"].astype(np.uint64)).max())
     nm = int((ra["md_off"] + ra["md_len"].astype(np.uint64)).max())
     assert np.array_equal(ca[:nc], cb[:nc]) and np.array_equal(ma[:nm], mb[:nm])
+    # Pinned output buffers are written by the device directly: the same results.
+    from swiftbwa_b200.abi import CIGAR_RESULT_DTYPE
+    ccap, mcap = engine.cigar_caps(tasks)
+    po = (torch.full((len(tasks) * CIGAR_RESULT_DTYPE.itemsize,), 0xA5, dtype=torch.uint8).pin_memory().numpy()
+          .view(CIGAR_RESULT_DTYPE),
+          torch.full((ccap,), -1, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
+          torch.full((mcap,), 0xA5, dtype=torch.uint8).pin_memory().numpy())
+    rc, cc, mc = engine.cigar_batch_raw(sc, pb, pt, out=po)
+    assert rc is po[0] and np.array_equal(ra, rc)
+    assert np.array_equal(ca[:nc], cc[:nc]) and np.array_equal(ma[:nm], mc[:nm])
 
 
 def test_alu_probes(engine):
