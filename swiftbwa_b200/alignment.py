@@ -138,9 +138,12 @@ class Engine:
                                          ptr(cig, C.c_uint32), cap), "swb_global_batch")
         return res, cig
 
-    def local_batch(self, sc: Scoring, bases: np.ndarray, tasks: np.ndarray) -> np.ndarray:
+    def local_batch(self, sc: Scoring, bases: np.ndarray, tasks: np.ndarray,
+                    out: Optional[np.ndarray] = None) -> np.ndarray:
         assert tasks.dtype == LOCAL_TASK_DTYPE
-        out = np.zeros(len(tasks), LOCAL_RESULT_DTYPE)
+        if out is None:
+            out = np.zeros(len(tasks), LOCAL_RESULT_DTYPE)
+        assert out.dtype == LOCAL_RESULT_DTYPE and len(out) >= len(tasks)
         bases = np.ascontiguousarray(bases, dtype=np.uint8)
         _check(self.lib.swb_local_batch(self.h, C.byref(sc), ptr(bases), bases.size,
                                         tasks.ctypes.data, len(tasks), out.ctypes.data),
@@ -205,17 +208,24 @@ class Engine:
         return self.cigar_batch(scoring, bases, t)[0]
 
     def extend_chains(self, sc: Scoring, bases: np.ndarray, seeds: np.ndarray, chains: np.ndarray,
-                      genome_len: int):
+                      genome_len: int, out=None):
         """ExtensionAligner.extend for every chain (SEED_DTYPE seeds, CHAIN_DTYPE
         chains) against the uploaded forward strand -> (REGION_DTYPE array,
         per-chain region counts, GPU rounds).  Chain c's regions are
-        regions[seed_off : seed_off + counts[c]]."""
+        regions[seed_off : seed_off + counts[c]].  out: optional (regions,
+        counts) arrays of at least len(seeds) and len(chains) entries to write
+        into (in pinned memory the device writes them directly)."""
         assert seeds.dtype == abi.SEED_DTYPE and chains.dtype == abi.CHAIN_DTYPE
         bases = np.ascontiguousarray(bases, dtype=np.uint8)
         if bases.size == 0:
             bases = np.zeros(1, np.uint8)
-        out = np.zeros(max(len(seeds), 1), abi.REGION_DTYPE)
-        counts = np.zeros(max(len(chains), 1), np.uint32)
+        if out is None:
+            out = np.zeros(max(len(seeds), 1), abi.REGION_DTYPE)
+            counts = np.zeros(max(len(chains), 1), np.uint32)
+        else:
+            out, counts = out
+            assert out.dtype == abi.REGION_DTYPE and len(out) >= len(seeds)
+            assert counts.dtype == np.uint32 and len(counts) >= len(chains)
         rounds = C.c_uint32()
         _check(self.lib.swb_extend_chains(self.h, C.byref(sc), ptr(bases), bases.size, seeds.ctypes.data, len(seeds),
                                           chains.ctypes.data, len(chains), genome_len, out.ctypes.data,
@@ -322,14 +332,26 @@ class Engine:
 
     def smem_batch(self, bases: np.ndarray, read_off: np.ndarray, read_len: np.ndarray, min_seed_len: int,
                    min_intv: int = 1, cap_per_read: int = 64, split_len: int = 0, split_width: int = 10,
-                   out_cap: Optional[int] = None):
+                   out_cap: Optional[int] = None, out=None):
         """SMEMFinder.findAllSMEMs per read on the resident FM index, then (with
         split_len > 0) BWAMemAligner.internalReseed -> (SMEM_DTYPE packed
-        SMEMs, n_out, out_off); read r's SMEMs are out[out_off[r] : out_off[r] + n_out[r]]."""
+        SMEMs, n_out, out_off); read r's SMEMs are out[out_off[r] : out_off[r] + n_out[r]].
+        out: optional (SMEMs, n_out, out_off) arrays to write into (the SMEM
+        array's length is the capacity; in pinned memory the device writes
+        them directly)."""
         bases = np.ascontiguousarray(bases, dtype=np.uint8)
         read_off = np.ascontiguousarray(read_off, dtype=np.uint64)
         read_len = np.ascontiguousarray(read_len, dtype=np.int32)
         n = read_off.size
+        if out is not None:
+            sm, n_out, out_off = out
+            assert sm.dtype == SMEM_DTYPE and n_out.dtype == np.uint32 and out_off.dtype == np.uint64
+            assert len(n_out) >= max(n, 1) and len(out_off) >= max(n, 1)
+            _check(self.lib.swb_smem_batch(self.h, ptr(bases), bases.size, read_off.ctypes.data, read_len.ctypes.data,
+                                           n, int(min_seed_len), int(min_intv), int(split_len), int(split_width),
+                                           int(cap_per_read), sm.ctypes.data, int(sm.size), n_out.ctypes.data,
+                                           out_off.ctypes.data), "swb_smem_batch")
+            return sm, n_out[:n], out_off[:n]
         grow = out_cap is None
         if grow:
             out_cap = int(read_len.astype(np.int64).clip(0).sum()) + 16   # usually enough; grown below if not

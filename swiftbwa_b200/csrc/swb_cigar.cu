@@ -314,15 +314,7 @@ extern "C" int swb_cigar_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_
     // index, DP tasks) by the host threads, then one copy.  Bases and tasks
     // the caller already holds in pinned memory are copied from there
     // directly instead.
-    auto pinned = [](const void *p) {
-        cudaPointerAttributes at{};
-        if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-            cudaGetLastError();
-            return false;
-        }
-        return at.type == cudaMemoryTypeHost;
-    };
-    const bool direct = n_bases > 0 && pinned(bases) && pinned(tasks);
+    const bool direct = n_bases > 0 && is_pinned(bases) && is_pinned(tasks);
     char *stage = (char *)ctx->h_in.p;
     {
         const size_t bper = (n_bases + nth - 1) / nth;
@@ -409,7 +401,7 @@ extern "C" int swb_cigar_batch(swb_ctx *ctx, const swb_scoring *sc, const uint8_
     // buffers when they are pinned, else through pinned staging and host
     // threads.
     const size_t r_bytes = n * sizeof(swb_cigar_result), c_bytes = tot_c * 4;
-    const bool direct_out = pinned(results) && (tot_c == 0 || pinned(cigar_out)) && (tot_m == 0 || pinned(md_out));
+    const bool direct_out = is_pinned(results) && (tot_c == 0 || is_pinned(cigar_out)) && (tot_m == 0 || is_pinned(md_out));
     if (direct_out) {
         SWB_CUDA(cudaMemcpyAsync(results, base + o_res, r_bytes, cudaMemcpyDeviceToHost, st));
         if (tot_c) SWB_CUDA(cudaMemcpyAsync(cigar_out, d_cig, c_bytes, cudaMemcpyDeviceToHost, st));

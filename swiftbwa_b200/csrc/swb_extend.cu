@@ -430,10 +430,16 @@ extern "C" int swb_extend_chains(swb_ctx *ctx, const swb_scoring *sc, const uint
 
     SWB_CUDA(cudaMemsetAsync(ctx->d_counters, 0, sizeof(unsigned long long) * kNumCounters, st));
     SWB_CUDA(cudaEventRecord(ctx->ev_start, st));
-    // Inputs through the context's pinned staging buffer (host threads copy,
-    // then one transfer for the bases and one for the seeds and chains,
-    // which sit together at the start of the chain buffer).
-    {
+    // Inputs: straight from the caller's buffers when they are pinned, else
+    // through the context's pinned staging buffer (host threads copy, then
+    // one transfer for the bases and one for the seeds and chains, which sit
+    // together at the start of the chain buffer).
+    if ((n_bases == 0 || is_pinned(bases)) && (n_seeds == 0 || is_pinned(seeds)) && is_pinned(chains)) {
+        if (n_bases) SWB_CUDA(cudaMemcpyAsync(ctx->d_bases.p, bases, n_bases, cudaMemcpyHostToDevice, st));
+        if (n_seeds)
+            SWB_CUDA(cudaMemcpyAsync(base + o_seeds, seeds, n_seeds * sizeof(swb_seed), cudaMemcpyHostToDevice, st));
+        SWB_CUDA(cudaMemcpyAsync(base + o_chains, chains, nc * sizeof(swb_chain), cudaMemcpyHostToDevice, st));
+    } else {
         const size_t sc_bytes = o_chains + nc * sizeof(swb_chain);
         if ((rc = ensure_host(ctx, ctx->h_in, al256(n_bases) + sc_bytes))) return rc;
         char *stage = (char *)ctx->h_in.p, *stage_sc = stage + al256(n_bases);

@@ -189,6 +189,8 @@ struct DevSpan {
     size_t bytes;
 };
 void par_copy(void *dst, const void *src, size_t bytes);
+// True when p lies in page-locked host memory (cudaHostAlloc or registered).
+bool is_pinned(const void *p);
 int d2h_staged(swb_ctx *ctx, cudaStream_t st, std::initializer_list<DevSpan> parts, cudaEvent_t after_copies = nullptr);
 
 // Grow-only allocation against the context budget.

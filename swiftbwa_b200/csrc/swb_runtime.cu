@@ -199,21 +199,42 @@ void swb::par_copy(void *dst, const void *src, size_t bytes) {
     for (auto &x : th) x.join();
 }
 
+bool swb::is_pinned(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+// Parts whose destination is pinned are copied there directly; the rest go
+// through the context's pinned staging buffer and host threads.
 int swb::d2h_staged(swb_ctx *ctx, cudaStream_t st, std::initializer_list<DevSpan> parts, cudaEvent_t after_copies) {
     size_t total = 0;
-    for (const DevSpan &p : parts) total += align256(p.bytes);
+    std::vector<bool> direct;
+    for (const DevSpan &p : parts) {
+        direct.push_back(p.bytes > 0 && is_pinned(p.dst));
+        if (!direct.back()) total += align256(p.bytes);
+    }
     int rc;
     if ((rc = ensure_host(ctx, ctx->h_out, std::max<size_t>(total, 256)))) return rc;
     char *stage = (char *)ctx->h_out.p;
-    size_t off = 0;
+    size_t off = 0, k = 0;
     for (const DevSpan &p : parts) {
+        if (direct[k++]) {
+            SWB_CUDA(cudaMemcpyAsync(p.dst, p.dev, p.bytes, cudaMemcpyDeviceToHost, st));
+            continue;
+        }
         if (p.bytes) SWB_CUDA(cudaMemcpyAsync(stage + off, p.dev, p.bytes, cudaMemcpyDeviceToHost, st));
         off += align256(p.bytes);
     }
     if (after_copies) SWB_CUDA(cudaEventRecord(after_copies, st));
     SWB_CUDA(cudaStreamSynchronize(st));
-    off = 0;
+    off = 0, k = 0;
     for (const DevSpan &p : parts) {
+        if (direct[k++]) continue;
         par_copy(p.dst, stage + off, p.bytes);
         off += align256(p.bytes);
     }

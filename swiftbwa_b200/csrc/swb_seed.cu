@@ -541,14 +541,21 @@ int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uin
     g.first_over = d_misc + 1;
     g.cand = (longlong2 *)sp;
     g.entries = entries;
-    // Inputs through the context's pinned staging buffer in the device layout
+    // Inputs: straight from the caller's buffers when all three are pinned,
+    // else through the context's pinned staging buffer in the device layout
     // (host threads copy, then one transfer).
-    if ((rc = ensure_host(ctx, ctx->h_in, b_bytes + o_bytes + l_bytes))) return rc;
-    char *stage = (char *)ctx->h_in.p;
-    par_copy(stage, bases, n_bases);
-    par_copy(stage + b_bytes, read_off, n_reads * 8);
-    par_copy(stage + b_bytes + o_bytes, read_len, n_reads * 4);
-    SWB_CUDA(cudaMemcpyAsync(in, stage, b_bytes + o_bytes + l_bytes, cudaMemcpyHostToDevice, st));
+    if (is_pinned(bases) && is_pinned(read_off) && is_pinned(read_len)) {
+        SWB_CUDA(cudaMemcpyAsync(in, bases, n_bases, cudaMemcpyHostToDevice, st));
+        SWB_CUDA(cudaMemcpyAsync(in + b_bytes, read_off, n_reads * 8, cudaMemcpyHostToDevice, st));
+        SWB_CUDA(cudaMemcpyAsync(in + b_bytes + o_bytes, read_len, n_reads * 4, cudaMemcpyHostToDevice, st));
+    } else {
+        if ((rc = ensure_host(ctx, ctx->h_in, b_bytes + o_bytes + l_bytes))) return rc;
+        char *stage = (char *)ctx->h_in.p;
+        par_copy(stage, bases, n_bases);
+        par_copy(stage + b_bytes, read_off, n_reads * 8);
+        par_copy(stage + b_bytes + o_bytes, read_len, n_reads * 4);
+        SWB_CUDA(cudaMemcpyAsync(in, stage, b_bytes + o_bytes + l_bytes, cudaMemcpyHostToDevice, st));
+    }
     SWB_CUDA(cudaMemsetAsync(d_misc, 0, 4, st));
     SWB_CUDA(cudaMemsetAsync(d_misc + 1, 0xFF, 4, st));
     SWB_CUDA(cudaMemsetAsync(ctx->d_counters, 0, sizeof(unsigned long long) * kNumCounters, st));

@@ -53,16 +53,6 @@ uint64_t now_ns() {
         .count();
 }
 
-bool is_pinned(const void *p) {
-    if (!p) return false;
-    cudaPointerAttributes a;
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return a.type == cudaMemoryTypeHost;
-}
-
 struct Req {
     uint64_t ticket = 0;
     const uint8_t *bases = nullptr;

@@ -67,6 +67,14 @@ def test_extend_chains_matches_oracle(engine, oracle_mod, name):
     wl = W.chains(ref, 77 + len(name), 1500, 150, sub=0.03, indel=0.01, spurious_frac=0.3, a=sc.a)
     rounds = _compare(engine, oracle_mod, sc, wl)
     assert rounds >= 1
+    if name == "default":   # pinned inputs and outputs: copied straight to and from the device
+        import torch
+        from swiftbwa_b200.abi import REGION_DTYPE
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8)).pin_memory().numpy().view(a.dtype)
+        regs, counts, _ = engine.extend_chains(sc, wl.bases, wl.seeds, wl.chains, ref.n)
+        out = (pin(np.zeros(len(wl.seeds), REGION_DTYPE)), pin(np.full(len(wl.chains), 7, np.uint32)))
+        pr, pc, _ = engine.extend_chains(sc, pin(wl.bases), pin(wl.seeds), pin(wl.chains), ref.n, out=out)
+        assert pr is out[0] and np.array_equal(pc, counts) and np.array_equal(pr, regs)
 
 
 def test_extend_chains_edges(engine, oracle_mod):

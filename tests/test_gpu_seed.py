@@ -96,6 +96,15 @@ def test_long_and_ragged_reads(engine, oracle_mod, index):
     assert over == 0 and np.array_equal(gn, en) and en.sum() > 0
     for r in range(n):
         assert np.array_equal(got[goff[r]: goff[r] + gn[r]], exp[r * cap: r * cap + en[r]]), f"read {r}"
+    # Pinned reads and outputs: copied straight to and from the device, the same SMEMs.
+    import torch
+    from swiftbwa_b200.abi import SMEM_DTYPE
+    tot = int(gn.sum())
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8)).pin_memory().numpy().view(a.dtype)
+    out = (pin(np.full((tot + 1) * SMEM_DTYPE.itemsize, 0xA5, np.uint8)).view(SMEM_DTYPE),
+           pin(np.zeros(n, np.uint32)), pin(np.zeros(n, np.uint64)))
+    pg, pn, po = engine.smem_batch(pin(bases), pin(off), pin(lens), 15, cap_per_read=cap, split_len=28, out=out)
+    assert np.array_equal(pn, gn) and np.array_equal(po, goff) and np.array_equal(pg[:tot], got[:tot])
 
 
 def test_small_window_reports_counts(engine, oracle_mod, index):
