@@ -195,7 +195,8 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
     """Configs 0, 2, 3, 4, 5 and the config-1 NW+CIGAR stage, each bounded to a
     few seconds of GPU time; CPU-oracle samples beside them."""
     from swiftbwa_b200 import workloads as W
-    from swiftbwa_b200.abi import EXT_RESULT_DTYPE, CIGAR_RESULT_DTYPE, CIGAR_TASK_DTYPE
+    from swiftbwa_b200.abi import (EXT_RESULT_DTYPE, CIGAR_RESULT_DTYPE, CIGAR_TASK_DTYPE, LOCAL_RESULT_DTYPE,
+                                   REGION_DTYPE, SMEM_DTYPE)
     from oracle import oracle
     threads = os.cpu_count() or 1
     out = {}
@@ -263,12 +264,19 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
     if want("config3"):
         wl3 = W.config3(n=args.c3_pairs)
         eng.upload_reference(wl3.ref.pac, wl3.ref.n)
-        eng.local_batch(sc, wl3.bases, wl3.tasks[:1000])
+        # Inputs and results in pinned host memory (allocated once), as the
+        # headline's end-to-end leg.
+        pb3 = torch.from_numpy(wl3.bases).pin_memory().numpy()
+        pt3 = torch.from_numpy(wl3.tasks.view(np.uint8)).pin_memory().numpy().view(wl3.tasks.dtype)
+        po3 = torch.empty(len(wl3.tasks) * LOCAL_RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy() \
+            .view(LOCAL_RESULT_DTYPE)
+        eng.local_batch(sc, pb3, pt3[:1000], out=po3)
         t0 = time.perf_counter()
-        r3 = eng.local_batch(sc, wl3.bases, wl3.tasks)
+        r3 = eng.local_batch(sc, pb3, pt3, out=po3)
         e2e3 = time.perf_counter() - t0
         ms3, cells3 = eng.last_batch_stats()
         c3 = {"pairs": len(wl3.tasks), "kernel_ms": ms3, "rescues_per_s": len(wl3.tasks) / ms3 * 1e3,
+              "buffers": "pinned host memory (bases, tasks, results; allocated once)",
               "e2e_rescues_per_s": len(wl3.tasks) / e2e3, "gcups": cells3 / ms3 / 1e6,
               "hits": int(np.sum(r3["score"] >= 19))}
         if cpu_on:
@@ -386,16 +394,25 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
     if want("config5_extend_chains"):
         wl5 = W.config5(n_reads=args.c5_chains, ref_len=args.ref_len)
         eng.upload_reference(wl5.ref.pac, wl5.ref.n)
-        eng.extend_chains(sc, wl5.bases, wl5.seeds, wl5.chains, wl5.ref.n)
+        # Inputs and outputs in pinned host memory (allocated once), as the
+        # headline's end-to-end leg: the device reads and writes them directly.
+        pb5 = torch.from_numpy(wl5.bases).pin_memory().numpy()
+        ps5 = torch.from_numpy(wl5.seeds.view(np.uint8)).pin_memory().numpy().view(wl5.seeds.dtype)
+        pc5 = torch.from_numpy(wl5.chains.view(np.uint8)).pin_memory().numpy().view(wl5.chains.dtype)
+        po5 = (torch.empty(max(len(wl5.seeds), 1) * REGION_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy()
+               .view(REGION_DTYPE),
+               torch.empty(max(len(wl5.chains), 1), dtype=torch.int32).pin_memory().numpy().view(np.uint32))
+        eng.extend_chains(sc, pb5, ps5, pc5, wl5.ref.n, out=po5)
         times = []
         for _ in range(3):
             t0 = time.perf_counter()
-            g5, n5, rounds5 = eng.extend_chains(sc, wl5.bases, wl5.seeds, wl5.chains, wl5.ref.n)
+            g5, n5, rounds5 = eng.extend_chains(sc, pb5, ps5, pc5, wl5.ref.n, out=po5)
             times.append(time.perf_counter() - t0)
         e2e5 = float(np.median(times))
         _, cells5 = eng.last_batch_stats()
         c5 = {"chains": len(wl5.chains), "seeds": len(wl5.seeds), "regions": int(n5.sum()), "rounds": rounds5,
-              "chains_per_s": len(wl5.chains) / e2e5, "gcups_wall": cells5 / e2e5 / 1e9}
+              "chains_per_s": len(wl5.chains) / e2e5, "gcups_wall": cells5 / e2e5 / 1e9,
+              "buffers": "pinned host memory (bases, seeds, chains, regions, counts; allocated once)"}
         if cpu_on:
             s5 = 100_000
             t0 = time.perf_counter()
@@ -429,18 +446,29 @@ def secondary_suite(eng, sc, args, dev, torch, cpu_on=True, only=None):
         # Phases 1 and 1.25 of alignReadPhase1to3: findAllSMEMs, then internal
         # re-seeding (split length Int(Float(19) * 1.5 + 0.499) = 28, split width 10).
         split6 = oracle.split_len_of(19, 1.5)
-        eng.smem_batch(wl6.bases[: 10_000 * L], off6[:10_000], len6[:10_000], 19, cap_per_read=cap6,
-                       split_len=split6)
+        # One call with library-sized outputs sizes the pinned output buffers;
+        # the timed calls read pinned reads and write pinned outputs directly.
+        _, n0, _ = eng.smem_batch(wl6.bases, off6, len6, 19, cap_per_read=cap6, split_len=split6)
+        tot6 = int(n0.sum())
+        pb6 = torch.from_numpy(wl6.bases).pin_memory().numpy()
+        poff6 = torch.from_numpy(off6.view(np.uint8)).pin_memory().numpy().view(np.uint64)
+        plen6 = torch.from_numpy(len6.view(np.uint8)).pin_memory().numpy().view(np.int32)
+        pout6 = (torch.empty((tot6 + 1024) * SMEM_DTYPE.itemsize, dtype=torch.uint8).pin_memory().numpy()
+                 .view(SMEM_DTYPE),
+                 torch.empty(nr, dtype=torch.int32).pin_memory().numpy().view(np.uint32),
+                 torch.empty(nr * 8, dtype=torch.uint8).pin_memory().numpy().view(np.uint64))
+        eng.smem_batch(pb6, poff6, plen6, 19, cap_per_read=cap6, split_len=split6, out=pout6)
         times = []
         for _ in range(3):
             t0 = time.perf_counter()
-            sm6, n6, o6 = eng.smem_batch(wl6.bases, off6, len6, 19, cap_per_read=cap6, split_len=split6)
+            sm6, n6, o6 = eng.smem_batch(pb6, poff6, plen6, 19, cap_per_read=cap6, split_len=split6, out=pout6)
             times.append(time.perf_counter() - t0)
         e2e6 = float(np.median(times))
         ms6, exts6 = eng.last_batch_stats()
         # Bytes the rank queries read: one or two 64-byte checkpoints per
         # backward extension, counted as 96 bytes (1.5 checkpoints) each.
         c6 = {"reads": nr, "read_len": L, "smems": int(n6.sum()), "kernel_ms": ms6,
+              "buffers": "pinned host memory (reads, offsets, lengths, SMEMs, counts, offsets; allocated once)",
               "reads_per_s_kernel": nr / ms6 * 1e3, "reads_per_s_e2e": nr / e2e6,
               "smems_per_s_kernel": float(n6.sum()) / ms6 * 1e3,
               "backward_extensions": int(exts6), "backward_ext_per_s": exts6 / ms6 * 1e3,
