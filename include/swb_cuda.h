@@ -344,7 +344,10 @@ typedef struct swb_region {
  * (left, its band retry, right, its band retry), so the covered-region
  * skip, the retries and the left-to-right h0 chaining are the reference's.
  * Chain c's regions are out[seed_off .. seed_off + n_regions[c]) (at most
- * one region per seed).  *rounds (optional) receives the GPU batches run. */
+ * one region per seed).  *rounds (optional) receives the GPU batches run.
+ * Inputs (bases, seeds, chains) and outputs (out, n_regions) in pinned host
+ * memory are copied straight to and from the device; pageable ones go
+ * through the context's pinned staging buffer and host threads. */
 int swb_extend_chains(swb_ctx *ctx, const swb_scoring *sc,
                       const uint8_t *bases, size_t n_bases,
                       const swb_seed *seeds, size_t n_seeds,
@@ -451,7 +454,9 @@ int swb_upload_bwt(swb_ctx *ctx, const swb_bwt_checkpoint *cp, uint64_t n_cp, co
  * out_cap the call returns SWB_ERR_TOO_LARGE with n_out and out_off filled
  * and nothing written to out.  Either way the caller can retry with larger
  * bounds, and every other read's results are complete.  At most 2^31-16
- * reads per call.  Replaces
+ * reads per call.  Inputs (bases, read_off, read_len) and outputs (out,
+ * n_out, out_off) in pinned host memory are copied straight to and from the
+ * device; pageable ones go through pinned staging and host threads.  Replaces
  * the CPU loop of BWAMemAligner.alignReadPhase1to3 (BWAMemAligner.swift:133-139)
  * and the Metal forward kernel (Kernels/smem_forward.metal:117) for a batch. */
 int swb_smem_batch(swb_ctx *ctx, const uint8_t *bases, size_t n_bases, const uint64_t *read_off,
