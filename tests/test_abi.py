@@ -84,3 +84,18 @@ def test_init_without_gpu_reports_no_device(lib):
         pytest.skip("a GPU is visible here")
     assert rc == abi.SWB_ERR_NO_DEVICE
     assert b"device" in lib.swb_last_error_message()
+
+
+def test_cigar_caps_follow_the_header_rule():
+    """Engine.cigar_caps sizes swb_cigar_batch's outputs by the header's rule:
+    cigar_cap = sum(qlen + rlen + 2) words, md_cap = sum(6*(qlen+rlen)+8) bytes
+    (one spare entry each)."""
+    import numpy as np
+    from swiftbwa_b200.alignment import Engine
+    rng = np.random.default_rng(3)
+    t = np.zeros(1000, abi.CIGAR_TASK_DTYPE)
+    t["qlen"] = rng.integers(0, 300, t.size)
+    t["rlen"] = rng.integers(0, 400, t.size)
+    q, r = t["qlen"].astype(np.int64), t["rlen"].astype(np.int64)
+    assert Engine.cigar_caps(t) == (int((q + r + 2).sum()) + 1, int((6 * (q + r) + 8).sum()) + 1)
+    assert Engine.cigar_caps(t[:0]) == (1, 1)
