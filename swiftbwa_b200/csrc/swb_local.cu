@@ -260,9 +260,9 @@ __device__ PassOut striped_pass(const LocalArgs &a, const swb_local_task &tk, bo
     return o;
 }
 
-// Five 128-thread blocks per SM (96 registers; one 4-byte spill since the
-// target rows are loaded 16 columns ahead, which still ran 5 % faster; six
-// blocks spill more).  The grid is the device's resident blocks; each
+// Five 128-thread blocks per SM (96 registers: no spills up to 10 stripes,
+// 44-164 bytes per thread from 11 to 16; six blocks spill more).  The grid
+// is the device's resident blocks; each
 // half-warp claims its next task of the bin from the bin's counter, longest
 // target first (the sort puts them last), so the launch ends with the work
 // rather than on a partly filled last wave of fixed slices.
@@ -509,9 +509,10 @@ int launch_local(swb_ctx *ctx, const DevScoring &sc, const uint8_t *d_bases, con
     unsigned long long *pbuf = (unsigned long long *)(ebuf + (size_t)(max_t + 1) * nsl);
 
     LocalArgs a{sc, d_bases, ctx->d_pac, d_tasks, d_out, idx2, bin_start, fallback, fallback_n, d_cells, claim};
-    // Bin sizes are not known on the host; each instantiation's grid covers
-    // up to n tasks and idles past its slice.  Only stripe counts that can
-    // occur for max_q are launched.
+    // Bin sizes are not known on the host; each instantiation's grid is the
+    // device's resident blocks (fewer for small batches), whose half-warps
+    // claim the bin's tasks and leave when it has none left.  Only stripe
+    // counts that can occur for max_q are launched.
     const int max_sn = imin(16, (max_q + 15) / 16);
     using L = int (*)(swb_ctx *, const LocalArgs &, cudaStream_t, uint32_t *, int, size_t, size_t);
     static const L fns[17] = {nullptr,        launch_sn<1>,  launch_sn<2>,  launch_sn<3>,  launch_sn<4>,  launch_sn<5>,
