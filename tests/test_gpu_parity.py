@@ -225,6 +225,27 @@ def test_local_fuzz(engine, oracle_mod, si):
     assert bad.size == 0, f"{bad.size} mismatches, first {bad[:5]}: {got[bad[:3]]} vs {exp[bad[:3]]} tasks {d['tasks'][bad[:3]]}"
 
 
+def test_local_many_claims_per_half_warp(oracle_mod):
+    """60k mate-rescue pairs of one stripe count (150-base mates, ~700-base
+    windows): the striped kernel's grid is the device's resident blocks, so
+    each half-warp claims about ten tasks of the bin from its counter, longest
+    target first; every field against the oracle."""
+    from swiftbwa_b200 import workloads as W
+    from swiftbwa_b200.alignment import Engine
+    sc = Scoring.default()
+    wl = W.config3(n=60_000)
+    eng = Engine(0)
+    try:
+        eng.upload_reference(wl.ref.pac, wl.ref.n)
+        got = eng.local_batch(sc, wl.bases, wl.tasks)
+    finally:
+        eng.close()
+    exp, _ = oracle_mod.local_batch(sc, wl.bases, wl.tasks, pac=wl.ref.pac, ref_bases=wl.ref.n, n_threads=8)
+    bad = _cmp_struct(got, exp, got.dtype.names)
+    assert bad.size == 0, f"{bad.size} mismatches, first {bad[:5]}"
+    assert (exp["score"] > 0).sum() > 50_000
+
+
 def test_ext_config_workloads_chunked(engine, oracle_mod):
     """Config-0 and a 2.6M-task config-1 shard through the host entry point
     (the latter runs as pipelined chunks), every task against the oracle."""
